@@ -1,0 +1,67 @@
+"""Build the sm_100a engine library in-tree.
+
+    python -m eemd4cuda_b200.build            # release + checked libraries
+
+Outputs (git-ignored, shipped next to the sources):
+    eemd4cuda_b200/lib/libeemd_b200.so          release build
+    eemd4cuda_b200/lib/libeemd_b200_checked.so  -DEEMD_CHECKED: every staged
+        index is range-checked on the device and a violation is reported as an
+        error status instead of an out-of-bounds access
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+LIB = PKG / "lib"
+INCLUDE = PKG.parent / "include"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = [
+    "-O3", "-lineinfo", "-std=c++17", "--fmad=false",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "-shared",
+    "-I", str(INCLUDE),
+]
+SOURCES = ["eemd_engine.cu"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found; the sm_100a engine cannot be built")
+
+
+def _stale(out: Path, deps) -> bool:
+    if not out.exists():
+        return True
+    t = out.stat().st_mtime
+    return any(p.stat().st_mtime > t for p in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> list[Path]:
+    LIB.mkdir(exist_ok=True)
+    deps = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+    outs = []
+    for name, extra in (("libeemd_b200.so", []), ("libeemd_b200_checked.so", ["-DEEMD_CHECKED"])):
+        out = LIB / name
+        outs.append(out)
+        if not force and not _stale(out, deps):
+            continue
+        tmp = out.with_suffix(".so.tmp")
+        cmd = [nvcc(), *ARCH, *COMMON, *extra, "-o", str(tmp), *[str(CSRC / s) for s in SOURCES]]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+        os.replace(tmp, out)
+    return outs
+
+
+if __name__ == "__main__":
+    for p in build(force="--force" in sys.argv, verbose=True):
+        print(p)

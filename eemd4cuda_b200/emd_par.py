@@ -1,0 +1,354 @@
+"""Drop-in replacement of the reference's public EMD/EEMD module (emd_par.py).
+
+PUBLIC API (same names, arguments and errors as emd_par.py:1-33, 260-301)
+    result = decompose(x, method='auto', E=64, eps=0.2, tau=0.25,
+                       max_sifts=50, max_imf=-1, min_extrema=4,
+                       end='natural', n_workers=None, seed=0, batch=None)
+    result.imfs / .residual / .n_modes / .stats / .recon_error()
+    result.save(path) / EMDResult.load(path)
+    gpu_eemd_full(X[E,N], E, tau, max_sifts, max_imf) -> (imfs, nsift, nmode)
+    make_reference_sweep(...)
+
+Every decomposition runs on the sm_100a engine (libeemd_b200.so); there is
+no CPU backend, so method='cpu' raises ValueError.  PyTorch tensors serve as
+device buffers only.
+
+Keyword-only extensions:
+    noise  'philox' (default): counter-based device noise keyed by
+           (seed, trial); 'reference-gpu': the host stream of the reference's
+           GPU path (one default_rng(seed) draw of (E, N), emd_par.py:225-233);
+           'reference-cpu': the per-trial seeds of its CPU path
+           (emd_par.py:117-118).  The two reference streams are drawn on the
+           host with numpy and injected, so results match the reference's
+           inputs bit for bit.
+    rules  'ref' (emd_ref.py stop rules, default) or 'numba' (emd_gpu.py).
+    exact  True: reference float64 operation order (parity mode).
+    dtype  np.float64 (default) or np.float32 storage.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+
+__all__ = ["decompose", "EMDResult", "make_reference_sweep", "gpu_eemd_full", "EngineConfig"]
+
+
+# =====================================================================
+# Result container (emd_par.py:67-97)
+# =====================================================================
+@dataclass
+class EMDResult:
+    imfs: np.ndarray          # [n_modes, N]
+    residual: np.ndarray      # [N]
+    n_modes: int
+    stats: dict = field(default_factory=dict)
+
+    def recon_error(self) -> float:
+        """Partition-of-unity check: max|x - (sum(imfs)+residual)| (0 if x not stored)."""
+        recon = self.imfs.sum(axis=0) + self.residual
+        x = self.stats.get("x", None)
+        if x is None:
+            return 0.0
+        return float(np.max(np.abs(x - recon)))
+
+    def save(self, path: str):
+        scalars = {k: v for k, v in self.stats.items()
+                   if isinstance(v, (int, float, str, np.integer, np.floating))
+                   and k not in ("n_modes",)}
+        np.savez_compressed(path, imfs=self.imfs, residual=self.residual,
+                            n_modes=self.n_modes, **scalars)
+
+    @staticmethod
+    def load(path: str) -> "EMDResult":
+        d = np.load(path, allow_pickle=False)
+        return EMDResult(imfs=d["imfs"], residual=d["residual"], n_modes=int(d["n_modes"]),
+                         stats={k: d[k] for k in d.files
+                                if k not in ("imfs", "residual", "n_modes")})
+
+
+@dataclass
+class EngineConfig:
+    """Engine knobs beyond the reference's signature (0 = autotune)."""
+    tile: int = 0
+    knots_per_block: int = 0
+    halo: int = 0
+    watchdog: int = 0
+
+
+_RULES = {"ref": L.EEMD_RULES_REF, "numba": L.EEMD_RULES_NUMBA}
+_ENDS = {"natural": L.EEMD_END_NATURAL, "mirror": L.EEMD_END_MIRROR}
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("the B200 EEMD engine needs a CUDA device (no CPU fallback)")
+    return torch
+
+
+def imf_slots(N: int, max_imf: int) -> int:
+    """IMF slots per trial: max_imf, or for max_imf=-1 a bound on the number of
+    modes of an N-sample signal (each IMF removes the fastest oscillation; the
+    reference's GPU path caps at 64, emd_par.py:205-206)."""
+    if max_imf is not None and max_imf != -1:
+        if max_imf < 1:
+            raise ValueError("max_imf must be -1 or >= 1")
+        return int(max_imf)
+    return int(min(64, max(8, math.ceil(math.log2(max(N, 2))) + 8)))
+
+
+def make_params(*, dtype=np.float64, noise_mode=L.EEMD_NOISE_NONE, eps=0.2, seed=0, tau=0.25,
+                max_sifts=50, max_imf=16, min_extrema=4, end="natural", rules="ref",
+                exact=False, config: EngineConfig | None = None) -> L.EemdParams:
+    if end not in _ENDS:
+        raise ValueError("end must be 'natural' or 'mirror'")
+    if rules not in _RULES:
+        raise ValueError("rules must be 'ref' or 'numba'")
+    if int(max_sifts) < 1:
+        raise ValueError("max_sifts must be >= 1")
+    dt = np.dtype(dtype)
+    if dt not in (np.dtype(np.float64), np.dtype(np.float32)):
+        raise ValueError("dtype must be float64 or float32")
+    if exact and dt != np.dtype(np.float64):
+        raise ValueError("exact mode needs float64")
+    cfg = config or EngineConfig()
+    p = L.default_params()
+    p.dtype = L.EEMD_F64 if dt == np.dtype(np.float64) else L.EEMD_F32
+    p.noise_mode = int(noise_mode)
+    p.eps = float(eps)
+    p.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+    p.tau = float(tau)
+    p.max_sifts = int(max_sifts)
+    p.max_imf = int(max_imf)
+    p.min_extrema = int(min_extrema)
+    p.end_mode = _ENDS[end]
+    p.rules = _RULES[rules]
+    p.exact = 1 if exact else 0
+    p.tile = int(cfg.tile)
+    p.knots_per_block = int(cfg.knots_per_block)
+    p.halo = int(cfg.halo)
+    p.watchdog = int(cfg.watchdog)
+    return p
+
+
+def _tdtype(torch, dt):
+    return torch.float64 if np.dtype(dt) == np.dtype(np.float64) else torch.float32
+
+
+def reference_noise(x: np.ndarray, E: int, eps: float, seed: int, stream: str) -> np.ndarray:
+    """The reference's own noise arrays, scaled by eps*std(x).
+    'reference-gpu': emd_par.py:225,233 (one default_rng(seed) stream, (E, N));
+    'reference-cpu': emd_par.py:117-118 (default_rng((seed*1000003+e) mod 2^64) per trial)."""
+    N = len(x)
+    sigma = eps * np.std(x)
+    if stream == "reference-gpu":
+        return np.random.default_rng(seed).standard_normal((E, N)) * sigma
+    if stream == "reference-cpu":
+        out = np.empty((E, N))
+        for e in range(E):
+            rng = np.random.default_rng((seed * 1000003 + e) & 0xFFFFFFFFFFFFFFFF)
+            out[e] = rng.standard_normal(N) * sigma
+        return out
+    raise ValueError("unknown noise stream %r" % (stream,))
+
+
+def _auto_batch(torch, p, N, E, bytes_per_el):
+    """Trials resident at once: 70 % of free device memory (emd_par.py:214-223)."""
+    free, _ = torch.cuda.mem_get_info()
+    per_trial = L.workspace_size(p, [N], 1, False)
+    b = max(1, int(free * 0.7 // max(per_trial, 1)))
+    return min(E, b)
+
+
+def _run_ensemble(x, *, E, eps, tau, max_sifts, max_imf, min_extrema, end, seed, batch,
+                  noise, rules, exact, dtype, config):
+    """EEMD of one signal: batches of trials into device sums, then mean/residual."""
+    torch = _torch()
+    N = len(x)
+    slots = imf_slots(N, max_imf)
+    dt = np.dtype(dtype)
+    tdt = _tdtype(torch, dt)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    if E == 1:
+        nmode_kind = L.EEMD_NOISE_NONE
+    elif noise == "philox":
+        nmode_kind = L.EEMD_NOISE_PHILOX
+    elif noise in ("reference-gpu", "reference-cpu"):
+        nmode_kind = L.EEMD_NOISE_INJECTED
+    else:
+        raise ValueError("noise must be 'philox', 'reference-gpu' or 'reference-cpu'")
+    p = make_params(dtype=dt, noise_mode=nmode_kind, eps=eps, seed=seed, tau=tau,
+                    max_sifts=max_sifts, max_imf=slots, min_extrema=min_extrema, end=end,
+                    rules=rules, exact=exact, config=config)
+    if batch is None:
+        batch = _auto_batch(torch, p, N, E, dt.itemsize)
+    batch = max(1, min(int(batch), E))
+    host_noise = (reference_noise(x, E, eps, seed, noise)
+                  if nmode_kind == L.EEMD_NOISE_INJECTED else None)
+
+    xd = torch.from_numpy(np.ascontiguousarray(x, dtype=dt)).to(dev)
+    imf_sum = torch.zeros((slots, N), dtype=torch.float64, device=dev)
+    mode_count = torch.zeros((slots,), dtype=torch.int32, device=dev)
+    per_trial_sifts, per_trial_modes, flags_all = [], [], []
+    ws = None
+    t0 = time.time()
+    for b0 in range(0, E, batch):
+        b1 = min(E, b0 + batch)
+        Eb = b1 - b0
+        need = L.workspace_size(p, [N], Eb, False)
+        if ws is None or ws.numel() < need:
+            ws = torch.empty((need,), dtype=torch.uint8, device=dev)
+        nz = None
+        if host_noise is not None:
+            nz = torch.from_numpy(np.ascontiguousarray(host_noise[b0:b1], dtype=dt)).to(dev)
+        nsift = torch.empty((Eb,), dtype=torch.int32, device=dev)
+        nmode = torch.empty((Eb,), dtype=torch.int32, device=dev)
+        flags = torch.empty((Eb,), dtype=torch.int32, device=dev)
+        L.run(p, xd, [N], b0, Eb, ws, noise=nz, imf_sum=imf_sum, mode_count=mode_count,
+              nsift=nsift, nmode=nmode, flags=flags)
+        per_trial_sifts.extend(nsift.cpu().tolist())
+        per_trial_modes.extend(nmode.cpu().tolist())
+        flags_all.extend(flags.cpu().tolist())
+    imf_mean = torch.empty((slots, N), dtype=torch.float64, device=dev)
+    resid = torch.empty((N,), dtype=torch.float64, device=dev)
+    n_modes_d = torch.empty((1,), dtype=torch.int32, device=dev)
+    L.finalize(p, xd, [N], imf_sum, mode_count, imf_mean, resid, n_modes_d)
+    n_modes = int(n_modes_d.item())
+    imfs = imf_mean[:n_modes].cpu().numpy()
+    residual = resid.cpu().numpy()
+    dt_s = time.time() - t0
+    reached = any(f & 1 for f in flags_all)
+    stats = dict(method="gpu", backend="b200", E=E, n_modes=n_modes, batch=batch,
+                 per_trial_total_sifts=np.array(per_trial_sifts),
+                 per_trial_n_modes=np.array(per_trial_modes),
+                 max_imf_reached=bool(reached and max_imf == -1),
+                 gpu_time_s=dt_s, noise=noise if E > 1 else "none", x=np.asarray(x, dtype=float))
+    return imfs, residual, stats
+
+
+def _run_single(x, *, tau, max_sifts, max_imf, min_extrema, end, rules, exact, dtype, config):
+    """Plain EMD (E=1): the trial's own IMFs and its sequential residual, like
+    the reference's E=1 CPU path (emd_par.py:146-154)."""
+    torch = _torch()
+    N = len(x)
+    slots = imf_slots(N, max_imf)
+    dt = np.dtype(dtype)
+    tdt = _tdtype(torch, dt)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    p = make_params(dtype=dt, noise_mode=L.EEMD_NOISE_NONE, tau=tau, max_sifts=max_sifts,
+                    max_imf=slots, min_extrema=min_extrema, end=end, rules=rules, exact=exact,
+                    config=config)
+    xd = torch.from_numpy(np.ascontiguousarray(x, dtype=dt)).to(dev)
+    ws = torch.empty((L.workspace_size(p, [N], 1, True),), dtype=torch.uint8, device=dev)
+    imfs = torch.zeros((1, slots, N), dtype=tdt, device=dev)
+    resid = torch.empty((1, N), dtype=tdt, device=dev)
+    nsift = torch.empty((1,), dtype=torch.int32, device=dev)
+    nmode = torch.empty((1,), dtype=torch.int32, device=dev)
+    msifts = torch.empty((1, slots), dtype=torch.int32, device=dev)
+    flags = torch.empty((1,), dtype=torch.int32, device=dev)
+    t0 = time.time()
+    L.run(p, xd, [N], 0, 1, ws, imfs=imfs, resid_out=resid, nsift=nsift, nmode=nmode,
+          mode_sifts=msifts, flags=flags)
+    nm = int(nmode.item())
+    out = imfs[0, :nm].to(torch.float64).cpu().numpy()
+    res = resid[0].to(torch.float64).cpu().numpy()
+    per_mode = msifts[0, :nm].cpu().tolist()
+    stats = dict(method="gpu", backend="b200", E=1, n_modes=nm, total_sifts=int(nsift.item()),
+                 per_mode_sifts=per_mode, per_trial_total_sifts=np.array([int(nsift.item())]),
+                 max_imf_reached=bool(int(flags.item()) & 1 and max_imf == -1),
+                 gpu_time_s=time.time() - t0, x=np.asarray(x, dtype=float))
+    return out, res, stats
+
+
+# =====================================================================
+# Public API (emd_par.py:260-301)
+# =====================================================================
+def decompose(x, method="auto", E=64, eps=0.2, tau=0.25, max_sifts=50, max_imf=-1,
+              min_extrema=4, end="natural", n_workers=None, seed=0, parallel=True, batch=None,
+              nthreads=128, *, noise="philox", rules="ref", exact=False, dtype=np.float64,
+              config: EngineConfig | None = None):
+    """Decompose a 1-D signal x into IMFs (+ residual) on the B200 engine.
+
+    Arguments follow emd_par.decompose; n_workers, parallel and nthreads are
+    accepted for signature compatibility and ignored (the engine picks its own
+    launch shapes).  Returns EMDResult with .imfs [n_modes, N] (float64),
+    .residual [N], .n_modes and .stats.
+    """
+    x = np.asarray(x, dtype=float)
+    if x.ndim != 1:
+        raise ValueError("x must be 1-D")
+    N = len(x)
+    if N < 8:
+        raise ValueError("signal too short for EMD (need >= 8 samples)")
+    if method == "cpu":
+        raise ValueError("method='cpu' is not provided by the B200 engine (no CPU backend); "
+                         "use method='gpu' or 'auto'")
+    if method not in ("auto", "gpu"):
+        raise ValueError("method must be 'auto', 'cpu', or 'gpu'")
+    E = int(E)
+    if E < 1:
+        raise ValueError("E must be >= 1")
+    if E == 1:
+        imfs, resid, stats = _run_single(x, tau=tau, max_sifts=max_sifts, max_imf=max_imf,
+                                         min_extrema=min_extrema, end=end, rules=rules,
+                                         exact=exact, dtype=dtype, config=config)
+    else:
+        imfs, resid, stats = _run_ensemble(x, E=E, eps=eps, tau=tau, max_sifts=max_sifts,
+                                           max_imf=max_imf, min_extrema=min_extrema, end=end,
+                                           seed=seed, batch=batch, noise=noise, rules=rules,
+                                           exact=exact, dtype=dtype, config=config)
+    return EMDResult(imfs=imfs, residual=resid, n_modes=imfs.shape[0], stats=stats)
+
+
+def gpu_eemd_full(x, E=64, tau=0.25, max_sifts=50, max_imf=12, seed=0, K=None, nthreads=128,
+                  batch=None, *, rules="numba", exact=False, end="natural", min_extrema=4,
+                  config: EngineConfig | None = None):
+    """Raw per-trial decomposition of already perturbed signals
+    (emd_gpu.py:301-334).  x: [E, N] (or [N] with E=1).
+    Returns (imfs [E, max nmode, N], nsift [E], nmode [E]) as numpy arrays.
+    Defaults to the numba kernel's stop rules (rules='numba')."""
+    x = np.asarray(x, dtype=np.float64)
+    if x.ndim == 1:
+        if E != 1:
+            raise ValueError(
+                "1-D input x is a single trial (E=1). For E>1 pass a 2-D "
+                "(E, N) array of perturbed signals, e.g. x[None,:] + noises.")
+        x = x[None, :]
+    E, N = x.shape
+    if N < 3:
+        raise ValueError("signal too short")
+    torch = _torch()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    p = make_params(noise_mode=L.EEMD_NOISE_PREPERTURBED, tau=tau, max_sifts=max_sifts,
+                    max_imf=int(max_imf), min_extrema=min_extrema, end=end, rules=rules,
+                    exact=exact, config=config)
+    xd = torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+    out = torch.zeros((E, int(max_imf), N), dtype=torch.float64, device=dev)
+    nsift = torch.zeros((E,), dtype=torch.int32, device=dev)
+    nmode = torch.zeros((E,), dtype=torch.int32, device=dev)
+    ws = torch.empty((L.workspace_size(p, [N], E, True),), dtype=torch.uint8, device=dev)
+    L.run(p, xd, [N], 0, E, ws, imfs=out, nsift=nsift, nmode=nmode)
+    nm = nmode.cpu().numpy()
+    maxm = int(nm.max()) if nm.size else 0
+    return out[:, :maxm].cpu().numpy(), nsift.cpu().numpy(), nm
+
+
+# =====================================================================
+# Reference signal (emd_par.py:307-318)
+# =====================================================================
+def make_reference_sweep(FS=44100, T=10.0, F1=20.0, F2=20000.0, noise_level=0.01, seed=0):
+    """10-octave log sine sweep F1..F2 over T seconds at FS, plus white noise at
+    noise_level (fraction of the unit peak).  Returns (x, t)."""
+    N = int(FS * T)
+    t = np.arange(N) / FS
+    ratio = F2 / F1
+    phi = 2 * np.pi * F1 * T * (ratio ** (t / T) - 1.0) / np.log(ratio)
+    x = np.sin(phi)
+    rng = np.random.default_rng(seed)
+    x = x + noise_level * rng.standard_normal(N)
+    return x, t

@@ -1,0 +1,108 @@
+"""The C-ABI library loads and exports what include/eemd_b200.h declares.
+
+Only host-side entry points are called here (no GPU work): version, strerror,
+default parameters, workspace sizing and argument validation.
+"""
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+from eemd4cuda_b200 import _lib as L
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "eemd_b200.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(eemd_[a-z_]+)\s*\(", text)))
+
+
+def test_header_lists_the_bound_symbols():
+    assert declared_functions() == sorted(L.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(str(L.lib_path()))
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+
+
+def test_checked_build_exports_too():
+    p = L.LIB_DIR / "libeemd_b200_checked.so"
+    lib = ctypes.CDLL(str(p))
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+
+
+def test_version_and_strerror():
+    lib = L.load()
+    assert lib.eemd_version() == L.ABI_VERSION
+    assert L.strerror(0) == "ok"
+    assert "workspace" in L.strerror(L.EEMD_E_NOMEM)
+    assert "watchdog" in L.strerror(L.EEMD_E_TIMEOUT)
+
+
+def test_struct_layout():
+    assert ctypes.sizeof(L.EemdParams) == 80
+    assert L.EemdParams.watchdog.offset == 72
+    p = L.default_params()
+    assert p.dtype == L.EEMD_F64 and p.max_sifts == 50 and p.min_extrema == 4
+    assert abs(p.tau - 0.25) < 1e-15 and p.rules == L.EEMD_RULES_REF
+
+
+def test_workspace_size_scales():
+    p = L.default_params()
+    p.max_imf = 8
+    a = L.workspace_size(p, [48000], 1, False)
+    b = L.workspace_size(p, [48000], 10, False)
+    c = L.workspace_size(p, [48000], 10, True)
+    assert 9 * a < b < 11 * a + 4096
+    assert c < b  # external IMF buffer is not carved from the workspace
+    p.dtype = L.EEMD_F32
+    assert L.workspace_size(p, [48000], 10, False) < b
+
+
+@pytest.mark.parametrize("field,value", [("dtype", 7), ("max_sifts", 0), ("max_imf", 0),
+                                         ("end_mode", 5), ("rules", 9), ("tile", 300),
+                                         ("noise_mode", 11)])
+def test_bad_params_rejected(field, value):
+    p = L.default_params()
+    setattr(p, field, value)
+    with pytest.raises(ValueError):
+        L.workspace_size(p, [1000], 1, False)
+
+
+def test_exact_float32_not_supported():
+    p = L.default_params()
+    p.dtype = L.EEMD_F32
+    p.exact = 1
+    with pytest.raises(L.EngineError) as ei:
+        L.workspace_size(p, [1000], 1, False)
+    assert ei.value.status == L.EEMD_E_NOTSUP
+
+
+def test_short_signal_rejected():
+    p = L.default_params()
+    with pytest.raises(ValueError):
+        L.workspace_size(p, [2], 1, False)
+
+
+def test_run_rejects_small_workspace_without_touching_the_device():
+    """eemd_run validates sizes on the host before any CUDA call."""
+    lib = L.load()
+    p = L.default_params()
+    la = L.lengths_array([1000])
+    need = L.workspace_size(p, [1000], 1, False)
+    rc = lib.eemd_run(ctypes.byref(p), ctypes.c_void_p(16), la, 1, 0, 1, None, None, None, None,
+                      None, None, None, None, None, None, ctypes.c_void_p(16), need - 1, None)
+    assert rc == L.EEMD_E_NOMEM
+    rc = lib.eemd_run(ctypes.byref(p), None, la, 1, 0, 1, None, None, None, None,
+                      None, None, None, None, None, None, ctypes.c_void_p(16), need, None)
+    assert rc == L.EEMD_E_BADARG
+    p.noise_mode = L.EEMD_NOISE_INJECTED
+    rc = lib.eemd_run(ctypes.byref(p), ctypes.c_void_p(16), la, 1, 0, 1, None, None, None, None,
+                      None, None, None, None, None, None, ctypes.c_void_p(16), need, None)
+    assert rc == L.EEMD_E_BADARG
