@@ -125,60 +125,73 @@ def run_reference(args):
 # clocks
 # ---------------------------------------------------------------------------
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event reasons sampled every 10 ms during the timed
+    region (NVML; nvidia-smi at 200 ms when NVML is unavailable)."""
+
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4}
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
-        self.proc = None
-        self.lines: list[str] = []
+        self.samples: list[tuple[float, float, int]] = []
+        self.stop_evt = threading.Event()
         self.thread = None
+        self.nvml = None
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except (OSError, FileNotFoundError):
-            self.proc = None
-            return
-        self.thread = threading.Thread(target=self._read, daemon=True)
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.nvml = (nv, h)
+        except Exception:
+            self.nvml = None
+        self.thread = threading.Thread(target=self._run, daemon=True)
         self.thread.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        if self.nvml is not None:
+            nv, h = self.nvml
+            getr = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            while not self.stop_evt.is_set():
+                try:
+                    self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                         float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)),
+                                         int(getr(h))))
+                except Exception:
+                    break
+                self.stop_evt.wait(0.01)
+            return
+        try:
+            proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", "--query-gpu=clocks.sm,clocks.max.sm,"
+                 "clocks_event_reasons.active", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            return
+        while not self.stop_evt.is_set():
+            line = proc.stdout.readline()
+            if not line:
+                break
+            parts = [q.strip() for q in line.split(",")]
+            try:
+                self.samples.append((float(parts[0]), float(parts[1]), int(parts[2], 16)))
+            except (ValueError, IndexError):
+                pass
+        proc.terminate()
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
+        self.stop_evt.set()
         if self.thread:
-            self.thread.join(timeout=2)
-        sm, smax, reasons = [], [], set()
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for ln in self.lines:
-            parts = [q.strip() for q in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-            except ValueError:
-                continue
-            for nm, val in zip(names, parts[5:9]):
-                if val.lower().startswith("active"):
-                    reasons.add(nm)
-        if not sm:
+            self.thread.join(timeout=5)
+        if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        reasons = sorted(k for k, bit in self.REASONS.items()
+                         if any(r & bit for _, _, r in self.samples))
+        return {"sm_mhz": statistics.median(s for s, _, _ in self.samples),
+                "sm_max_mhz": max(m for _, m, _ in self.samples), "reasons": reasons,
+                "samples": len(self.samples), "source": "nvml" if self.nvml else "nvidia-smi"}
 
 
 # ---------------------------------------------------------------------------
@@ -195,13 +208,15 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
-def eval_algorithmic_bytes(klog: np.ndarray, nmode: np.ndarray, bytes_el: int) -> float:
-    """Algorithmic bytes of all k_eval launches of one run, from the per-sift knot log.
+def emd_algorithmic_bytes(klog: np.ndarray, nmode: np.ndarray, bytes_el: int) -> float:
+    """Algorithmic bytes of one k_emd launch, from the per-sift knot log.
 
-    Per sift of one trial: read h and write h (2*N*b), read the sift's knots and
-    second derivatives (P*(4+b+8)), write the next knots (P'*(4+b)); the last sift
-    of an IMF also reads and writes the residual (2*N*b).  Per trial once: read x
-    and write the residual (2*N*b) plus the first knots."""
+    Per trial: read x and write the residual (2*N*b) and the first knot list
+    (P0*(4+b)).  Per sift with P = maxima+minima knots: the solve reads the knots
+    (P*(4+b)) and writes the second derivatives (8*P); the sweep reads and writes
+    h (2*N*b), reads knots and second derivatives (P*(4+b+8)) and writes the
+    next knot list (P'*(4+b)).  The sift that closes an IMF also reads and
+    writes the residual (2*N*b)."""
     total = 0.0
     kb = 4 + bytes_el
     for e in range(klog.shape[0]):
@@ -211,16 +226,16 @@ def eval_algorithmic_bytes(klog: np.ndarray, nmode: np.ndarray, bytes_el: int) -
                 a, b = klog[e, m, k]
                 if a < 0:
                     break
-                seq.append((m, k, int(a) + int(b)))
-        total += 2 * N * bytes_el  # init: x in, residual out
+                seq.append((m, int(a) + int(b)))
+        total += 2 * N * bytes_el
         if seq:
-            total += seq[0][2] * kb
-        for i, (m, k, P) in enumerate(seq):
-            Pn = seq[i + 1][2] if i + 1 < len(seq) else P
-            total += 2 * N * bytes_el + P * (kb + 8) + Pn * kb
-            last = (i + 1 == len(seq)) or (seq[i + 1][0] != m)
-            if last:
-                total += 2 * N * bytes_el
+            total += seq[0][1] * kb
+        for i, (m, P) in enumerate(seq):
+            Pn = seq[i + 1][1] if i + 1 < len(seq) else P
+            total += P * kb + 8 * P                      # solve
+            total += 2 * N * bytes_el + P * (kb + 8) + Pn * kb   # sweep
+            if i + 1 == len(seq) or seq[i + 1][0] != m:
+                total += 2 * N * bytes_el                # residual update at the IMF close
     return total
 
 
@@ -303,12 +318,12 @@ def run_ours(args):
     torch.cuda.synchronize()
     kt = times.as_dict()
     launches_per_step = sum(v["launches"] for v in kt.values()) + 1  # + k_finalize
-    ev = kt["eval"]
-    eval_bytes = eval_algorithmic_bytes(klog.cpu().numpy(), nmode.cpu().numpy(), 4)
-    eval_gbs = eval_bytes / (ev["ms"] / 1e3) / 1e9 if ev["ms"] > 0 else 0.0
+    ev = kt["emd"]
+    emd_bytes = emd_algorithmic_bytes(klog.cpu().numpy(), nmode.cpu().numpy(), 4)
+    emd_gbs = emd_bytes / (ev["ms"] / 1e3) / 1e9 if ev["ms"] > 0 else 0.0
     peak, peak_kind = measured_peak_hbm()
     traffic = None
-    tf = ROOT / "profiles" / "eval_traffic.json"
+    tf = ROOT / "profiles" / "emd_traffic.json"
     if tf.exists():
         try:
             traffic = json.loads(tf.read_text()).get("bytes_per_launch")
@@ -358,11 +373,11 @@ def run_ours(args):
                 "h2d_bytes_per_step": N * 4,
                 "d2h_bytes_per_step": n_modes_e2e * N * 8 + N * 8 + 3 * E * 4},
         "gpu_launches": launches_per_step * args.steps,
-        "roofline": {"bound": "hbm", "kernel": "k_eval", "achieved": round(eval_gbs, 2),
+        "roofline": {"bound": "hbm", "kernel": "k_emd", "achieved": round(emd_gbs, 2),
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": round(eval_gbs / peak, 4),
+                     "frac": round(emd_gbs / peak, 4),
                      "traffic": traffic, "algorithmic_bytes_per_launch":
-                         round(eval_bytes / max(ev["launches"], 1)),
+                         round(emd_bytes / max(ev["launches"], 1)),
                      "avg_launch_ms": round(ev["ms"] / max(ev["launches"], 1), 5)},
         "kernel_split_ms": {k: round(v["ms"], 4) for k, v in kt.items()},
         "kernel_launches": {k: v["launches"] for k, v in kt.items()},

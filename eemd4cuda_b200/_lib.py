@@ -37,7 +37,7 @@ ABI_VERSION = 1
 EXPORTS = ("eemd_default_params", "eemd_version", "eemd_strerror",
            "eemd_workspace_size", "eemd_run", "eemd_run_traced", "eemd_finalize")
 
-KERNEL_KINDS = ("sigma", "init", "plan", "solve", "eval", "reduce", "outputs", "unused")
+KERNEL_KINDS = ("sigma", "emd", "reduce", "outputs", "k4", "k5", "k6", "k7")
 
 
 class EemdParams(ctypes.Structure):
@@ -69,7 +69,7 @@ class KernelTimes(ctypes.Structure):
 
     def as_dict(self) -> dict:
         return {k: {"ms": float(self.ms[i]), "launches": int(self.launches[i])}
-                for i, k in enumerate(KERNEL_KINDS) if k != "unused"}
+                for i, k in enumerate(KERNEL_KINDS) if not k.startswith("k")}
 
 
 class EngineError(RuntimeError):

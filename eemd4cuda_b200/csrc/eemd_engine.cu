@@ -11,16 +11,24 @@
 //   emd_par.py:198-254  ensemble noise and per-mode masked mean
 //
 // Numerics.  exact=1 reproduces the reference's float64 operation order
-// (separately rounded products, IEEE divisions; the file is compiled with
-// --fmad=false so the compiler never contracts a*b+c).  exact=0 uses explicit
-// fma() and one reciprocal per row / interval.
+// (separately rounded products, IEEE divisions, serial-Thomas recurrences;
+// the file is compiled with --fmad=false so the compiler never contracts
+// a*b+c).  exact=0 uses explicit fma(), a Newton-refined reciprocal per row,
+// a twisted (two-sided) seam-window factorisation held in registers, and the
+// monomial form of each spline interval.
 #include "../../include/eemd_b200.h"
 #include "eemd_internal.cuh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
+#include <climits>
 #include <cstdio>
 #include <cstring>
+#include <numeric>
 #include <vector>
+
+namespace cg = cooperative_groups;
 
 namespace eemd {
 
@@ -35,43 +43,18 @@ template <typename T>
 __device__ __forceinline__ double ldv(const void* p, int64_t i) {
     return (double)(static_cast<const T*>(p)[i]);
 }
-template <typename T>
-__device__ __forceinline__ void stv(void* p, int64_t i, double v) {
-    static_cast<T*>(p)[i] = (T)v;
-}
+
 // value rounded to the storage type, held in double
 template <typename T>
 __device__ __forceinline__ double rnd(double v) { return (double)(T)v; }
 
-__device__ __forceinline__ unsigned long long lb_pack(uint64_t flag, uint32_t a, uint32_t b) {
-    return (flag << 62) | ((uint64_t)(a & 0x7fffffffu) << 31) | (uint64_t)(b & 0x7fffffffu);
-}
-__device__ __forceinline__ uint32_t lb_max(unsigned long long v) { return (uint32_t)((v >> 31) & 0x7fffffffu); }
-__device__ __forceinline__ uint32_t lb_min(unsigned long long v) { return (uint32_t)(v & 0x7fffffffu); }
-__device__ __forceinline__ uint32_t lb_flag(unsigned long long v) { return (uint32_t)(v >> 62); }
-
-// largest pos in [0, count) with pref[pos] <= key (pref non-decreasing, pref[0] = 0)
-__device__ __forceinline__ int find_item(const int32_t* pref, int count, int key) {
-    int lo = 0, hi = count;  // invariant pref[lo] <= key < pref[hi] (pref[count] = total)
-    while (hi - lo > 1) {
-        int mid = (lo + hi) >> 1;
-        if (pref[mid] <= key) lo = mid; else hi = mid;
-    }
-    return lo;
-}
-
-// Knot i2 of the envelope in "mirror space" (emd_ref.py:92-96): with mir=1 the
-// list is [2t0-t1, t0..t_{P-1}, 2t_{P-1}-t_{P-2}] with values [y1, y.., y_{P-2}].
-template <typename T>
-__device__ __forceinline__ void knot2(const int32_t* kt, const T* ky, int P, int mir, int i2,
-                                      int& t, double& y) {
-    if (mir) {
-        if (i2 == 0) { t = 2 * kt[0] - kt[1]; y = (double)ky[1]; return; }
-        if (i2 == P + 1) { t = 2 * kt[P - 1] - kt[P - 2]; y = (double)ky[P - 2]; return; }
-        i2 -= 1;
-    }
-    t = kt[i2];
-    y = (double)ky[i2];
+// 1/x: hardware approximation refined by one Newton step on f(y) = 1/y - x,
+// y <- y + y(1 - xy); relative error about 2^-50 or better.
+__device__ __forceinline__ double fast_rcp(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double e = fma(-x, y, 1.0);
+    return fma(y, e, y);
 }
 
 // emd_ref.py:67-75 (and emd_gpu.py:96-100), reference operation order
@@ -83,16 +66,6 @@ __device__ __forceinline__ double spline_exact(double t, double tl, double tr, d
     double a3 = a * a * a;
     double b3 = b * b * b;
     return (a * yl + b * yr) + (((a3 - a) * Ml + (b3 - b) * Mr) * (h * h)) / 6.0;
-}
-
-// same cubic with the interval's reciprocal and h^2/6 precomputed
-__device__ __forceinline__ double spline_fast(double t, double tl, double tr, double yl, double yr,
-                                              double Ml, double Mr, double inv_h, double h26) {
-    double a = (tr - t) * inv_h;
-    double b = (t - tl) * inv_h;
-    double ca = a * fma(a, a, -1.0);
-    double cb = b * fma(b, b, -1.0);
-    return fma(a, yl, b * yr) + fma(ca, Ml, cb * Mr) * h26;
 }
 
 // ---------------------------------------------------------------------------
@@ -156,21 +129,22 @@ __device__ __forceinline__ double2 block_sum2(double2 v, double2* sh) {
 // k_sigma: per-signal eps*std(x) (population std, emd_par.py:117, 225)
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(1024) k_sigma(Ctx C, double eps, double* sigma_out) {
+__global__ void __launch_bounds__(1024) k_sigma(const SignalDesc* sdesc, const void* xv, double eps,
+                                                double* sigma_out) {
     __shared__ double2 sh[32];
+    __shared__ double mean_s;
     const int s = blockIdx.x;
-    const SignalDesc d = C.sd[s];
-    const T* x = static_cast<const T*>(C.x) + d.x_off;
+    const SignalDesc d = sdesc[s];
+    const T* x = static_cast<const T*>(xv) + d.x_off;
     double acc = 0.0;
     for (int64_t i = threadIdx.x; i < d.n; i += 1024) acc += (double)x[i];
     double2 r = block_sum2<1024>(make_double2(acc, 0.0), sh);
-    __shared__ double mean_s;
     if (threadIdx.x == 0) mean_s = r.x / (double)d.n;
     __syncthreads();
     const double mean = mean_s;
     acc = 0.0;
     for (int64_t i = threadIdx.x; i < d.n; i += 1024) {
-        double dv = (double)x[i] - mean;
+        const double dv = (double)x[i] - mean;
         acc += dv * dv;
     }
     r = block_sum2<1024>(make_double2(acc, 0.0), sh);
@@ -178,274 +152,336 @@ __global__ void __launch_bounds__(1024) k_sigma(Ctx C, double eps, double* sigma
 }
 
 // ---------------------------------------------------------------------------
-// k_init: task states
+// per-CTA task context (shared memory)
 // ---------------------------------------------------------------------------
-__global__ void k_init(Ctx C) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= C.n_tasks) return;
-    TaskState s;
-    memset(&s, 0, sizeof(s));
-    s.phase = PH_INIT;
-    C.ts[i] = s;
+struct Xchg {              // one CTA's published segment results (DSMEM-visible)
+    double hf[2], hl[2];   // h after the step: first two / last two samples of the segment
+    double rf[2], rl[2];   // residual after the step: same positions
+    double num, den;       // SD partial sums of the segment
+    int cnt[2];            // new knots (maxima, minima) found in the segment
+};
+
+struct TaskSm {
+    int task, n, s0, s1, rank, csize;
+    int phase, imf, sift, kpar, src_resid, imf_from_resid;
+    int nsift_total, nmode, mode_sifts_cur, flags, step, mode;
+    int P[2];                  // current knot totals
+    int pref[2][MAXC + 1];     // current knots before each segment
+    int mir[2], p2[2], tfirst[2], tlast[2];
+    double cval[2];            // constant envelope when P == 1
+    // sweep scalars
+    int left_knot[2];
+    int run_cur[2], run_new[2];
+    double hold_m1, hold_m2, rold_m1, rold_p, hold_p, f_m1, g_m1;
+    double hf0, hf1, rf0, rf1;
+};
+
+struct Smem {
+    double* h;       // [TILE+2] old h (index j+1 = tile sample j; 0 and tl+1 are halos)
+    double* f;       // [TILE+2] new values
+    double* r;       // [TILE+2] residual
+    int* kt;         // [2][cap] knot sample index
+    double* c0;      // [2][cap] exact: knot value;          fast: monomial c0 (= knot value)
+    double* c1;      // [2][cap] exact: second derivative;   fast: monomial c1
+    double* c2;      // [2][cap] fast: monomial c2
+    double* c3;      // [2][cap] fast: monomial c3
+    int* skt;        // solve staging (padded): knot sample index
+    double* ssl;     // solve staging (padded): slope of the interval starting at the knot
+    int cap;
+};
+
+constexpr int RUN_MAX = 4;            // consecutive samples per thread in a tile
+constexpr int NWARP = THREADS / 32;
+
+__host__ __device__ inline int stage_pad(int k) { return k + (k >> 4); }
+
+__host__ __device__ inline size_t smem_bytes(int TILE) {
+    const int cap = (TILE >> 1) + 8;
+    size_t sweep = (size_t)3 * (TILE + 2) * 8 + (size_t)2 * cap * (4 + 4 * 8);
+    size_t solve = (size_t)stage_pad(SOLVE_CAP) * (4 + 8) + 64;
+    return sweep > solve ? sweep : solve;
+}
+
+__device__ __forceinline__ Smem carve(unsigned char* base, int TILE) {
+    Smem m;
+    m.cap = (TILE >> 1) + 8;
+    double* d = reinterpret_cast<double*>(base);
+    m.h = d;
+    m.f = m.h + (TILE + 2);
+    m.r = m.f + (TILE + 2);
+    m.c0 = m.r + (TILE + 2);
+    m.c1 = m.c0 + 2 * m.cap;
+    m.c2 = m.c1 + 2 * m.cap;
+    m.c3 = m.c2 + 2 * m.cap;
+    m.kt = reinterpret_cast<int*>(m.c3 + 2 * m.cap);
+    // solve staging overlays the sweep buffers (used in a different phase)
+    m.ssl = d;
+    m.skt = reinterpret_cast<int*>(d + stage_pad(SOLVE_CAP) + 2);
+    return m;
 }
 
 // ---------------------------------------------------------------------------
-// k_plan: compact the live tasks into the eval list (tiles) and the solve list
-// (window chunks) of this step.  One CTA.
+// segmented knot lists: real knot i lives in segment r = seg_of(i) at
+// position i - pref[r] of that segment's list
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int solve_chunks(const Ctx& C, int P) {
-    int mir = (C.end_mode == EEMD_END_MIRROR && P >= 3) ? 1 : 0;
-    int n = P + 2 * mir - 2;
-    int nwin = n > 0 ? (n + C.B - 1) / C.B : 1;
-    return (nwin + SOLVE_THREADS - 1) / SOLVE_THREADS;
+struct Slot {
+    int32_t* kt;   // slot base
+    void* ky;
+    double* M;
+};
+
+__device__ __forceinline__ int64_t knot_index(const Ctx& C, int par, int env, int seg, int i) {
+    return ((int64_t)((par * 2 + env) * C.csize + seg)) * C.segcap + i;
 }
 
-__global__ void __launch_bounds__(PLAN_THREADS) k_plan(Ctx C) {
-    __shared__ int4 wsum[PLAN_THREADS / 32];
-    __shared__ int4 carry;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    if (tid == 0) carry = make_int4(0, 0, 0, 0);
-    __syncthreads();
-    for (int base = 0; base < C.n_tasks; base += PLAN_THREADS) {
-        const int task = base + tid;
-        int ph = PH_DONE;
-        if (task < C.n_tasks) ph = C.ts[task].phase;
-        int4 v = make_int4(0, 0, 0, 0);  // (eval items, eval tiles, solve items, solve chunks)
-        int c0 = 0, c1 = 0;
-        if (ph != PH_DONE) {
-            v.x = 1;
-            v.y = C.td[task].ntiles;
-            if (ph == PH_SIFT) {
-                const TaskState s = C.ts[task];
-                c0 = solve_chunks(C, s.pmax);
-                c1 = solve_chunks(C, s.pmin);
-                v.z = 2;
-                v.w = c0 + c1;
-            }
-        }
-        // block exclusive scan of v
-        int4 inc = v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int4 t;
-            t.x = __shfl_up_sync(0xffffffffu, inc.x, o);
-            t.y = __shfl_up_sync(0xffffffffu, inc.y, o);
-            t.z = __shfl_up_sync(0xffffffffu, inc.z, o);
-            t.w = __shfl_up_sync(0xffffffffu, inc.w, o);
-            if (lane >= o) { inc.x += t.x; inc.y += t.y; inc.z += t.z; inc.w += t.w; }
-        }
-        if (lane == 31) wsum[wid] = inc;
-        __syncthreads();
-        if (wid == 0) {
-            int4 w = wsum[lane];
-            int4 wi = w;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                int4 t;
-                t.x = __shfl_up_sync(0xffffffffu, wi.x, o);
-                t.y = __shfl_up_sync(0xffffffffu, wi.y, o);
-                t.z = __shfl_up_sync(0xffffffffu, wi.z, o);
-                t.w = __shfl_up_sync(0xffffffffu, wi.w, o);
-                if (lane >= o) { wi.x += t.x; wi.y += t.y; wi.z += t.z; wi.w += t.w; }
-            }
-            wsum[lane] = make_int4(wi.x - w.x, wi.y - w.y, wi.z - w.z, wi.w - w.w);
-        }
-        __syncthreads();
-        const int4 wb = wsum[wid];
-        const int4 cb = carry;
-        int4 ex;
-        ex.x = cb.x + wb.x + inc.x - v.x;
-        ex.y = cb.y + wb.y + inc.y - v.y;
-        ex.z = cb.z + wb.z + inc.z - v.z;
-        ex.w = cb.w + wb.w + inc.w - v.w;
-        if (v.x) {
-            C.el_task[ex.x] = task;
-            C.el_pref[ex.x] = ex.y;
-        }
-        if (v.z) {
-            C.sl_item[ex.z] = task * 2;
-            C.sl_pref[ex.z] = ex.w;
-            C.sl_item[ex.z + 1] = task * 2 + 1;
-            C.sl_pref[ex.z + 1] = ex.w + c0;
-        }
-        __syncthreads();
-        if (tid == PLAN_THREADS - 1) {
-            carry = make_int4(ex.x + v.x, ex.y + v.y, ex.z + v.z, ex.w + v.w);
-        }
-        __syncthreads();
+// segment holding real knot i: largest r with pref[r] <= i
+__device__ __forceinline__ int seg_of(const int* pref, int csize, int i) {
+    int lo = 0, hi = csize;  // pref[lo] <= i < pref[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (pref[mid] <= i) lo = mid; else hi = mid;
     }
-    if (tid == 0) {
-        const int4 c = carry;
-        C.el_pref[c.x] = c.y;
-        C.sl_pref[c.z] = c.w;
-        Header* h = C.hdr;
-        h->n_elist = c.x;
-        h->eval_total = c.y;
-        h->n_slist = c.z;
-        h->solve_total = c.w;
-        h->eval_ticket = 0u;
-        h->solve_ticket = 0u;
-        h->active = c.x;
-        h->step = h->step + 1;
+    return lo;
+}
+
+template <typename T>
+__device__ __forceinline__ void real_knot(const Ctx& C, const Slot& sl, const TaskSm& S, int env, int i,
+                                          int& t, double& y) {
+    const int* pr = S.pref[env];
+    int r = S.rank;  // most lookups fall in the CTA's own segment
+    if (i < pr[r] || i >= pr[r + 1]) r = seg_of(pr, S.csize, i);
+    const int64_t o = knot_index(C, S.kpar, env, r, i - pr[r]);
+    t = __ldcg(sl.kt + o);
+    y = (double)__ldcg(static_cast<const T*>(sl.ky) + o);
+}
+
+// Knot i2 in "mirror space" (emd_ref.py:92-96): with mir=1 the list is
+// [2t0-t1, t0..t_{P-1}, 2t_{P-1}-t_{P-2}] with values [y1, y.., y_{P-2}].
+template <typename T>
+__device__ __forceinline__ void knot2(const Ctx& C, const Slot& sl, const TaskSm& S, int env, int i2,
+                                      int& t, double& y) {
+    const int P = S.P[env];
+    if (S.mir[env]) {
+        if (i2 == 0) {
+            int t0, t1;
+            double y0, y1;
+            real_knot<T>(C, sl, S, env, 0, t0, y0);
+            real_knot<T>(C, sl, S, env, 1, t1, y1);
+            t = 2 * t0 - t1;
+            y = y1;
+            return;
+        }
+        if (i2 == P + 1) {
+            int ta, tb;
+            double ya, yb;
+            real_knot<T>(C, sl, S, env, P - 1, ta, ya);
+            real_knot<T>(C, sl, S, env, P - 2, tb, yb);
+            t = 2 * ta - tb;
+            y = yb;
+            return;
+        }
+        i2 -= 1;
     }
+    real_knot<T>(C, sl, S, env, i2, t, y);
 }
 
 // ---------------------------------------------------------------------------
-// k_solve: decay-seamed block Thomas (emd_gpu_v5_dsbt.py:51-74 window solve,
-// emd_ref.py:31-65 system + Thomas).  One thread per window of B owned rows,
-// halo S rows on each side with the outer couplings dropped; only owned rows
-// are written (the seam error decays as (2-sqrt(3))^S).  The rows are built
-// on the fly from the knots (no materialised d/l/u/r slabs).
+// solve: decay-seamed block Thomas over the cluster
 // ---------------------------------------------------------------------------
-template <typename T, bool EXACT>
-__device__ __forceinline__ void solve_window(const Ctx& C, int task, int env, int chunk, int w) {
-    const TaskDesc d = C.td[task];
-    const TaskState s = C.ts[task];
-    const int P = env ? s.pmin : s.pmax;
-    const int64_t plane = (int64_t)(s.kpar * 2 + env) * C.KC + d.k_off;
-    const int32_t* kt = C.kt + plane;
-    const T* ky = static_cast<const T*>(C.ky) + plane;
-    double* M2 = C.M + (int64_t)env * C.KC + d.k_off;
-    const int mir = (C.end_mode == EEMD_END_MIRROR && P >= 3) ? 1 : 0;
-    const int p2 = P + 2 * mir;
-    const int n = p2 - 2;
+// Row i (mirror space, i = 0..n-1 for M2[i+1]) from staged knots k = i - base:
+//   H0 = t_{i+1}-t_i, H1 = t_{i+2}-t_{i+1}, d = 2(H0+H1), l = H0 (i>=1),
+//   u = H1 (i<=n-2), r = 6(slope_{i+1} - slope_i)          (emd_ref.py:31-48)
+// The sweeps slide along the rows: each row loads one new knot and one slope.
+struct Row {
+    double dg, l, u, r;
+};
+
+__device__ __forceinline__ Row row_of(int ta, int tb, int tc, double sa, double sb, int i, int n) {
+    const double H0 = (double)(tb - ta), H1 = (double)(tc - tb);
+    Row w;
+    w.dg = 2.0 * (H0 + H1);
+    w.l = (i >= 1) ? H0 : 0.0;
+    w.u = (i <= n - 2) ? H1 : 0.0;
+    w.r = 6.0 * (sb - sa);
+    return w;
+}
+
+#define SKT(k) skt[stage_pad(k)]
+#define SSL(k) ssl[stage_pad(k)]
+
+// exact: forward elimination from w0 (outer coupling dropped), back
+// substitution from w1; identical recurrences to serial Thomas (emd_ref.py:50-65)
+__device__ void window_exact(const Ctx& C, const int* skt, const double* ssl, int base, int n, int w,
+                             double* M2, int p2) {
     const int B = C.B, S = C.S;
-    const int nwin = n > 0 ? (n + B - 1) / B : 1;
-    if (w >= nwin) return;
-    if (n <= 0) {
-        for (int i = 0; i < p2; ++i) M2[i] = 0.0;
-        return;
-    }
-    if (p2 > d.kcap) { raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, task); return; }
     const int o0 = w * B;
     const int o1 = min(n, o0 + B) - 1;
     const int w0 = max(0, o0 - S);
     const int w1 = min(n - 1, o1 + S);
-    double2* sc = C.scr + d.scr_off + (int64_t)env * d.scr_env +
-                  (int64_t)chunk * (B + S) * SOLVE_THREADS + threadIdx.x;
-
-    int ta, tb, tc;
-    double ya, yb, yc;
-    knot2<T>(kt, ky, P, mir, w0, ta, ya);
-    knot2<T>(kt, ky, P, mir, w0 + 1, tb, yb);
+    const int64_t gthreads = (int64_t)gridDim.x * blockDim.x;
+    double2* sc = C.scr + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     double cp = 0.0, dp = 0.0;
+    int ta = SKT(w0 - base), tb = SKT(w0 + 1 - base);
+    double sa = SSL(w0 - base);
     for (int i = w0; i <= w1; ++i) {
-        knot2<T>(kt, ky, P, mir, i + 2, tc, yc);
-        const double H0 = (double)(tb - ta);
-        const double H1 = (double)(tc - tb);
-        const double dg = 2.0 * (H0 + H1);
-        const double l = (i >= 1) ? H0 : 0.0;
-        const double u = (i <= n - 2) ? H1 : 0.0;
-        const double r = 6.0 * ((yc - yb) / H1 - (yb - ya) / H0);
-        double c, dv;
-        if (EXACT) {
-            c = (i == w1) ? 0.0 : u / (dg - l * cp);
-            dv = (r - l * dp) / (dg - l * cp);
-        } else {
-            const double inv = 1.0 / fma(-l, cp, dg);
-            c = (i == w1) ? 0.0 : u * inv;
-            dv = fma(-l, dp, r) * inv;
-        }
-        if (i >= o0) sc[(int64_t)(i - o0) * SOLVE_THREADS] = make_double2(c, dv);
+        const int tc = SKT(i + 2 - base);
+        const double sb = SSL(i + 1 - base);
+        const Row rw = row_of(ta, tb, tc, sa, sb, i, n);
+        const double c = (i == w1) ? 0.0 : rw.u / (rw.dg - rw.l * cp);
+        const double dv = (rw.r - rw.l * dp) / (rw.dg - rw.l * cp);
+        if (i >= o0) sc[(int64_t)(i - o0) * gthreads] = make_double2(c, dv);
         cp = c;
         dp = dv;
-        ta = tb; ya = yb;
-        tb = tc; yb = yc;
+        ta = tb;
+        tb = tc;
+        sa = sb;
     }
     double xv = dp;
     if (w1 <= o1) M2[w1 + 1] = xv;
     for (int i = w1 - 1; i >= o0; --i) {
-        const double2 cd = sc[(int64_t)(i - o0) * SOLVE_THREADS];
-        xv = EXACT ? (cd.y - cd.x * xv) : fma(-cd.x, xv, cd.y);
+        const double2 cd = sc[(int64_t)(i - o0) * gthreads];
+        xv = cd.y - cd.x * xv;
         if (i <= o1) M2[i + 1] = xv;
     }
     if (o0 == 0) M2[0] = 0.0;
     if (o1 == n - 1) M2[p2 - 1] = 0.0;
 }
 
+// fast: twisted factorisation of the window.  A left sweep (LU, coupling
+// dropped at w0) keeps its (c, d) for the owned rows in registers; a right
+// sweep (UL, coupling dropped at w1) meets it, and each owned unknown is
+//   x_i = (r_i - l_i d_{i-1} - u_i g_{i+1}) / (dg_i - l_i c_{i-1} - u_i e_{i+1}).
+__device__ void window_fast(const Ctx& C, const int* skt, const double* ssl, int base, int n, int w,
+                            double* M2, int p2) {
+    const int S = C.S;
+    const int o0 = w * FAST_B;
+    const int cnt = min(FAST_B, n - o0);
+    const int o1 = o0 + cnt - 1;
+    const int w0 = max(0, o0 - S);
+    const int w1 = min(n - 1, o1 + S);
+    double fc[FAST_B], fd[FAST_B];
+    double cp = 0.0, dp = 0.0;
+    int ta = SKT(w0 - base), tb = SKT(w0 + 1 - base);
+    double sa = SSL(w0 - base);
+    for (int i = w0; i <= o0 - 2; ++i) {
+        const int tc = SKT(i + 2 - base);
+        const double sb = SSL(i + 1 - base);
+        const Row rw = row_of(ta, tb, tc, sa, sb, i, n);
+        const double inv = fast_rcp(fma(-rw.l, cp, rw.dg));
+        cp = rw.u * inv;
+        dp = fma(-rw.l, dp, rw.r) * inv;
+        ta = tb;
+        tb = tc;
+        sa = sb;
+    }
+    // forward state after rows o0-1 .. o1-1 (row -1 does not exist: zero state)
+#pragma unroll
+    for (int k = 0; k < FAST_B; ++k) {
+        const int i = o0 - 1 + k;
+        if (k < cnt) {
+            if (i >= 0) {
+                const int tc = SKT(i + 2 - base);
+                const double sb = SSL(i + 1 - base);
+                const Row rw = row_of(ta, tb, tc, sa, sb, i, n);
+                const double inv = fast_rcp(fma(-rw.l, cp, rw.dg));
+                cp = rw.u * inv;
+                dp = fma(-rw.l, dp, rw.r) * inv;
+                ta = tb;
+                tb = tc;
+                sa = sb;
+            }
+            fc[k] = cp;
+            fd[k] = dp;
+        }
+    }
+    // right sweep from w1 down to o1+1, then combine over the owned rows
+    double e = 0.0, g = 0.0;
+    int ub = SKT(w1 + 1 - base), uc = SKT(w1 + 2 - base);
+    double vb = SSL(w1 + 1 - base);
+    for (int i = w1; i > o1; --i) {
+        const int ua = SKT(i - base);
+        const double va = SSL(i - base);
+        const Row rw = row_of(ua, ub, uc, va, vb, i, n);
+        const double inv = fast_rcp(fma(-rw.u, e, rw.dg));
+        e = rw.l * inv;
+        g = fma(-rw.u, g, rw.r) * inv;
+        uc = ub;
+        ub = ua;
+        vb = va;
+    }
+#pragma unroll
+    for (int k = FAST_B - 1; k >= 0; --k) {
+        if (k < cnt) {
+            const int i = o0 + k;
+            const int ua = SKT(i - base);
+            const double va = SSL(i - base);
+            const Row rw = row_of(ua, ub, uc, va, vb, i, n);
+            const double num = fma(-rw.u, g, fma(-rw.l, fd[k], rw.r));
+            const double den = fma(-rw.u, e, fma(-rw.l, fc[k], rw.dg));
+            M2[i + 1] = num * fast_rcp(den);
+            const double inv = fast_rcp(fma(-rw.u, e, rw.dg));
+            e = rw.l * inv;
+            g = fma(-rw.u, g, rw.r) * inv;
+            uc = ub;
+            ub = ua;
+            vb = va;
+        }
+    }
+    if (o0 == 0) M2[0] = 0.0;
+    if (o1 == n - 1) M2[p2 - 1] = 0.0;
+}
+
+#undef SKT
+#undef SSL
+
 template <typename T, bool EXACT>
-__global__ void __launch_bounds__(SOLVE_THREADS) k_solve(Ctx C) {
-    __shared__ int sh_ticket, sh_pos;
-    for (;;) {
-        if (threadIdx.x == 0) {
-            const int total = C.hdr->solve_total;
-            const int t = (int)atomicAdd(&C.hdr->solve_ticket, 1u);
-            sh_ticket = t;
-            sh_pos = (t < total) ? find_item(C.sl_pref, C.hdr->n_slist, t) : -1;
+__device__ void solve_task(const Ctx& C, const Slot& sl, TaskSm& S, const Smem& sm) {
+    const int tid = threadIdx.x;
+    for (int env = 0; env < 2; ++env) {
+        const int p2 = S.p2[env];
+        const int n = p2 - 2;
+        double* M2 = sl.M + (int64_t)env * C.kcap;
+        if (n <= 0) {
+            if (S.rank == 0 && tid < p2) M2[tid] = 0.0;
+            continue;
         }
-        __syncthreads();
-        const int ticket = sh_ticket, pos = sh_pos;
-        __syncthreads();
-        if (pos < 0) break;
-        const int item = C.sl_item[pos];
-        const int chunk = ticket - C.sl_pref[pos];
-        solve_window<T, EXACT>(C, item >> 1, item & 1, chunk, chunk * SOLVE_THREADS + threadIdx.x);
+        const int Bw = EXACT ? C.B : FAST_B;
+        const int nwin = (n + Bw - 1) / Bw;
+        const int wa = (int)((int64_t)S.rank * nwin / S.csize);
+        const int wb = (int)((int64_t)(S.rank + 1) * nwin / S.csize);
+        int wpp = (SOLVE_CAP - 2 * C.S - 8) / Bw;
+        wpp = max(1, min(wpp, THREADS));
+        for (int wbase = wa; wbase < wb; wbase += wpp) {
+            const int wend = min(wb, wbase + wpp);
+            const int rlo = max(0, wbase * Bw - C.S);
+            const int rhi = min(n - 1, min(n, wend * Bw) - 1 + C.S);
+            const int kcount = rhi + 3 - rlo;  // knots rlo .. rhi+2
+            __syncthreads();
+            for (int k = tid; k < kcount; k += THREADS) {
+                int ta, tb;
+                double ya, yb;
+                knot2<T>(C, sl, S, env, rlo + k, ta, ya);
+                sm.skt[stage_pad(k)] = ta;
+                if (k + 1 < kcount) {
+                    knot2<T>(C, sl, S, env, rlo + k + 1, tb, yb);
+                    // emd_ref.py:47: (y_{q+1}-y_q)/H_q, the same IEEE division
+                    sm.ssl[stage_pad(k)] = (yb - ya) / (double)(tb - ta);
+                }
+            }
+            __syncthreads();
+            const int w = wbase + tid;
+            if (w < wend) {
+                if (EXACT) window_exact(C, sm.skt, sm.ssl, rlo, n, w, M2, p2);
+                else window_fast(C, sm.skt, sm.ssl, rlo, n, w, M2, p2);
+            }
+        }
     }
+    __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
-// k_eval: the fused per-tile pass
+// sweep: the fused per-segment pass
 // ---------------------------------------------------------------------------
-enum TileMode : int { TM_INIT = 0, TM_SIFT = 1, TM_LAST = 2, TM_TRANS = 3 };
-
-struct TileInfo {
-    int task, tile, mode, n, t0, tl, ntiles, tile_off, is_last, q;
-    int imf, sift, kpar, src_resid, imf_from_resid;
-    int P[2], kb[2], kcnt[2], mir[2], p2[2], lo2[2], hi2[2];
-    int tfirst[2], tlast[2];  // virtual mirror knot positions
-    double cval[2];
-    int excl[2], agg[2];
-};
-
-__device__ __forceinline__ size_t eval_smem_bytes_dev(int TILE) {
-    const int W = TILE >> 5, cap = (TILE >> 1) + 8;
-    return (size_t)3 * (TILE + 2) * 8 + (size_t)2 * cap * 8 * 3 + (size_t)2 * cap * 4 + (size_t)4 * 2 * W * 4;
-}
-
-// knots strictly before sample t (t in the tile, or t0-1 / t0+tl) in mirror space
-__device__ __forceinline__ int count_less(const TileInfo& I, const unsigned* mask, const int* wb,
-                                          const int* skt, int env, int t) {
-    const int j = t - I.t0;
-    int c;
-    if (j < 0) {
-        const int kb = I.kb[env];
-        c = kb;
-        if (kb >= 1) {
-            const int loc = (kb - 1 + I.mir[env]) - I.lo2[env];
-            if (skt[loc] == t) c -= 1;
-        }
-    } else if (j >= I.tl) {
-        c = I.kb[env] + I.kcnt[env];
-    } else {
-        const int w = j >> 5, b = j & 31;
-        c = I.kb[env] + wb[w] + __popc(mask[w] & ((1u << b) - 1u));
-    }
-    if (I.mir[env]) c += (I.tfirst[env] < t ? 1 : 0) + (I.tlast[env] < t ? 1 : 0);
-    return c;
-}
-
-template <bool EXACT>
-__device__ __forceinline__ double env_value(const TileInfo& I, int env, int t, const unsigned* mask,
-                                            const int* wb, const int* skt, const double* sky,
-                                            const double* sM, const double* saux, const Ctx& C) {
-    const int P = I.P[env];
-    if (P < 2) return I.cval[env];
-    int idx2 = count_less(I, mask, wb, skt, env, t) - 1;
-    idx2 = max(0, min(idx2, I.p2[env] - 2));
-    const int loc = idx2 - I.lo2[env];
-#ifdef EEMD_CHECKED
-    if (loc < 0 || loc + 1 > I.hi2[env] - I.lo2[env]) {
-        raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, 1000000 + loc);
-        return 0.0;
-    }
-#endif
-    const double tl = (double)skt[loc], tr = (double)skt[loc + 1];
-    if (EXACT) return spline_exact((double)t, tl, tr, sky[loc], sky[loc + 1], sM[loc], sM[loc + 1]);
-    const double h = tr - tl;
-    return spline_fast((double)t, tl, tr, sky[loc], sky[loc + 1], sM[loc], sM[loc + 1], saux[loc],
-                       h * h * (1.0 / 6.0));
-}
-
 template <typename T>
 __device__ __forceinline__ double trial_input(const Ctx& C, const TaskDesc& d, int64_t t) {
     const double xv = ldv<T>(C.x, d.x_off + t);
@@ -457,450 +493,603 @@ __device__ __forceinline__ double trial_input(const Ctx& C, const TaskDesc& d, i
     }
 }
 
-// IMF-level decision for the IMF about to start (emd_ref.py:120-127; emd_gpu.py:155-168)
-__device__ __forceinline__ void imf_level(const Ctx& C, TaskState& s, int cmax, int cmin) {
-    bool stop = (cmax + cmin < C.min_extrema);
-    if (C.rules == EEMD_RULES_NUMBA) stop = stop || cmax < 2 || cmin < 2;
-    if (stop) { s.phase = PH_DONE; return; }
-    if (s.imf >= C.max_imf) { s.phase = PH_DONE; s.flags |= 1; return; }
-    s.mode_sifts_cur = 0;
-    if (C.rules == EEMD_RULES_REF && (cmax < 1 || cmin < 1)) {
-        // emd_ref.py:132-133: the sift loop breaks before its first sift; the IMF is the residual
-        s.phase = PH_TRANS;
-        s.imf_from_resid = 1;
-        return;
+// Block-wide exclusive scan of two per-thread counts (one __syncthreads).
+// wtot: shared [2*NWARP], not reused before the next __syncthreads.
+__device__ __forceinline__ void block_scan2(int a, int b, int& ea, int& eb, int& ta, int& tb, int* wtot) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int ia = a, ib = b;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int xa = __shfl_up_sync(0xffffffffu, ia, o);
+        const int xb = __shfl_up_sync(0xffffffffu, ib, o);
+        if (lane >= o) { ia += xa; ib += xb; }
     }
-    s.phase = PH_SIFT;
-    s.sift = 0;
-    s.src_resid = 1;
-    s.imf_from_resid = 0;
-    s.kpar ^= 1;
-    s.pmax = cmax;
-    s.pmin = cmin;
+    if (lane == 31) { wtot[wid] = ia; wtot[NWARP + wid] = ib; }
+    __syncthreads();
+    int ba = 0, bb = 0;
+    ta = 0;
+    tb = 0;
+#pragma unroll
+    for (int w = 0; w < NWARP; ++w) {
+        const int va = wtot[w], vb = wtot[NWARP + w];
+        if (w < wid) { ba += va; bb += vb; }
+        ta += va;
+        tb += vb;
+    }
+    ea = ba + ia - a;
+    eb = bb + ib - b;
 }
 
-__device__ __forceinline__ void close_imf(const Ctx& C, TaskState& s, int task) {
-    if (C.mode_sifts) C.mode_sifts[(int64_t)task * C.max_imf + s.imf] = s.mode_sifts_cur;
-    s.nmode = s.imf + 1;
-    s.imf += 1;
-    s.mode_sifts_cur = 0;
+// Envelope value at t from the staged intervals; `cless` = knots strictly
+// before t in mirror space (emd_ref.py:70 searchsorted - 1, clipped).
+template <bool EXACT>
+__device__ __forceinline__ double env_at(const Smem& sm, int env, int cless, int t, int lo2, int p2) {
+    int idx2 = max(0, min(cless - 1, p2 - 2));
+    const int k = env * sm.cap + (idx2 - lo2);
+    if (EXACT) {
+        return spline_exact((double)t, (double)sm.kt[k], (double)sm.kt[k + 1], sm.c0[k], sm.c0[k + 1],
+                            sm.c1[k], sm.c1[k + 1]);
+    }
+    const double s = (double)(t - sm.kt[k]);
+    return fma(s, fma(s, fma(s, sm.c3[k], sm.c2[k]), sm.c1[k]), sm.c0[k]);
 }
 
-__device__ __forceinline__ void log_sift(const Ctx& C, int task, const TaskState& s) {
-    if (C.knot_log) {
-        int32_t* p = C.knot_log + (((int64_t)task * C.max_imf + s.imf) * C.max_sifts + s.sift) * 2;
-        p[0] = s.pmax;
-        p[1] = s.pmin;
-    }
+__device__ __forceinline__ int mirror_adj(const TaskSm& S, int env, int t) {
+    return S.mir[env] ? (S.tfirst[env] < t ? 1 : 0) + (S.tlast[env] < t ? 1 : 0) : 0;
 }
 
 template <typename T, bool EXACT>
-__global__ void __launch_bounds__(EVAL_THREADS) k_eval(Ctx C) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int TILE = C.tile;
-    const int W = TILE >> 5;
-    const int cap = (TILE >> 1) + 8;
-    double* s_h = reinterpret_cast<double*>(smem_raw);  // old h      [TILE+2]
-    double* s_f = s_h + (TILE + 2);                      // new values [TILE+2]
-    double* s_r = s_f + (TILE + 2);                      // residual   [TILE+2]
-    double* s_ky = s_r + (TILE + 2);                     // [2][cap]
-    double* s_M = s_ky + 2 * cap;                        // [2][cap]
-    double* s_aux = s_M + 2 * cap;                       // [2][cap] 1/h of interval
-    int* s_kt = reinterpret_cast<int*>(s_aux + 2 * cap); // [2][cap]
-    unsigned* s_mask = reinterpret_cast<unsigned*>(s_kt + 2 * cap);  // [2][W]
-    int* s_wb = reinterpret_cast<int*>(s_mask + 2 * W);               // [2][W]
-    unsigned* s_nm = reinterpret_cast<unsigned*>(s_wb + 2 * W);       // [2][W]
-    int* s_nb = reinterpret_cast<int*>(s_nm + 2 * W);                 // [2][W]
+__device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, const Smem& sm,
+                      cg::cluster_group& cl) {
+    __shared__ double2 s_red[NWARP];
+    __shared__ int s_w1[2 * NWARP], s_w2[2 * NWARP];
+    const int tid = threadIdx.x;
+    const int TILE = C.tile, run = TILE / THREADS, cap = sm.cap;
+    const int mode = S.mode, n = S.n, s0 = S.s0, s1 = S.s1, rank = S.rank;
+    const bool sifting = (mode == TM_SIFT || mode == TM_LAST);
+    const bool uses_r = (mode == TM_LAST || mode == TM_TRANS);
+    const int q = S.step & 1;
+    const TaskDesc d = C.td[S.task];
+    T* resid = static_cast<T*>(C.resid) + d.s_off;
+    T* imf_m = static_cast<T*>(C.imfs) + d.imf_off + (int64_t)min(S.imf, C.max_imf - 1) * n;
+    const T* src = (sifting && S.src_resid) ? resid : imf_m;
+    const int np = S.kpar ^ 1;
+    double num = 0.0, den = 0.0;
 
-    __shared__ TileInfo I;
-    __shared__ double2 s_red[EVAL_THREADS / 32];
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-
-    for (;;) {
-        // ---------------- 0. claim a tile ----------------
-        if (tid == 0) {
-            const int total = C.hdr->eval_total;
-            const int ticket = (int)atomicAdd(&C.hdr->eval_ticket, 1u);
-            if (ticket >= total) {
-                I.task = -1;
-            } else {
-                const int pos = find_item(C.el_pref, C.hdr->n_elist, ticket);
-                const int task = C.el_task[pos];
-                const TaskDesc d = C.td[task];
-                const TaskState s = C.ts[task];
-                I.task = task;
-                I.tile = ticket - C.el_pref[pos];
-                I.n = d.n;
-                I.t0 = I.tile * TILE;
-                I.tl = min(TILE, d.n - I.t0);
-                I.ntiles = d.ntiles;
-                I.tile_off = d.tile_off;
-                I.q = C.hdr->step & 1;
-                I.imf = s.imf;
-                I.sift = s.sift;
-                I.kpar = s.kpar;
-                I.src_resid = s.src_resid;
-                I.imf_from_resid = s.imf_from_resid;
-                I.P[0] = s.pmax;
-                I.P[1] = s.pmin;
-                if (s.phase == PH_INIT) I.mode = TM_INIT;
-                else if (s.phase == PH_TRANS) I.mode = TM_TRANS;
-                else I.mode = (s.sift + 1 >= C.max_sifts) ? TM_LAST : TM_SIFT;
+    if (tid == 0) {
+        S.run_cur[0] = S.run_cur[1] = 0;
+        S.run_new[0] = S.run_new[1] = 0;
+        S.hold_m1 = S.hold_m2 = S.rold_m1 = S.hold_p = S.rold_p = 0.0;
+        if (mode != TM_INIT) {
+            // neighbours' edge samples from their previous step (distributed shared memory)
+            if (s0 > 0) {
+                const Xchg* xl = cl.map_shared_rank(&X[q ^ 1], rank - 1);
+                S.hold_m1 = S.src_resid ? xl->rl[1] : xl->hl[1];
+                S.hold_m2 = S.src_resid ? xl->rl[0] : xl->hl[0];
+                S.rold_m1 = xl->rl[1];
             }
+            if (s1 < n) {
+                const Xchg* xr = cl.map_shared_rank(&X[q ^ 1], rank + 1);
+                S.hold_p = S.src_resid ? xr->rf[0] : xr->hf[0];
+                S.rold_p = xr->rf[0];
+            }
+        }
+    }
+    __syncthreads();
+
+    for (int t0 = s0; t0 < s1; t0 += TILE) {
+        const int tl = min(TILE, s1 - t0);
+        const bool first = (t0 == s0), last = (t0 + tl == s1);
+        const int j0 = tid * run;
+        // ---------------- (a) loads ----------------
+        double hv[RUN_MAX], rv[RUN_MAX], fv[RUN_MAX], gv[RUN_MAX];
+#pragma unroll
+        for (int i = 0; i < RUN_MAX; ++i) {
+            hv[i] = rv[i] = fv[i] = gv[i] = 0.0;
+            const int j = j0 + i;
+            if (i < run && j < tl) {
+                if (sifting) { hv[i] = (double)src[t0 + j]; sm.h[1 + j] = hv[i]; }
+                if (uses_r) { rv[i] = (double)resid[t0 + j]; sm.r[1 + j] = rv[i]; }
+            }
+        }
+        if (tid == 0) {
+            if (sifting) {
+                sm.h[0] = S.hold_m1;
+                sm.h[tl + 1] = (t0 + tl < n) ? (last ? S.hold_p : (double)src[t0 + tl]) : 0.0;
+            }
+            if (uses_r) {
+                sm.r[0] = first ? S.rold_m1 : S.g_m1;
+                sm.r[tl + 1] = (t0 + tl < n) ? (last ? S.rold_p : (double)resid[t0 + tl]) : 0.0;
+            }
+            if (!first) sm.f[0] = S.f_m1;
         }
         __syncthreads();
-        if (I.task < 0) break;
 
-        const int task = I.task, tile = I.tile, n = I.n, t0 = I.t0, tl = I.tl, mode = I.mode;
-        const TaskDesc d = C.td[task];
-        const int64_t gt = (int64_t)d.tile_off + tile;
-        const bool sifting = (mode == TM_SIFT || mode == TM_LAST);
-        T* resid = static_cast<T*>(C.resid) + d.s_off;
-        T* imf_m = static_cast<T*>(C.imfs) + d.imf_off + (int64_t)min(I.imf, C.max_imf - 1) * n;
-
-        // ---------------- 1. load the tile ----------------
+        // ---------------- (b) current knots: strict extrema of h in the run ----------------
+        unsigned kmx = 0u, kmn = 0u;
+        int kb[2] = {0, 0}, kc[2] = {0, 0}, lo2[2] = {0, 0}, hi2[2] = {-1, -1}, cl0[2] = {0, 0};
         if (sifting) {
-            const T* src = I.src_resid ? resid : imf_m;
-            for (int j = tid; j < tl; j += EVAL_THREADS) s_h[1 + j] = (double)src[t0 + j];
-            if (tid == 0 && t0 > 0) {
-                s_h[0] = I.src_resid ? C.redge[(int64_t)(I.imf & 1) * C.TT + gt - 1].y
-                                     : C.hedge[(int64_t)(I.sift & 1) * C.TT + gt - 1].y;
-            }
-            if (tid == 1 && t0 + tl < n) {
-                s_h[tl + 1] = I.src_resid ? C.redge[(int64_t)(I.imf & 1) * C.TT + gt + 1].x
-                                          : C.hedge[(int64_t)(I.sift & 1) * C.TT + gt + 1].x;
-            }
-        }
-        if (mode == TM_LAST || mode == TM_TRANS) {
-            for (int j = tid; j < tl; j += EVAL_THREADS) s_r[1 + j] = (double)resid[t0 + j];
-            if (tid == 0 && t0 > 0) s_r[0] = C.redge[(int64_t)(I.imf & 1) * C.TT + gt - 1].y;
-            if (tid == 1 && t0 + tl < n) s_r[tl + 1] = C.redge[(int64_t)(I.imf & 1) * C.TT + gt + 1].x;
-        }
-
-        // ---------------- 2. stage the current knots ----------------
-        if (sifting) {
-            if (tid < 2) {
-                const int env = tid;
-                const int P = I.P[env];
-                const int64_t plane = (int64_t)(I.kpar * 2 + env) * C.KC + d.k_off;
-                const int32_t* kt = C.kt + plane;
-                const T* ky = static_cast<const T*>(C.ky) + plane;
-                const int2 tp = C.tpref[(int64_t)I.kpar * C.TT + gt];
-                const int kb = env ? tp.y : tp.x;
-                int kend = P;
-                if (tile + 1 < I.ntiles) {
-                    const int2 tn = C.tpref[(int64_t)I.kpar * C.TT + gt + 1];
-                    kend = env ? tn.y : tn.x;
-                }
-                const int mir = (C.end_mode == EEMD_END_MIRROR && P >= 3) ? 1 : 0;
-                I.kb[env] = kb;
-                I.kcnt[env] = kend - kb;
-                I.mir[env] = mir;
-                I.p2[env] = P + 2 * mir;
-                I.cval[env] = (P == 1) ? (double)ky[0] : 0.0;
-                if (P >= 2) {
-                    I.lo2[env] = max(0, mir + kb - 2);
-                    I.hi2[env] = min(P + 2 * mir - 1, mir + kb + (kend - kb) + 1);
-                } else {
-                    I.lo2[env] = 0;
-                    I.hi2[env] = -1;
-                }
-                if (mir) {
-                    I.tfirst[env] = 2 * kt[0] - kt[1];
-                    I.tlast[env] = 2 * kt[P - 1] - kt[P - 2];
-                } else {
-                    I.tfirst[env] = 0;
-                    I.tlast[env] = 0;
-                }
-                if (I.hi2[env] - I.lo2[env] + 1 > cap || I.kcnt[env] < 0 || I.kcnt[env] > (TILE >> 1) + 1) {
-                    raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, task);
-                    I.hi2[env] = I.lo2[env] - 1;
-                    I.kcnt[env] = 0;
+#pragma unroll
+            for (int i = 0; i < RUN_MAX; ++i) {
+                const int j = j0 + i, t = t0 + j;
+                if (i < run && j < tl && t >= 1 && t <= n - 2) {
+                    const double a = sm.h[j], c = sm.h[j + 2], v = hv[i];
+                    if (v > a && v > c) kmx |= 1u << i;
+                    if (v < a && v < c) kmn |= 1u << i;
                 }
             }
-            for (int w = tid; w < 2 * W; w += EVAL_THREADS) s_mask[w] = 0u;
-            __syncthreads();
+            int ex, en, tx, tn;
+            block_scan2(__popc(kmx), __popc(kmn), ex, en, tx, tn, s_w1);
+            kc[0] = tx;
+            kc[1] = tn;
 #pragma unroll
             for (int env = 0; env < 2; ++env) {
-                const int P = I.P[env];
-                const int64_t plane = (int64_t)(I.kpar * 2 + env) * C.KC + d.k_off;
-                const int32_t* kt = C.kt + plane;
-                const T* ky = static_cast<const T*>(C.ky) + plane;
-                const double* M2 = C.M + (int64_t)env * C.KC + d.k_off;
-                const int lo2 = I.lo2[env], cnt = I.hi2[env] - lo2 + 1;
-                for (int k = tid; k < cnt; k += EVAL_THREADS) {
-                    int tt;
-                    double yy;
-                    knot2<T>(kt, ky, P, I.mir[env], lo2 + k, tt, yy);
-                    s_kt[env * cap + k] = tt;
-                    s_ky[env * cap + k] = yy;
-                    s_M[env * cap + k] = M2[lo2 + k];
+                kb[env] = S.pref[env][rank] + S.run_cur[env];
+                const int P = S.P[env];
+                if (P >= 2) {
+                    lo2[env] = max(0, S.mir[env] + kb[env] - 2);
+                    hi2[env] = min(S.p2[env] - 1, S.mir[env] + kb[env] + kc[env] + 1);
                 }
-                const int kb = I.kb[env], kc = I.kcnt[env];
-                for (int k = tid; k < kc; k += EVAL_THREADS) {
-                    const int j = kt[kb + k] - t0;
-                    if (j >= 0 && j < tl) atomicOr(&s_mask[env * W + (j >> 5)], 1u << (j & 31));
-                    else raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, 2000000 + task);
+            }
+            cl0[0] = kb[0] + ex;
+            cl0[1] = kb[1] + en;
+            if (tid == 0) {
+                for (int env = 0; env < 2; ++env) {
+                    if (hi2[env] - lo2[env] + 1 > cap || kb[env] + kc[env] > S.P[env]) {
+                        raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
+                    }
+                }
+            }
+            for (int env = 0; env < 2; ++env)
+                if (hi2[env] - lo2[env] + 1 > cap || kb[env] + kc[env] > S.P[env]) hi2[env] = lo2[env] - 1;
+            // ---------------- (c) stage the intervals the tile uses ----------------
+            const int n0 = hi2[0] - lo2[0] + 1, n1 = hi2[1] - lo2[1] + 1;
+            for (int k = tid; k < n0 + n1; k += THREADS) {
+                const int env = (k >= n0) ? 1 : 0;
+                const int kk = k - env * n0;
+                const int cnt = env ? n1 : n0;
+                const int i2 = lo2[env] + kk;
+                const double* M2 = sl.M + (int64_t)env * C.kcap;
+                int ta;
+                double ya;
+                knot2<T>(C, sl, S, env, i2, ta, ya);
+                const double Ma = __ldcg(M2 + i2);
+                const int o = env * cap + kk;
+                sm.kt[o] = ta;
+                sm.c0[o] = ya;
+                if (EXACT) {
+                    sm.c1[o] = Ma;
+                } else if (kk + 1 < cnt) {
+                    // monomial form of interval [i2, i2+1]: y + s(c1 + s(c2 + s c3)), s = t - t_i2,
+                    // c1 = (y'-y)/h - h(2M + M')/6, c2 = M/2, c3 = (M'-M)/(6h)
+                    int tb;
+                    double yb;
+                    knot2<T>(C, sl, S, env, i2 + 1, tb, yb);
+                    const double Mb = __ldcg(M2 + i2 + 1);
+                    const double h = (double)(tb - ta);
+                    const double ih = fast_rcp(h);
+                    sm.c1[o] = fma(yb - ya, ih, -h * fma(2.0, Ma, Mb) * (1.0 / 6.0));
+                    sm.c2[o] = 0.5 * Ma;
+                    sm.c3[o] = (Mb - Ma) * ih * (1.0 / 6.0);
+                }
+            }
+            if (tid == 0) {
+                // is t0-1 a knot of each kind? (only the segment's first tile evaluates t0-1)
+                S.left_knot[0] = S.left_knot[1] = 0;
+                if (first && t0 - 1 >= 1 && t0 - 1 <= n - 2) {
+                    const double a = S.hold_m2, b = sm.h[0], c = sm.h[1];
+                    S.left_knot[0] = (b > a) && (b > c);
+                    S.left_knot[1] = (b < a) && (b < c);
                 }
             }
             __syncthreads();
-            if (!EXACT) {
-                for (int k = tid; k < 2 * cap; k += EVAL_THREADS) {
-                    const int env = k >= cap ? 1 : 0, kk = k - env * cap;
-                    if (kk < I.hi2[env] - I.lo2[env]) {
-                        s_aux[k] = 1.0 / (double)(s_kt[k + 1] - s_kt[k]);
-                    }
-                }
-            }
-            if (wid < 2) {  // exclusive prefix of the word popcounts
-                const int env = wid;
-                int carry = 0;
-                for (int w0 = 0; w0 < W; w0 += 32) {
-                    const int w = w0 + lane;
-                    const int c = (w < W) ? __popc(s_mask[env * W + w]) : 0;
-                    int inc = c;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const int t = __shfl_up_sync(0xffffffffu, inc, o);
-                        if (lane >= o) inc += t;
-                    }
-                    if (w < W) s_wb[env * W + w] = carry + inc - c;
-                    carry += __shfl_sync(0xffffffffu, inc, 31);
-                }
-            }
         }
-        __syncthreads();
 
-        // ---------------- 3. compute the new values (tile + 1-sample halo) ----------------
-        double num = 0.0, den = 0.0;
-        for (int jj = tid; jj < tl + 2; jj += EVAL_THREADS) {
-            const int j = jj - 1;
-            const int t = t0 + j;
-            if (t < 0 || t >= n) continue;
-            if (sifting) {
-                const double h = s_h[jj];
-                const double eu = env_value<EXACT>(I, 0, t, s_mask, s_wb, s_kt, s_ky, s_M, s_aux, C);
-                const double el = env_value<EXACT>(I, 1, t, s_mask + W, s_wb + W, s_kt + cap, s_ky + cap,
-                                                   s_M + cap, s_aux + cap, C);
-                const double m = 0.5 * (eu + el);
-                const double hn = rnd<T>(h - m);
-                s_f[jj] = hn;
-                if (j >= 0 && j < tl) {
+        // ---------------- (d) new values ----------------
+        int cl[2] = {cl0[0], cl0[1]};
+#pragma unroll
+        for (int i = 0; i < RUN_MAX; ++i) {
+            const int j = j0 + i, t = t0 + j;
+            if (i < run && j < tl) {
+                if (sifting) {
+                    const double h = hv[i];
+                    const double eu = (S.P[0] < 2) ? S.cval[0]
+                                      : env_at<EXACT>(sm, 0, cl[0] + mirror_adj(S, 0, t), t, lo2[0], S.p2[0]);
+                    const double el = (S.P[1] < 2) ? S.cval[1]
+                                      : env_at<EXACT>(sm, 1, cl[1] + mirror_adj(S, 1, t), t, lo2[1], S.p2[1]);
+                    cl[0] += (kmx >> i) & 1u;
+                    cl[1] += (kmn >> i) & 1u;
+                    const double m = 0.5 * (eu + el);
+                    const double hn = rnd<T>(h - m);
+                    fv[i] = hn;
                     if (C.rules == EEMD_RULES_NUMBA) {
-                        num += m * m;
+                        num = EXACT ? num + m * m : fma(m, m, num);
                     } else {
                         const double dd = h - hn;
-                        num += dd * dd;
+                        num = EXACT ? num + dd * dd : fma(dd, dd, num);
                     }
-                    den += h * h;
+                    den = EXACT ? den + h * h : fma(h, h, den);
+                    gv[i] = (mode == TM_LAST) ? rnd<T>(rv[i] - hn) : hn;
+                } else if (mode == TM_TRANS) {
+                    const double hvv = S.imf_from_resid ? rv[i] : (double)imf_m[t];
+                    fv[i] = rnd<T>(rv[i] - hvv);
+                    gv[i] = fv[i];
+                } else {  // TM_INIT
+                    fv[i] = trial_input<T>(C, d, t);
+                    gv[i] = fv[i];
                 }
-                if (mode == TM_LAST) s_r[jj] = rnd<T>(s_r[jj] - hn);
-            } else if (mode == TM_TRANS) {
-                const double ro = s_r[jj];
-                const double hv = I.imf_from_resid ? ro : (double)imf_m[t];
-                s_f[jj] = rnd<T>(ro - hv);
-            } else {  // TM_INIT
-                s_f[jj] = trial_input<T>(C, d, t);
+                sm.f[1 + j] = fv[i];
+                if (mode == TM_LAST) sm.r[1 + j] = gv[i];
             }
         }
-        __syncthreads();
-        const double* G = (mode == TM_LAST) ? s_r : s_f;  // signal whose extrema are the next knots
-
-        // ---------------- 4. next knots: flags, counts ----------------
-        for (int j0 = 0; j0 < TILE; j0 += EVAL_THREADS) {
-            const int j = j0 + tid;
-            const int t = t0 + j;
-            bool fmx = false, fmn = false;
-            if (j < tl && t >= 1 && t <= n - 2) {
-                const double g = G[j + 1], gl = G[j], gr = G[j + 2];
-                fmx = (g > gl) && (g > gr);
-                fmn = (g < gl) && (g < gr);
-            }
-            const unsigned bm = __ballot_sync(0xffffffffu, fmx);
-            const unsigned bn = __ballot_sync(0xffffffffu, fmn);
-            if (lane == 0 && j < TILE) {
-                s_nm[j >> 5] = bm;
-                s_nm[W + (j >> 5)] = bn;
-            }
-        }
-        __syncthreads();
-        if (wid < 2) {
-            const int env = wid;
-            int carry = 0;
-            for (int w0 = 0; w0 < W; w0 += 32) {
-                const int w = w0 + lane;
-                const int c = (w < W) ? __popc(s_nm[env * W + w]) : 0;
-                int inc = c;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int t = __shfl_up_sync(0xffffffffu, inc, o);
-                    if (lane >= o) inc += t;
-                }
-                if (w < W) s_nb[env * W + w] = carry + inc - c;
-                carry += __shfl_sync(0xffffffffu, inc, 31);
-            }
-            if (lane == 0) I.agg[env] = carry;
-        }
-        __syncthreads();
-
-        // ---------------- 5. decoupled look-back over the task's tiles ----------------
         if (tid == 0) {
-            unsigned long long* st = C.status + (int64_t)I.q * C.TT + d.tile_off;
-            const uint32_t amax = (uint32_t)I.agg[0], amin = (uint32_t)I.agg[1];
-            uint32_t emax = 0, emin = 0;
-            if (tile == 0) {
-                atomicExch(&st[0], lb_pack(LB_INC, amax, amin));
-            } else {
-                atomicExch(&st[tile], lb_pack(LB_AGG, amax, amin));
-                const long long limit = C.watchdog > 0 ? C.watchdog : -C.watchdog;
-                if (C.watchdog < 0) {
-                    // watchdog test mode: wait on a flag nothing sets, give up after `limit` polls
-                    long long spins = 0;
-                    while (*((volatile int32_t*)&C.hdr->pad[0]) == 0) {
-                        if (++spins > limit) {
-                            raise_error(C.hdr, EEMD_E_TIMEOUT, task);
-                            break;
-                        }
-                        __nanosleep(32);
-                    }
+            // halo samples t0-1 (first tile of the segment) and t0+tl
+            for (int side = 0; side < 2; ++side) {
+                int jj, t;
+                if (side == 0) {
+                    if (!(first && t0 > 0)) continue;
+                    jj = 0;
+                    t = t0 - 1;
+                } else {
+                    if (t0 + tl >= n) continue;
+                    jj = tl + 1;
+                    t = t0 + tl;
                 }
-                int k = tile - 1;
-                long long spins = 0;
-                while (k >= 0) {
-                    const unsigned long long v = *((volatile unsigned long long*)&st[k]);
-                    const uint32_t fl = lb_flag(v);
-                    if (fl == LB_EMPTY) {
-                        if (++spins > limit) {
-                            raise_error(C.hdr, EEMD_E_TIMEOUT, task);
-                            break;
+                double fn, gn;
+                if (sifting) {
+                    double e2[2];
+                    for (int env = 0; env < 2; ++env) {
+                        if (S.P[env] < 2) {
+                            e2[env] = S.cval[env];
+                        } else {
+                            const int c = (side == 0 ? kb[env] - S.left_knot[env] : kb[env] + kc[env]) +
+                                          mirror_adj(S, env, t);
+                            e2[env] = env_at<EXACT>(sm, env, c, t, lo2[env], S.p2[env]);
                         }
-                        __nanosleep(64);
-                        continue;
                     }
-                    emax += lb_max(v);
-                    emin += lb_min(v);
-                    if (fl == LB_INC) break;
-                    --k;
+                    const double m = 0.5 * (e2[0] + e2[1]);
+                    fn = rnd<T>(sm.h[jj] - m);
+                    gn = (mode == TM_LAST) ? rnd<T>(sm.r[jj] - fn) : fn;
+                } else if (mode == TM_TRANS) {
+                    const double ro = sm.r[jj];
+                    const double hvv = S.imf_from_resid ? ro : (double)__ldcg(imf_m + t);
+                    fn = rnd<T>(ro - hvv);
+                    gn = fn;
+                } else {
+                    fn = trial_input<T>(C, d, t);
+                    gn = fn;
                 }
-                atomicExch(&st[tile], lb_pack(LB_INC, emax + amax, emin + amin));
+                sm.f[jj] = fn;
+                if (mode == TM_LAST) sm.r[jj] = gn;
             }
-            // clear this tile's word of the other plane for the next step
-            C.status[(int64_t)(I.q ^ 1) * C.TT + gt] = 0ull;
-            I.excl[0] = (int)emax;
-            I.excl[1] = (int)emin;
-            C.tpref[(int64_t)(I.kpar ^ 1) * C.TT + gt] = make_int2((int)emax, (int)emin);
         }
         __syncthreads();
+        const double* G = (mode == TM_LAST) ? sm.r : sm.f;  // signal whose extrema are the next knots
 
-        // ---------------- 6. write knots, samples, edges ----------------
-        {
-            const int np = I.kpar ^ 1;
-            const int64_t pmx = (int64_t)(np * 2 + 0) * C.KC + d.k_off;
-            const int64_t pmn = (int64_t)(np * 2 + 1) * C.KC + d.k_off;
-            int32_t* ktx = C.kt + pmx;
-            int32_t* ktn = C.kt + pmn;
-            T* kyx = static_cast<T*>(C.ky) + pmx;
-            T* kyn = static_cast<T*>(C.ky) + pmn;
-            const int kcap_real = d.kcap - 2;
-            for (int j = tid; j < tl; j += EVAL_THREADS) {
-                const int t = t0 + j;
-                const int w = j >> 5, b = j & 31;
-                const unsigned lt = (1u << b) - 1u;
-                const unsigned mx = s_nm[w], mn = s_nm[W + w];
-                const double g = G[j + 1];
-                if ((mx >> b) & 1u) {
-                    const int pos = I.excl[0] + s_nb[w] + __popc(mx & lt);
-                    if (pos < kcap_real) { ktx[pos] = t; kyx[pos] = (T)g; }
-                    else raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, task);
-                }
-                if ((mn >> b) & 1u) {
-                    const int pos = I.excl[1] + s_nb[W + w] + __popc(mn & lt);
-                    if (pos < kcap_real) { ktn[pos] = t; kyn[pos] = (T)g; }
-                    else raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, task);
-                }
-                switch (mode) {
-                    case TM_SIFT: imf_m[t] = (T)s_f[j + 1]; break;
-                    case TM_LAST: imf_m[t] = (T)s_f[j + 1]; resid[t] = (T)s_r[j + 1]; break;
-                    case TM_TRANS:
-                        resid[t] = (T)s_f[j + 1];
-                        if (I.imf_from_resid) imf_m[t] = (T)s_r[j + 1];
-                        break;
-                    default: resid[t] = (T)s_f[j + 1]; break;
-                }
-            }
-            if (tid == 0) {
-                const double2 e = make_double2(G[1], G[tl]);
-                if (mode == TM_SIFT) C.hedge[(int64_t)((I.sift + 1) & 1) * C.TT + gt] = e;
-                else if (mode == TM_INIT) C.redge[gt] = e;
-                else C.redge[(int64_t)((I.imf + 1) & 1) * C.TT + gt] = e;
+        // ---------------- (e) next knots ----------------
+        unsigned nmx = 0u, nmn = 0u;
+#pragma unroll
+        for (int i = 0; i < RUN_MAX; ++i) {
+            const int j = j0 + i, t = t0 + j;
+            if (i < run && j < tl && t >= 1 && t <= n - 2) {
+                const double a = G[j], c = G[j + 2], v = gv[i];
+                if (v > a && v > c) nmx |= 1u << i;
+                if (v < a && v < c) nmn |= 1u << i;
             }
         }
+        int ex2, en2, tx2, tn2;
+        block_scan2(__popc(nmx), __popc(nmn), ex2, en2, tx2, tn2, s_w2);
 
-        // ---------------- 7. SD partial sums, completion ----------------
+        // ---------------- (f) writes ----------------
         {
-            const double2 r = block_sum2<EVAL_THREADS>(make_double2(num, den), s_red);
+            const int64_t pmx = knot_index(C, np, 0, rank, 0);
+            const int64_t pmn = knot_index(C, np, 1, rank, 0);
+            int px = S.run_new[0] + ex2, pn = S.run_new[1] + en2;
+#pragma unroll
+            for (int i = 0; i < RUN_MAX; ++i) {
+                const int j = j0 + i, t = t0 + j;
+                if (i < run && j < tl) {
+                    if ((nmx >> i) & 1u) {
+                        if (px < C.segcap) {
+                            sl.kt[pmx + px] = t;
+                            static_cast<T*>(sl.ky)[pmx + px] = (T)gv[i];
+                        } else {
+                            raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
+                        }
+                        ++px;
+                    }
+                    if ((nmn >> i) & 1u) {
+                        if (pn < C.segcap) {
+                            sl.kt[pmn + pn] = t;
+                            static_cast<T*>(sl.ky)[pmn + pn] = (T)gv[i];
+                        } else {
+                            raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
+                        }
+                        ++pn;
+                    }
+                    switch (mode) {
+                        case TM_SIFT: imf_m[t] = (T)fv[i]; break;
+                        case TM_LAST: imf_m[t] = (T)fv[i]; resid[t] = (T)gv[i]; break;
+                        case TM_TRANS:
+                            resid[t] = (T)fv[i];
+                            if (S.imf_from_resid) imf_m[t] = (T)rv[i];
+                            break;
+                        default: resid[t] = (T)fv[i]; break;
+                    }
+                }
+            }
+        }
+        // ---------------- (g) carry to the next tile, segment edges ----------------
+        if (tid == 0) {
+            const double* R = (mode == TM_LAST) ? sm.r : sm.f;  // residual after the step (non-SIFT)
+            if (first) {
+                S.hf0 = sm.f[1];
+                S.hf1 = (tl >= 2) ? sm.f[2] : 0.0;
+                S.rf0 = R[1];
+                S.rf1 = (tl >= 2) ? R[2] : 0.0;
+            }
+            if (last) {
+                Xchg& xo = X[q];
+                xo.hl[0] = (tl >= 2) ? sm.f[tl - 1] : S.f_m1;
+                xo.hl[1] = sm.f[tl];
+                xo.rl[0] = (tl >= 2) ? R[tl - 1] : S.g_m1;
+                xo.rl[1] = R[tl];
+            }
+            S.f_m1 = sm.f[tl];
+            S.g_m1 = G[tl];
+            if (sifting) {
+                S.hold_m2 = (tl >= 2) ? sm.h[tl - 1] : sm.h[0];
+                S.hold_m1 = sm.h[tl];
+            }
+            S.run_cur[0] += kc[0];
+            S.run_cur[1] += kc[1];
+            S.run_new[0] += tx2;
+            S.run_new[1] += tn2;
+        }
+        __syncthreads();
+    }
+    // ---------------- publish the segment's results ----------------
+    const double2 rs = block_sum2<THREADS>(make_double2(num, den), s_red);
+    if (tid == 0) {
+        Xchg& xo = X[q];
+        xo.hf[0] = S.hf0;
+        xo.hf[1] = S.hf1;
+        if (mode == TM_SIFT) {
+            // the residual is unchanged by a plain sift: carry the previous edges
+            const Xchg& xp = X[q ^ 1];
+            xo.rf[0] = xp.rf[0];
+            xo.rf[1] = xp.rf[1];
+            xo.rl[0] = xp.rl[0];
+            xo.rl[1] = xp.rl[1];
+        } else {
+            xo.rf[0] = S.rf0;
+            xo.rf[1] = S.rf1;
+        }
+        xo.num = rs.x;
+        xo.den = rs.y;
+        xo.cnt[0] = S.run_new[0];
+        xo.cnt[1] = S.run_new[1];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// decisions (emd_ref.py:120-153; emd_gpu.py:152-274)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void log_sift(const Ctx& C, const TaskSm& S) {
+    if (C.knot_log && S.rank == 0) {
+        int32_t* p = C.knot_log + (((int64_t)S.task * C.max_imf + S.imf) * C.max_sifts + S.sift) * 2;
+        p[0] = S.P[0];
+        p[1] = S.P[1];
+    }
+}
+
+__device__ __forceinline__ void close_imf(const Ctx& C, TaskSm& S) {
+    if (C.mode_sifts && S.rank == 0) C.mode_sifts[(int64_t)S.task * C.max_imf + S.imf] = S.mode_sifts_cur;
+    S.nmode = S.imf + 1;
+    S.imf += 1;
+    S.mode_sifts_cur = 0;
+}
+
+// adopt the knots the last sweep produced (segment counts nc[env][r])
+__device__ __forceinline__ void adopt(TaskSm& S, const int nc[2][MAXC], int cmax, int cmin) {
+    S.kpar ^= 1;
+    S.P[0] = cmax;
+    S.P[1] = cmin;
+    for (int env = 0; env < 2; ++env) {
+        int acc = 0;
+        for (int r = 0; r < S.csize; ++r) {
+            S.pref[env][r] = acc;
+            acc += nc[env][r];
+        }
+        S.pref[env][S.csize] = acc;
+    }
+}
+
+__device__ __forceinline__ void imf_level(const Ctx& C, TaskSm& S, const int nc[2][MAXC], int cmax,
+                                          int cmin) {
+    bool stop = (cmax + cmin < C.min_extrema);
+    if (C.rules == EEMD_RULES_NUMBA) stop = stop || cmax < 2 || cmin < 2;
+    if (stop) { S.phase = PH_DONE; return; }
+    if (S.imf >= C.max_imf) { S.phase = PH_DONE; S.flags |= 1; return; }
+    S.mode_sifts_cur = 0;
+    if (C.rules == EEMD_RULES_REF && (cmax < 1 || cmin < 1)) {
+        // emd_ref.py:132-133: the sift loop breaks before its first sift; the IMF is the residual
+        S.phase = PH_TRANS;
+        S.imf_from_resid = 1;
+        return;
+    }
+    S.phase = PH_SIFT;
+    S.sift = 0;
+    S.src_resid = 1;
+    S.imf_from_resid = 0;
+    adopt(S, nc, cmax, cmin);
+}
+
+__device__ void decide(const Ctx& C, TaskSm& S, Xchg* X, cg::cluster_group& cl) {
+    if (threadIdx.x == 0) {
+        const int q = S.step & 1;
+        double num = 0.0, den = 0.0;
+        int nc[2][MAXC];
+        int cmax = 0, cmin = 0;
+        for (int r = 0; r < S.csize; ++r) {
+            const Xchg* xr = cl.map_shared_rank(&X[q], r);
+            num += xr->num;
+            den += xr->den;
+            nc[0][r] = xr->cnt[0];
+            nc[1][r] = xr->cnt[1];
+            cmax += nc[0][r];
+            cmin += nc[1][r];
+        }
+        const int mode = S.mode;
+        if (mode == TM_SIFT) {
+            log_sift(C, S);
+            S.mode_sifts_cur += 1;
+            S.nsift_total += 1;
+            const double sdv = den > 0.0 ? num / den : 0.0;
+            bool stop = (S.sift >= 1) && (sdv < C.tau);
+            if (!stop) stop = (C.rules == EEMD_RULES_NUMBA) ? (cmax < 2 || cmin < 2) : (cmax < 1 || cmin < 1);
+            if (stop) {
+                S.phase = PH_TRANS;
+                S.imf_from_resid = 0;
+            } else {
+                S.sift += 1;
+                S.src_resid = 0;
+                adopt(S, nc, cmax, cmin);
+            }
+        } else if (mode == TM_LAST) {
+            log_sift(C, S);
+            S.mode_sifts_cur += 1;
+            S.nsift_total += 1;
+            close_imf(C, S);
+            imf_level(C, S, nc, cmax, cmin);
+        } else if (mode == TM_TRANS) {
+            close_imf(C, S);
+            imf_level(C, S, nc, cmax, cmin);
+        } else {
+            S.imf = 0;
+            S.nmode = 0;
+            imf_level(C, S, nc, cmax, cmin);
+        }
+        S.step += 1;
+        // every IMF ends after at most max_sifts sifts plus one closing step
+        if (S.phase != PH_DONE && S.step > 2 + C.max_imf * (C.max_sifts + 1)) {
+            raise_error(C.hdr, EEMD_E_TIMEOUT, S.task);
+            S.phase = PH_DONE;
+        }
+    }
+    __syncthreads();
+}
+
+// per-step constants of the envelopes (mirror knots, constant envelope)
+template <typename T>
+__device__ void step_setup(const Ctx& C, const Slot& sl, TaskSm& S) {
+    if (threadIdx.x < 2) {
+        const int env = threadIdx.x;
+        const int P = S.P[env];
+        const int mir = (C.end_mode == EEMD_END_MIRROR && P >= 3) ? 1 : 0;
+        S.mir[env] = mir;
+        S.p2[env] = P + 2 * mir;
+        S.cval[env] = 0.0;
+        S.tfirst[env] = S.tlast[env] = 0;
+        if (P >= 1) {
+            int t0;
+            double y0;
+            real_knot<T>(C, sl, S, env, 0, t0, y0);
+            if (P == 1) S.cval[env] = y0;
+            if (mir) {
+                int t1, ta, tb;
+                double y1, ya, yb;
+                real_knot<T>(C, sl, S, env, 1, t1, y1);
+                real_knot<T>(C, sl, S, env, P - 1, ta, ya);
+                real_knot<T>(C, sl, S, env, P - 2, tb, yb);
+                S.tfirst[env] = 2 * t0 - t1;
+                S.tlast[env] = 2 * ta - tb;
+            }
+        }
+        if (S.p2[env] > C.kcap) raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// k_emd: the persistent cluster kernel
+// ---------------------------------------------------------------------------
+template <typename T, bool EXACT>
+__global__ void __launch_bounds__(THREADS, 2) k_emd(Ctx C) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ TaskSm S;
+    __shared__ Xchg X[2];
+    __shared__ int s_claim;
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    const int csize = (int)cl.num_blocks();
+    const int slot = blockIdx.x / csize;
+    const int tid = threadIdx.x;
+    const Smem sm = carve(smem_raw, C.tile);
+    Slot sl;
+    sl.kt = C.kt + (int64_t)slot * C.slot_knots;
+    sl.ky = static_cast<T*>(C.ky) + (int64_t)slot * C.slot_knots;
+    sl.M = C.M + (int64_t)slot * C.slot_M;
+
+    for (;;) {
+        if (rank == 0 && tid == 0) s_claim = atomicAdd(&C.hdr->next_task, 1);
+        cl.sync();
+        const int q = *cl.map_shared_rank(&s_claim, 0);
+        cl.sync();
+        if (q >= C.n_tasks) break;
+        if (tid == 0) {
+            const int task = C.order[q];
+            const TaskDesc d = C.td[task];
+            S.task = task;
+            S.n = d.n;
+            S.rank = rank;
+            S.csize = csize;
+            S.s0 = min(d.n, rank * d.seg);
+            S.s1 = min(d.n, S.s0 + d.seg);
+            S.phase = PH_INIT;
+            S.imf = S.sift = S.kpar = S.src_resid = S.imf_from_resid = 0;
+            S.nsift_total = S.nmode = S.mode_sifts_cur = S.flags = S.step = 0;
+            S.P[0] = S.P[1] = 0;
+            for (int r = 0; r <= MAXC; ++r) S.pref[0][r] = S.pref[1][r] = 0;
+            S.mir[0] = S.mir[1] = 0;
+            S.f_m1 = S.g_m1 = 0.0;
+            if (C.watchdog < 0 && rank == 0) {
+                // watchdog test mode: a bounded wait on a flag nothing sets
+                long long spins = 0;
+                while (*((volatile int32_t*)&C.hdr->wd_flag) == 0) {
+                    if (++spins > -C.watchdog) {
+                        raise_error(C.hdr, EEMD_E_TIMEOUT, task);
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+            }
+        }
+        __syncthreads();
+        while (S.phase != PH_DONE) {
             if (tid == 0) {
-                C.partial[gt] = r;
-                __threadfence();
-                const unsigned old = atomicAdd(&C.ts[task].done_count, 1u);
-                I.is_last = (old + 1 == (unsigned)I.ntiles) ? 1 : 0;
+                if (S.phase == PH_INIT) S.mode = TM_INIT;
+                else if (S.phase == PH_TRANS) S.mode = TM_TRANS;
+                else S.mode = (S.sift + 1 >= C.max_sifts) ? TM_LAST : TM_SIFT;
             }
             __syncthreads();
+            if (S.mode == TM_SIFT || S.mode == TM_LAST) {
+                step_setup<T>(C, sl, S);
+                solve_task<T, EXACT>(C, sl, S, sm);
+                cl.sync();  // second derivatives of every segment visible
+            }
+            sweep<T, EXACT>(C, sl, S, X, sm, cl);
+            cl.sync();  // segment results published
+            decide(C, S, X, cl);
         }
-
-        // ---------------- 8. per-task decision (last tile to finish) ----------------
-        if (I.is_last) {
-            __threadfence();
-            double2 acc = make_double2(0.0, 0.0);
-            if (sifting) {
-                for (int i = tid; i < I.ntiles; i += EVAL_THREADS) {
-                    const double2 p = __ldcg(&C.partial[(int64_t)d.tile_off + i]);
-                    acc.x += p.x;
-                    acc.y += p.y;
-                }
-            }
-            acc = block_sum2<EVAL_THREADS>(acc, s_red);
-            if (tid == 0) {
-                const unsigned long long v =
-                    __ldcg(&C.status[(int64_t)I.q * C.TT + d.tile_off + I.ntiles - 1]);
-                const int cmax = (int)lb_max(v), cmin = (int)lb_min(v);
-                TaskState s = C.ts[task];
-                if (mode == TM_SIFT) {
-                    log_sift(C, task, s);
-                    s.mode_sifts_cur += 1;
-                    s.nsift_total += 1;
-                    const double sdv = acc.y > 0.0 ? acc.x / acc.y : 0.0;
-                    bool stop = (s.sift >= 1) && (sdv < C.tau);
-                    if (!stop) {
-                        stop = (C.rules == EEMD_RULES_NUMBA) ? (cmax < 2 || cmin < 2) : (cmax < 1 || cmin < 1);
-                    }
-                    if (stop) {
-                        s.phase = PH_TRANS;
-                        s.imf_from_resid = 0;
-                    } else {
-                        s.sift += 1;
-                        s.kpar ^= 1;
-                        s.pmax = cmax;
-                        s.pmin = cmin;
-                        s.src_resid = 0;
-                    }
-                } else if (mode == TM_LAST) {
-                    log_sift(C, task, s);
-                    s.mode_sifts_cur += 1;
-                    s.nsift_total += 1;
-                    close_imf(C, s, task);
-                    imf_level(C, s, cmax, cmin);
-                } else if (mode == TM_TRANS) {
-                    close_imf(C, s, task);
-                    imf_level(C, s, cmax, cmin);
-                } else {
-                    s.imf = 0;
-                    s.nmode = 0;
-                    imf_level(C, s, cmax, cmin);
-                }
-                s.done_count = 0u;
-                C.ts[task] = s;
-            }
+        if (rank == 0 && tid == 0) {
+            TaskOut o;
+            o.nsift = S.nsift_total;
+            o.nmode = S.nmode;
+            o.flags = S.flags;
+            o.pad = 0;
+            C.tout[S.task] = o;
+            atomicAdd(&C.hdr->n_done, 1);
         }
         __syncthreads();
     }
@@ -910,22 +1099,23 @@ __global__ void __launch_bounds__(EVAL_THREADS) k_eval(Ctx C) {
 // k_reduce: imf_sum[s][m][t] += trial-ordered sum over the batch (emd_par.py:241-245)
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void k_reduce(Ctx C, double* imf_sum, int32_t* mode_count) {
+__global__ void k_reduce(const SignalDesc* sdesc, const TaskDesc* td, const TaskOut* tout, const void* imfs,
+                         int trial_count, int max_imf, double* imf_sum, int32_t* mode_count) {
     const int s = blockIdx.z, m = blockIdx.y;
-    const SignalDesc sd = C.sd[s];
+    const SignalDesc sd = sdesc[s];
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (mode_count && blockIdx.x == 0 && threadIdx.x == 0) {
         int cnt = 0;
-        for (int e = 0; e < C.trial_count; ++e) cnt += (C.ts[sd.first_task + e].nmode > m) ? 1 : 0;
-        mode_count[(int64_t)s * C.max_imf + m] += cnt;
+        for (int e = 0; e < trial_count; ++e) cnt += (tout[sd.first_task + e].nmode > m) ? 1 : 0;
+        mode_count[(int64_t)s * max_imf + m] += cnt;
     }
     if (!imf_sum || t >= sd.n) return;
     double acc = 0.0;
     bool any = false;
-    for (int e = 0; e < C.trial_count; ++e) {
+    for (int e = 0; e < trial_count; ++e) {
         const int task = sd.first_task + e;
-        if (C.ts[task].nmode > m) {
-            const double v = ldv<T>(C.imfs, C.td[task].imf_off + (int64_t)m * sd.n + t);
+        if (tout[task].nmode > m) {
+            const double v = ldv<T>(imfs, td[task].imf_off + (int64_t)m * sd.n + t);
             acc = any ? acc + v : v;
             any = true;
         }
@@ -936,13 +1126,13 @@ __global__ void k_reduce(Ctx C, double* imf_sum, int32_t* mode_count) {
     }
 }
 
-__global__ void k_outputs(Ctx C, int32_t* nsift, int32_t* nmode, int32_t* flags) {
+__global__ void k_outputs(const TaskOut* tout, int n_tasks, int32_t* nsift, int32_t* nmode, int32_t* flags) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= C.n_tasks) return;
-    const TaskState s = C.ts[i];
-    if (nsift) nsift[i] = s.nsift_total;
-    if (nmode) nmode[i] = s.nmode;
-    if (flags) flags[i] = s.flags;
+    if (i >= n_tasks) return;
+    const TaskOut o = tout[i];
+    if (nsift) nsift[i] = o.nsift;
+    if (nmode) nmode[i] = o.nmode;
+    if (flags) flags[i] = o.flags;
 }
 
 // ---------------------------------------------------------------------------
@@ -985,32 +1175,30 @@ using namespace eemd;
 
 namespace {
 
+constexpr int ASSUMED_SMS = 148;        // B200
+constexpr int ASSUMED_CTAS_PER_SM = 2;  // resident k_emd CTAs per SM the grid is sized for
+
 struct Layout {
     std::vector<TaskDesc> td;
     std::vector<SignalDesc> sd;
-    int64_t TT = 0, NS = 0, KC = 0, NIMF = 0, SCR = 0;
-    int tile = 0, B = 0, S = 0;
-    int max_chunks = 0;
-    size_t o_hdr, o_td, o_ts, o_sd, o_sigma, o_el_task, o_el_pref, o_sl_item, o_sl_pref;
-    size_t o_status, o_partial, o_tpref, o_hedge, o_redge, o_resid, o_imfs, o_kt, o_ky, o_M, o_scr;
+    std::vector<int32_t> order;
+    int64_t NS = 0, NIMF = 0, slot_knots = 0, slot_M = 0;
+    int tile = 0, B = 0, S = 0, csize = 1, slots = 1, segcap = 0, kcap = 0, scr_rows = 0;
+    size_t o_hdr, o_td, o_order, o_tout, o_sd, o_sigma, o_resid, o_imfs, o_kt, o_ky, o_M, o_scr;
     size_t total = 0;
 };
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-int autotune_tile(int64_t nmax) {
-    // length buckets: short signals use small tiles so that a task spans
-    // several CTAs; long ones amortise the tile's halo and look-back.
-    if (nmax <= 8192) return 512;
-    if (nmax <= 262144) return 1024;
-    return 2048;
-}
+// Launch shapes by length bucket.  The cluster spreads one task over several
+// SMs when there are fewer tasks than CTA slots; tiles live inside a segment.
+int autotune_tile(int64_t seg) { return seg <= 4096 ? 512 : 1024; }
 
-int autotune_block(int64_t nmax) { return nmax <= 262144 ? 64 : 256; }
-
-size_t eval_smem_bytes(int TILE) {
-    const int W = TILE >> 5, cap = (TILE >> 1) + 8;
-    return (size_t)3 * (TILE + 2) * 8 + (size_t)2 * cap * 8 * 3 + (size_t)2 * cap * 4 + (size_t)4 * 2 * W * 4;
+int autotune_csize(int64_t n_tasks, int64_t nmin) {
+    const int64_t budget = (int64_t)ASSUMED_SMS * ASSUMED_CTAS_PER_SM;
+    int c = (int)std::max<int64_t>(1, std::min<int64_t>(8, budget / std::max<int64_t>(n_tasks, 1)));
+    while (c > 1 && nmin / c < 2048) --c;
+    return c;
 }
 
 int check_params(const eemd_params* p) {
@@ -1021,8 +1209,9 @@ int check_params(const eemd_params* p) {
     if (p->end_mode != EEMD_END_NATURAL && p->end_mode != EEMD_END_MIRROR) return EEMD_E_BADARG;
     if (p->rules != EEMD_RULES_REF && p->rules != EEMD_RULES_NUMBA) return EEMD_E_BADARG;
     if (p->noise_mode < EEMD_NOISE_NONE || p->noise_mode > EEMD_NOISE_PREPERTURBED) return EEMD_E_BADARG;
-    if (p->tile != 0 && (p->tile < 256 || p->tile > 4096 || p->tile % 256 != 0)) return EEMD_E_BADARG;
-    if (p->knots_per_block < 0 || p->halo < 0) return EEMD_E_BADARG;
+    if (p->tile != 0 && p->tile != 256 && p->tile != 512 && p->tile != 1024) return EEMD_E_BADARG;
+    if (p->knots_per_block < 0 || p->knots_per_block > 4096 || p->halo < 0 || p->halo > 256)
+        return EEMD_E_BADARG;
     return EEMD_OK;
 }
 
@@ -1033,19 +1222,21 @@ int make_layout(const eemd_params* p, const int64_t* lengths, int n_signals, int
     if (!lengths || n_signals < 1 || trial_count < 1) return EEMD_E_BADARG;
     const int64_t n_tasks = (int64_t)n_signals * trial_count;
     if (n_tasks > (1 << 24)) return EEMD_E_BADARG;
-    int64_t nmax = 0;
+    int64_t nmax = 0, nmin = INT64_MAX;
     for (int s = 0; s < n_signals; ++s) {
         if (lengths[s] < 3 || lengths[s] > (1LL << 30)) return EEMD_E_BADARG;
         nmax = std::max(nmax, lengths[s]);
+        nmin = std::min(nmin, lengths[s]);
     }
-    L.tile = p->tile ? p->tile : autotune_tile(nmax);
-    L.B = p->knots_per_block ? p->knots_per_block : autotune_block(nmax);
-    L.S = p->halo ? p->halo : 32;
+    L.csize = autotune_csize(n_tasks, nmin);
+    L.S = p->halo ? p->halo : (p->exact ? 32 : 24);
+    L.B = p->knots_per_block ? p->knots_per_block : 64;
+    if (p->exact && (2 * L.S + L.B + 8 > SOLVE_CAP)) return EEMD_E_BADARG;
+    if (!p->exact && 2 * L.S + FAST_B + 8 > SOLVE_CAP) return EEMD_E_BADARG;
+    int64_t segmax = 0;
     L.td.resize(n_tasks);
     L.sd.resize(n_signals);
-    int64_t xo = 0, so = 0, imo = 0, ko = 0, scro = 0, sumo = 0;
-    int64_t to = 0;
-    int64_t chunks = 0;
+    int64_t xo = 0, so = 0, imo = 0, sumo = 0;
     for (int s = 0; s < n_signals; ++s) {
         const int64_t n = lengths[s];
         SignalDesc& sd = L.sd[s];
@@ -1055,64 +1246,58 @@ int make_layout(const eemd_params* p, const int64_t* lengths, int n_signals, int
         sd.n = (int32_t)n;
         sd.first_task = s * trial_count;
         sumo += (int64_t)p->max_imf * n;
-        const int kcap = (int)(n / 2 + 4);
-        const int nwin_max = (kcap + L.B - 1) / L.B;
-        const int nch = (nwin_max + SOLVE_THREADS - 1) / SOLVE_THREADS;
-        const int64_t scr_env = (int64_t)nch * (L.B + L.S) * SOLVE_THREADS;
+        int64_t seg = (n + L.csize - 1) / L.csize;
+        seg = (seg + 31) / 32 * 32;
+        if ((L.csize - 1) * seg + 2 > n) return EEMD_E_BADARG;  // every segment keeps >= 2 samples
+        segmax = std::max(segmax, seg);
         for (int e = 0; e < trial_count; ++e) {
             TaskDesc& d = L.td[(int64_t)s * trial_count + e];
             d.x_off = (p->noise_mode == EEMD_NOISE_PREPERTURBED) ? so : xo;
             d.s_off = so;
             d.imf_off = imo;
-            d.k_off = ko;
-            d.scr_off = scro;
-            d.scr_env = scr_env;
             d.noise_off = so;
             d.n = (int32_t)n;
-            d.kcap = kcap;
-            d.tile_off = (int32_t)to;
-            d.ntiles = (int32_t)((n + L.tile - 1) / L.tile);
             d.signal = s;
             d.trial = trial_begin + e;
+            d.seg = (int32_t)seg;
             so += n;
             imo += (int64_t)p->max_imf * n;
-            ko += kcap;
-            scro += 2 * scr_env;
-            to += d.ntiles;
-            chunks += 2 * nch;
         }
         xo += n;
     }
-    if (to > (1LL << 30)) return EEMD_E_BADARG;
-    L.TT = to;
+    // longest tasks first: the work queue hands them out in this order
+    L.order.resize(n_tasks);
+    std::iota(L.order.begin(), L.order.end(), 0);
+    std::stable_sort(L.order.begin(), L.order.end(), [&](int a, int b) { return L.td[a].n > L.td[b].n; });
+    L.tile = p->tile ? p->tile : autotune_tile(segmax);
+    L.segcap = (int)(segmax / 2 + 2);
+    L.kcap = (int)(nmax / 2 + 4);
+    L.slots = (int)std::max<int64_t>(
+        1, std::min<int64_t>(n_tasks, (int64_t)ASSUMED_SMS * ASSUMED_CTAS_PER_SM / L.csize));
+    L.slot_knots = (int64_t)2 * 2 * L.csize * L.segcap;
+    L.slot_M = (int64_t)2 * L.kcap;
+    L.scr_rows = p->exact ? (L.B + L.S) : 0;
     L.NS = so;
-    L.KC = ko;
     L.NIMF = imo;
-    L.SCR = scro;
-    L.max_chunks = (int)std::min<int64_t>(chunks, 1 << 30);
     const size_t bt = (p->dtype == EEMD_F64) ? 8 : 4;
     size_t off = 0;
-    auto take = [&](size_t bytes) { size_t o = off; off = align_up(off + bytes, 256); return o; };
+    auto take = [&](size_t bytes) {
+        size_t o = off;
+        off = align_up(off + bytes, 256);
+        return o;
+    };
     L.o_hdr = take(sizeof(Header));
     L.o_td = take(sizeof(TaskDesc) * n_tasks);
-    L.o_ts = take(sizeof(TaskState) * n_tasks);
+    L.o_order = take(sizeof(int32_t) * n_tasks);
+    L.o_tout = take(sizeof(TaskOut) * n_tasks);
     L.o_sd = take(sizeof(SignalDesc) * n_signals);
     L.o_sigma = take(sizeof(double) * n_signals);
-    L.o_el_task = take(sizeof(int32_t) * (n_tasks + 1));
-    L.o_el_pref = take(sizeof(int32_t) * (n_tasks + 1));
-    L.o_sl_item = take(sizeof(int32_t) * (2 * n_tasks + 1));
-    L.o_sl_pref = take(sizeof(int32_t) * (2 * n_tasks + 1));
-    L.o_status = take(sizeof(unsigned long long) * 2 * L.TT);
-    L.o_partial = take(sizeof(double2) * L.TT);
-    L.o_tpref = take(sizeof(int2) * 2 * L.TT);
-    L.o_hedge = take(sizeof(double2) * 2 * L.TT);
-    L.o_redge = take(sizeof(double2) * 2 * L.TT);
     L.o_resid = take(bt * L.NS);
     L.o_imfs = imfs_external ? 0 : take(bt * L.NIMF);
-    L.o_kt = take(sizeof(int32_t) * 4 * L.KC);
-    L.o_ky = take(bt * 4 * L.KC);
-    L.o_M = take(sizeof(double) * 2 * L.KC);
-    L.o_scr = take(sizeof(double2) * L.SCR);
+    L.o_kt = take(sizeof(int32_t) * L.slot_knots * L.slots);
+    L.o_ky = take(bt * L.slot_knots * L.slots);
+    L.o_M = take(sizeof(double) * L.slot_M * L.slots);
+    L.o_scr = take(sizeof(double2) * (size_t)L.scr_rows * L.slots * L.csize * THREADS);
     L.total = off;
     return EEMD_OK;
 }
@@ -1156,36 +1341,29 @@ struct Tracer {
     }
 };
 
-template <typename K>
-int grid_for(K kernel, int threads, size_t smem, int64_t work_items) {
-    int dev = 0, nsm = 0, occ = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem);
-    if (occ < 1) occ = 1;
-    int64_t g = (int64_t)nsm * occ;
-    if (work_items < g) g = work_items;
-    return (int)std::max<int64_t>(g, 1);
-}
-
 template <typename T, bool EXACT>
-int launch_steps(const Ctx& C, const Layout& L, int nsteps, cudaStream_t st, Tracer& tr) {
-    const size_t smem = eval_smem_bytes(L.tile);
-    cudaFuncSetAttribute(k_eval<T, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    const int ge = grid_for(k_eval<T, EXACT>, EVAL_THREADS, smem, L.TT);
-    const int gs = grid_for(k_solve<T, EXACT>, SOLVE_THREADS, 0, L.max_chunks);
-    for (int i = 0; i < nsteps; ++i) {
-        tr.begin(EEMD_K_PLAN);
-        k_plan<<<1, PLAN_THREADS, 0, st>>>(C);
-        tr.end();
-        tr.begin(EEMD_K_SOLVE);
-        k_solve<T, EXACT><<<gs, SOLVE_THREADS, 0, st>>>(C);
-        tr.end();
-        tr.begin(EEMD_K_EVAL);
-        k_eval<T, EXACT><<<ge, EVAL_THREADS, smem, st>>>(C);
-        tr.end();
-    }
-    return cudaGetLastError() == cudaSuccess ? EEMD_OK : EEMD_E_CUDA;
+int launch_emd(const Ctx& C, const Layout& L, cudaStream_t st, Tracer& tr) {
+    const size_t smem = smem_bytes(L.tile);
+    if (cudaFuncSetAttribute(k_emd<T, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return EEMD_E_CUDA;
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3((unsigned)(L.slots * L.csize), 1, 1);
+    cfg.blockDim = dim3(THREADS, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)L.csize;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    tr.begin(EEMD_K_EMD);
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, k_emd<T, EXACT>, C);
+    tr.end();
+    return e == cudaSuccess ? EEMD_OK : EEMD_E_CUDA;
 }
 
 template <typename T>
@@ -1195,44 +1373,23 @@ int run_typed(const eemd_params* p, const Layout& L, Ctx& C, double* imf_sum, in
     const int64_t n_tasks = (int64_t)L.td.size();
     if (p->noise_mode == EEMD_NOISE_PHILOX) {
         tr.begin(EEMD_K_SIGMA);
-        k_sigma<T><<<(int)L.sd.size(), 1024, 0, st>>>(C, p->eps, const_cast<double*>(C.sigma));
+        k_sigma<T><<<(int)L.sd.size(), 1024, 0, st>>>(C.sd, C.x, p->eps, const_cast<double*>(C.sigma));
         tr.end();
     }
-    tr.begin(EEMD_K_INIT);
-    k_init<<<(int)((n_tasks + 255) / 256), 256, 0, st>>>(C);
-    tr.end();
-    const int64_t bound = 1 + (int64_t)p->max_imf * (p->max_sifts + 1);
-    const int chunk = (p->tau > 0.0) ? 8 : (int)std::min<int64_t>(bound, 1 << 30);
-    int64_t done = 0;
-    while (done < bound) {
-        const int k = (int)std::min<int64_t>(chunk, bound - done);
-        int rc = p->exact ? launch_steps<T, true>(C, L, k, st, tr) : launch_steps<T, false>(C, L, k, st, tr);
-        if (rc) return rc;
-        done += k;
-        if (done < bound) {
-            // a cheap plan tells how many tasks are still alive
-            tr.begin(EEMD_K_PLAN);
-            k_plan<<<1, PLAN_THREADS, 0, st>>>(C);
-            tr.end();
-            Header h;
-            if (cudaMemcpyAsync(&h, C.hdr, sizeof(Header), cudaMemcpyDeviceToHost, st) != cudaSuccess)
-                return EEMD_E_CUDA;
-            if (cudaStreamSynchronize(st) != cudaSuccess) return EEMD_E_CUDA;
-            if (h.error) break;
-            if (h.active == 0) break;
-        }
-    }
+    int rc = p->exact ? launch_emd<T, true>(C, L, st, tr) : launch_emd<T, false>(C, L, st, tr);
+    if (rc) return rc;
     if (imf_sum || mode_count) {
         int64_t nmax = 0;
         for (auto& s : L.sd) nmax = std::max<int64_t>(nmax, s.n);
         dim3 g((unsigned)((nmax + 255) / 256), (unsigned)p->max_imf, (unsigned)L.sd.size());
         tr.begin(EEMD_K_REDUCE);
-        k_reduce<T><<<g, 256, 0, st>>>(C, imf_sum, mode_count);
+        k_reduce<T><<<g, 256, 0, st>>>(C.sd, C.td, C.tout, C.imfs, C.trial_count, C.max_imf, imf_sum,
+                                        mode_count);
         tr.end();
     }
     if (nsift || nmode || flags) {
         tr.begin(EEMD_K_OUTPUTS);
-        k_outputs<<<(int)((n_tasks + 255) / 256), 256, 0, st>>>(C, nsift, nmode, flags);
+        k_outputs<<<(int)((n_tasks + 255) / 256), 256, 0, st>>>(C.tout, (int)n_tasks, nsift, nmode, flags);
         tr.end();
     }
     if (resid_out) {
@@ -1313,18 +1470,10 @@ int32_t eemd_run_traced(const eemd_params* p, const void* x, const int64_t* leng
     memset(&C, 0, sizeof(C));
     C.hdr = reinterpret_cast<Header*>(base + L.o_hdr);
     C.td = reinterpret_cast<const TaskDesc*>(base + L.o_td);
-    C.ts = reinterpret_cast<TaskState*>(base + L.o_ts);
+    C.order = reinterpret_cast<const int32_t*>(base + L.o_order);
+    C.tout = reinterpret_cast<TaskOut*>(base + L.o_tout);
     C.sd = reinterpret_cast<const SignalDesc*>(base + L.o_sd);
     C.sigma = reinterpret_cast<const double*>(base + L.o_sigma);
-    C.el_task = reinterpret_cast<int32_t*>(base + L.o_el_task);
-    C.el_pref = reinterpret_cast<int32_t*>(base + L.o_el_pref);
-    C.sl_item = reinterpret_cast<int32_t*>(base + L.o_sl_item);
-    C.sl_pref = reinterpret_cast<int32_t*>(base + L.o_sl_pref);
-    C.status = reinterpret_cast<unsigned long long*>(base + L.o_status);
-    C.partial = reinterpret_cast<double2*>(base + L.o_partial);
-    C.tpref = reinterpret_cast<int2*>(base + L.o_tpref);
-    C.hedge = reinterpret_cast<double2*>(base + L.o_hedge);
-    C.redge = reinterpret_cast<double2*>(base + L.o_redge);
     C.resid = base + L.o_resid;
     C.imfs = imfs ? imfs : (void*)(base + L.o_imfs);
     C.kt = reinterpret_cast<int32_t*>(base + L.o_kt);
@@ -1335,11 +1484,14 @@ int32_t eemd_run_traced(const eemd_params* p, const void* x, const int64_t* leng
     C.noise = noise;
     C.knot_log = knot_log;
     C.mode_sifts = mode_sifts;
-    C.TT = L.TT;
-    C.KC = L.KC;
+    C.slot_knots = L.slot_knots;
+    C.slot_M = L.slot_M;
+    C.segcap = L.segcap;
+    C.kcap = L.kcap;
     C.n_tasks = (int32_t)L.td.size();
     C.n_signals = n_signals;
     C.trial_count = trial_count;
+    C.csize = L.csize;
     C.max_sifts = p->max_sifts;
     C.max_imf = p->max_imf;
     C.min_extrema = p->min_extrema;
@@ -1349,21 +1501,21 @@ int32_t eemd_run_traced(const eemd_params* p, const void* x, const int64_t* leng
     C.tile = L.tile;
     C.B = L.B;
     C.S = L.S;
+    C.scr_rows = L.scr_rows;
     C.tau = p->tau;
     C.seed = p->seed;
     C.watchdog = p->watchdog != 0 ? p->watchdog : (1LL << 24);
 
-    // tables and zeroed control state
     if (cudaMemsetAsync(base + L.o_hdr, 0, sizeof(Header), st) != cudaSuccess) return EEMD_E_CUDA;
-    if (cudaMemsetAsync(base + L.o_status, 0, sizeof(unsigned long long) * 2 * L.TT, st) != cudaSuccess)
-        return EEMD_E_CUDA;
     if (cudaMemcpyAsync(base + L.o_td, L.td.data(), sizeof(TaskDesc) * L.td.size(), cudaMemcpyHostToDevice,
                         st) != cudaSuccess)
+        return EEMD_E_CUDA;
+    if (cudaMemcpyAsync(base + L.o_order, L.order.data(), sizeof(int32_t) * L.order.size(),
+                        cudaMemcpyHostToDevice, st) != cudaSuccess)
         return EEMD_E_CUDA;
     if (cudaMemcpyAsync(base + L.o_sd, L.sd.data(), sizeof(SignalDesc) * L.sd.size(),
                         cudaMemcpyHostToDevice, st) != cudaSuccess)
         return EEMD_E_CUDA;
-    // pageable-host copies above are staged before returning; keep L alive to the sync below anyway
     if (knot_log) {
         const size_t nb = sizeof(int32_t) * 2 * L.td.size() * (size_t)p->max_imf * p->max_sifts;
         if (cudaMemsetAsync(knot_log, 0xff, nb, st) != cudaSuccess) return EEMD_E_CUDA;
@@ -1384,6 +1536,7 @@ int32_t eemd_run_traced(const eemd_params* p, const void* x, const int64_t* leng
     Header h;
     if (cudaMemcpy(&h, C.hdr, sizeof(Header), cudaMemcpyDeviceToHost) != cudaSuccess) return EEMD_E_CUDA;
     if (h.error) return h.error;
+    if (h.n_done != C.n_tasks) return EEMD_E_CUDA;
     return EEMD_OK;
 }
 

@@ -2,80 +2,65 @@
 //
 // Work model.  A *task* is one (signal, trial) pair: the full EMD of one
 // perturbed signal (emd_ref.py:108-156 emd_1d; emd_gpu.py:120-285 runs the
-// same loop with one CUDA block per trial).  Here every task advances by one
-// *step* per round of three launches:
+// same loop with one CUDA block per trial).  Tasks are independent, so the
+// whole ensemble runs as ONE persistent kernel (k_emd): a thread-block cluster
+// of C CTAs takes a task from a queue and carries it through every IMF and
+// every sift before taking the next one.  CTA r of the cluster owns the
+// contiguous sample segment [r*seg, (r+1)*seg).  Per sift:
 //
-//   k_plan   one CTA: list the live tasks, their tiles and their solve chunks
-//   k_solve  decay-seamed block-Thomas solve of both envelope systems of
-//            every task that is sifting (emd_ref.py:31-65, emd_gpu_v5_dsbt.py:51-74)
-//   k_eval   fused pass over the task's samples, one tile per CTA: spline
-//            evaluation of both envelopes, mean subtraction, SD partial sums,
-//            extrema detection + compaction of the *next* sift's knots
-//            (decoupled look-back across the tiles of the task), IMF store,
-//            residual update and the per-task stop decision (last tile done)
+//   solve   both envelope systems, decay-seamed block Thomas: the windows of
+//           each envelope are split over the cluster's CTAs; knots are staged
+//           in shared memory; second derivatives go to global memory
+//           (emd_ref.py:31-65, emd_gpu_v5_dsbt.py:51-74)
+//   barrier.cluster (release/acquire)
+//   sweep   each CTA streams its segment tile by tile: spline evaluation of
+//           both envelopes, mean subtraction, SD partial sums, strict extrema
+//           of the new values compacted in time order into the segment's own
+//           knot list (no cross-CTA prefix is needed: a knot index is the
+//           segment prefix plus the position in the segment list), IMF store,
+//           residual update
+//   publish segment results (counts, SD partials, edge samples) in shared
+//           memory; barrier.cluster; every CTA reads all C entries through
+//           distributed shared memory and takes the same stop decision
 //
-// A task's step is one of: INIT (noise injection + first extrema scan),
-// SIFT (one sift; the last allowed sift of an IMF also closes the IMF),
-// TRANS (close an IMF that stopped on the SD rule or on missing extrema).
+// Knot lists, second derivatives and solve scratch live in per-cluster-slot
+// regions of the workspace; residuals and IMFs live per task.
 #pragma once
 #include <stdint.h>
 #include <cuda_runtime.h>
 
 namespace eemd {
 
+constexpr int THREADS = 256;      // threads per CTA of k_emd
+constexpr int MAXC = 16;          // largest cluster (non-portable size)
+constexpr int FAST_B = 8;         // owned rows per window, fast solve (register resident)
+constexpr int SOLVE_CAP = 4352;   // knots staged in shared memory per solve pass
+
 enum Phase : int32_t { PH_DONE = 0, PH_INIT = 1, PH_SIFT = 2, PH_TRANS = 3 };
-
-// status word of the decoupled look-back: [63:62] flag, [61:31] maxima, [30:0] minima
-enum : uint64_t { LB_EMPTY = 0, LB_AGG = 1, LB_INC = 2 };
-
-constexpr int EVAL_THREADS = 256;
-constexpr int SOLVE_THREADS = 128;
-constexpr int PLAN_THREADS = 1024;
+enum TileMode : int32_t { TM_INIT = 0, TM_SIFT = 1, TM_LAST = 2, TM_TRANS = 3 };
 
 struct Header {
     int32_t error;        // first EEMD_E_* raised on the device (0 = none)
     int32_t error_info;   // task index / detail of the first error
-    int32_t active;       // tasks not DONE after the last plan
-    int32_t step;         // plan counter (parity selects the look-back plane)
-    uint32_t eval_ticket;
-    uint32_t solve_ticket;
-    int32_t eval_total;   // tiles to process this step
-    int32_t solve_total;  // solve chunks this step
-    int32_t n_elist;
-    int32_t n_slist;
-    int32_t pad[6];
+    int32_t next_task;    // work queue head (index into the task order)
+    int32_t n_done;       // tasks finished
+    int32_t wd_flag;      // the watchdog test mode waits on this word; nothing sets it
+    int32_t pad[11];
 };
 
 struct TaskDesc {
     int64_t x_off;      // element offset of the task's source signal in x
     int64_t s_off;      // element offset in the residual array (and resid_out)
     int64_t imf_off;    // element offset of IMF slot 0 (slot m at + m*n)
-    int64_t k_off;      // offset in each knot plane (capacity kcap)
-    int64_t scr_off;    // double2 offset of the solve scratch, env 0
-    int64_t scr_env;    // double2 size of one env's scratch
     int64_t noise_off;  // element offset in the injected noise array
     int32_t n;          // samples
-    int32_t kcap;       // knot capacity per envelope (incl. 2 mirror knots)
-    int32_t tile_off;   // offset in the per-tile arrays
-    int32_t ntiles;
     int32_t signal;
     int32_t trial;      // absolute trial index (Philox counter)
+    int32_t seg;        // samples per segment (multiple of 32)
 };
 
-struct TaskState {
-    int32_t phase;
-    int32_t imf;            // index of the IMF being built
-    int32_t sift;           // index of the next sift of that IMF
-    int32_t kpar;           // knot/prefix plane holding the current knots
-    int32_t pmax, pmin;     // current knot counts (knots of the pending sift)
-    int32_t src_resid;      // the pending sift reads h from the residual
-    int32_t imf_from_resid; // pending TRANS: the IMF is the residual itself (0 sifts)
-    int32_t nsift_total;
-    int32_t nmode;
-    int32_t mode_sifts_cur;
-    int32_t flags;          // bit0: IMF slots exhausted while extrema remained
-    uint32_t done_count;    // tiles of this step finished (last one finalises)
-    int32_t pad[3];
+struct TaskOut {
+    int32_t nsift, nmode, flags, pad;
 };
 
 struct SignalDesc {
@@ -90,33 +75,27 @@ struct SignalDesc {
 struct Ctx {
     Header* hdr;
     const TaskDesc* td;
-    TaskState* ts;
+    const int32_t* order;         // task processing order (longest first)
+    TaskOut* tout;
     const SignalDesc* sd;
     const double* sigma;          // per signal: eps*std(x) (Philox noise scale)
-    int32_t* el_task;             // eval list: task
-    int32_t* el_pref;             // eval list: tile prefix (n_elist+1)
-    int32_t* sl_item;             // solve list: task*2+env
-    int32_t* sl_pref;             // solve list: chunk prefix
-    unsigned long long* status;   // [2][TT] look-back words
-    double2* partial;             // [TT] (num, den)
-    int2* tpref;                  // [2][TT] knots before the tile (max, min)
-    double2* hedge;               // [2][TT] h at the tile's first/last sample
-    double2* redge;               // [2][TT] residual at the tile's first/last sample
     void* resid;                  // residual per task (dtype)
     void* imfs;                   // IMF slots per task (dtype)
-    int32_t* kt;                  // [2 parity][2 env][KC] knot sample index
-    void* ky;                     // [2 parity][2 env][KC] knot value (dtype)
-    double* M;                    // [2 env][KC] spline second derivatives (mirror space)
-    double2* scr;                 // solve scratch (c, d') per window row
+    int32_t* kt;                  // per slot: [2 parity][2 env][C seg][segcap] knot sample index
+    void* ky;                     // per slot: same layout, knot value (dtype)
+    double* M;                    // per slot: [2 env][kcap] second derivatives (mirror space)
+    double2* scr;                 // exact-mode solve scratch: [rows][grid threads]
     const void* x;
     const void* noise;
     int32_t* knot_log;            // optional [task][max_imf][max_sifts][2]
     int32_t* mode_sifts;          // optional [task][max_imf]
-    int64_t TT;                   // total tiles
-    int64_t KC;                   // knot plane size
-    int32_t n_tasks, n_signals, trial_count;
+    int64_t slot_knots;           // kt/ky elements per slot
+    int64_t slot_M;               // M doubles per slot
+    int32_t segcap;               // knots of one kind per segment list
+    int32_t kcap;                 // knots per envelope in mirror space (M plane size)
+    int32_t n_tasks, n_signals, trial_count, csize;
     int32_t max_sifts, max_imf, min_extrema, end_mode, rules, noise_mode;
-    int32_t tile, B, S;
+    int32_t tile, B, S, scr_rows;
     double tau;
     uint64_t seed;
     long long watchdog;

@@ -138,12 +138,9 @@ int32_t eemd_run(const eemd_params* p, const void* x, const int64_t* lengths,
 
 /* Kernel kinds of eemd_run_traced() */
 #define EEMD_K_SIGMA   0  /* per-signal eps*std(x) */
-#define EEMD_K_INIT    1  /* task states */
-#define EEMD_K_PLAN    2  /* per-step work lists */
-#define EEMD_K_SOLVE   3  /* decay-seamed block-Thomas envelope solve */
-#define EEMD_K_EVAL    4  /* fused evaluation / subtraction / SD / extrema pass */
-#define EEMD_K_REDUCE  5  /* trial-ordered ensemble sum */
-#define EEMD_K_OUTPUTS 6  /* per-task counters */
+#define EEMD_K_EMD     1  /* persistent cluster kernel: every IMF and sift of every task */
+#define EEMD_K_REDUCE  2  /* trial-ordered ensemble sum */
+#define EEMD_K_OUTPUTS 3  /* per-task counters */
 #define EEMD_KERNEL_KINDS 8
 
 typedef struct eemd_kernel_times {

@@ -190,7 +190,7 @@ def test_determinism_and_seed(sweep):
     assert np.max(np.abs(a.imfs[:m] - c.imfs[:m])) > 0
 
 
-@pytest.mark.parametrize("tile", [256, 1024, 4096])
+@pytest.mark.parametrize("tile", [256, 512, 1024])
 def test_tile_size_invariance(sweep, tile):
     """Launch shape must not change results: the per-sample arithmetic is
     tile-independent (only the SD sum order moves)."""
