@@ -59,6 +59,8 @@ class EemdParams(ctypes.Structure):
         ("knots_per_block", c_int32),
         ("halo", c_int32),
         ("watchdog", c_int64),
+        ("cluster_size", c_int32),
+        ("reserved", c_int32),
     ]
 
 

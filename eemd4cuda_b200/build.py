@@ -7,6 +7,9 @@ Outputs (git-ignored, shipped next to the sources):
     eemd4cuda_b200/lib/libeemd_b200_checked.so  -DEEMD_CHECKED: every staged
         index is range-checked on the device and a violation is reported as an
         error status instead of an out-of-bounds access
+    eemd4cuda_b200/lib/libeemd_b200_trace.so    -DEEMD_TRACE: the persistent
+        kernel sums clock64() cycles per phase into the workspace header
+        (eemd4cuda_b200.trace reads them)
 """
 from __future__ import annotations
 
@@ -48,7 +51,8 @@ def build(force: bool = False, verbose: bool = False) -> list[Path]:
     LIB.mkdir(exist_ok=True)
     deps = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
     outs = []
-    for name, extra in (("libeemd_b200.so", []), ("libeemd_b200_checked.so", ["-DEEMD_CHECKED"])):
+    for name, extra in (("libeemd_b200.so", []), ("libeemd_b200_checked.so", ["-DEEMD_CHECKED"]),
+                        ("libeemd_b200_trace.so", ["-DEEMD_TRACE"])):
         out = LIB / name
         outs.append(out)
         if not force and not _stale(out, deps):

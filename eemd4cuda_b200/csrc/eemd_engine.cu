@@ -57,6 +57,27 @@ __device__ __forceinline__ double fast_rcp(double x) {
     return fma(y, e, y);
 }
 
+// Asynchronous global->shared copies (sm_80+ cp.async): a thread issues its
+// copies, commits them as a group and later waits for the group.
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+template <typename T>
+__device__ __forceinline__ void cp_async_el(T* smem, const T* gmem) {
+    if (sizeof(T) == 8) cp_async8(smem, gmem);
+    else cp_async4(smem, gmem);
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // emd_ref.py:67-75 (and emd_gpu.py:96-100), reference operation order
 __device__ __forceinline__ double spline_exact(double t, double tl, double tr, double yl, double yr,
                                                double Ml, double Mr) {
@@ -168,6 +189,7 @@ struct TaskSm {
     int P[2];                  // current knot totals
     int pref[2][MAXC + 1];     // current knots before each segment
     int mir[2], p2[2], tfirst[2], tlast[2];
+    double yfirst[2], ylast[2];  // values of the virtual mirror knots
     double cval[2];            // constant envelope when P == 1
     // sweep scalars
     int left_knot[2];
@@ -177,15 +199,18 @@ struct TaskSm {
 };
 
 struct Smem {
-    double* h;       // [TILE+2] old h (index j+1 = tile sample j; 0 and tl+1 are halos)
-    double* f;       // [TILE+2] new values
-    double* r;       // [TILE+2] residual
-    int* kt;         // [2][cap] knot sample index
-    double* c0;      // [2][cap] exact: knot value;          fast: monomial c0 (= knot value)
-    double* c1;      // [2][cap] exact: second derivative;   fast: monomial c1
+    void* hT[2];     // [TILE+2] old h, storage type (double buffer; index j+1 = sample j)
+    void* rT[2];     // [TILE+2] residual, storage type (double buffer)
+    double* f;       // [TILE+2] new values (0 and tl+1 are the halo samples)
+    double* g;       // [TILE+2] new residual (TM_LAST)
+    int* kt;         // [2][cap] staged knot sample index
+    void* ky;        // [2][cap] staged knot value, storage type
+    double* M;       // [2][cap] staged second derivative
+    double* c1;      // [2][cap] fast: monomial c1
     double* c2;      // [2][cap] fast: monomial c2
     double* c3;      // [2][cap] fast: monomial c3
     int* skt;        // solve staging (padded): knot sample index
+    void* sky;       // solve staging (padded): knot value, storage type
     double* ssl;     // solve staging (padded): slope of the interval starting at the knot
     int cap;
 };
@@ -195,28 +220,42 @@ constexpr int NWARP = THREADS / 32;
 
 __host__ __device__ inline int stage_pad(int k) { return k + (k >> 4); }
 
-__host__ __device__ inline size_t smem_bytes(int TILE) {
-    const int cap = (TILE >> 1) + 8;
-    size_t sweep = (size_t)3 * (TILE + 2) * 8 + (size_t)2 * cap * (4 + 4 * 8);
-    size_t solve = (size_t)stage_pad(SOLVE_CAP) * (4 + 8) + 64;
+__host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
+
+__host__ __device__ inline size_t smem_bytes(int TILE, int bt) {
+    const size_t cap = (size_t)(TILE >> 1) + 8;
+    const size_t tile = align16((size_t)(TILE + 2) * bt);
+    const size_t sweep = 4 * tile + 2 * align16((size_t)(TILE + 2) * 8) + 2 * align16(cap * 4) +
+                         2 * align16(cap * bt) + 8 * align16(cap * 8);
+    const size_t sp = (size_t)stage_pad(SOLVE_CAP);
+    const size_t solve = align16(sp * 8) + align16(sp * 4) + align16(sp * bt);
     return sweep > solve ? sweep : solve;
 }
 
+template <typename T>
 __device__ __forceinline__ Smem carve(unsigned char* base, int TILE) {
     Smem m;
-    m.cap = (TILE >> 1) + 8;
-    double* d = reinterpret_cast<double*>(base);
-    m.h = d;
-    m.f = m.h + (TILE + 2);
-    m.r = m.f + (TILE + 2);
-    m.c0 = m.r + (TILE + 2);
-    m.c1 = m.c0 + 2 * m.cap;
-    m.c2 = m.c1 + 2 * m.cap;
-    m.c3 = m.c2 + 2 * m.cap;
-    m.kt = reinterpret_cast<int*>(m.c3 + 2 * m.cap);
+    const size_t cap = (size_t)(TILE >> 1) + 8;
+    m.cap = (int)cap;
+    const size_t tile = align16((size_t)(TILE + 2) * sizeof(T));
+    unsigned char* p = base;
+    m.hT[0] = p; p += tile;
+    m.hT[1] = p; p += tile;
+    m.rT[0] = p; p += tile;
+    m.rT[1] = p; p += tile;
+    m.f = reinterpret_cast<double*>(p); p += align16((size_t)(TILE + 2) * 8);
+    m.g = reinterpret_cast<double*>(p); p += align16((size_t)(TILE + 2) * 8);
+    m.kt = reinterpret_cast<int*>(p); p += 2 * align16(cap * 4);
+    m.ky = p; p += 2 * align16(cap * sizeof(T));
+    m.M = reinterpret_cast<double*>(p); p += 2 * align16(cap * 8);
+    m.c1 = reinterpret_cast<double*>(p); p += 2 * align16(cap * 8);
+    m.c2 = reinterpret_cast<double*>(p); p += 2 * align16(cap * 8);
+    m.c3 = reinterpret_cast<double*>(p);
     // solve staging overlays the sweep buffers (used in a different phase)
-    m.ssl = d;
-    m.skt = reinterpret_cast<int*>(d + stage_pad(SOLVE_CAP) + 2);
+    const size_t sp = (size_t)stage_pad(SOLVE_CAP);
+    m.ssl = reinterpret_cast<double*>(base);
+    m.skt = reinterpret_cast<int*>(base + align16(sp * 8));
+    m.sky = base + align16(sp * 8) + align16(sp * 4);
     return m;
 }
 
@@ -244,15 +283,43 @@ __device__ __forceinline__ int seg_of(const int* pref, int csize, int i) {
     return lo;
 }
 
-template <typename T>
-__device__ __forceinline__ void real_knot(const Ctx& C, const Slot& sl, const TaskSm& S, int env, int i,
-                                          int& t, double& y) {
+// element offset of real knot i in the current knot plane
+__device__ __forceinline__ int64_t real_off(const Ctx& C, const TaskSm& S, int env, int i) {
     const int* pr = S.pref[env];
     int r = S.rank;  // most lookups fall in the CTA's own segment
     if (i < pr[r] || i >= pr[r + 1]) r = seg_of(pr, S.csize, i);
-    const int64_t o = knot_index(C, S.kpar, env, r, i - pr[r]);
+    return knot_index(C, S.kpar, env, r, i - pr[r]);
+}
+
+template <typename T>
+__device__ __forceinline__ void real_knot(const Ctx& C, const Slot& sl, const TaskSm& S, int env, int i,
+                                          int& t, double& y) {
+    const int64_t o = real_off(C, S, env, i);
     t = __ldcg(sl.kt + o);
     y = (double)__ldcg(static_cast<const T*>(sl.ky) + o);
+}
+
+// Stage mirror-space knot i2 into shared memory: an asynchronous copy for a
+// real knot, a direct store for a virtual mirror knot.
+template <typename T>
+__device__ __forceinline__ void stage_knot(const Ctx& C, const Slot& sl, const TaskSm& S, int env, int i2,
+                                           int* kt_s, T* ky_s) {
+    if (S.mir[env]) {
+        if (i2 == 0) {
+            *kt_s = S.tfirst[env];
+            *ky_s = (T)S.yfirst[env];
+            return;
+        }
+        if (i2 == S.P[env] + 1) {
+            *kt_s = S.tlast[env];
+            *ky_s = (T)S.ylast[env];
+            return;
+        }
+        i2 -= 1;
+    }
+    const int64_t o = real_off(C, S, env, i2);
+    cp_async4(kt_s, sl.kt + o);
+    cp_async_el<T>(ky_s, static_cast<const T*>(sl.ky) + o);
 }
 
 // Knot i2 in "mirror space" (emd_ref.py:92-96): with mir=1 the list is
@@ -456,17 +523,18 @@ __device__ void solve_task(const Ctx& C, const Slot& sl, TaskSm& S, const Smem& 
             const int rlo = max(0, wbase * Bw - C.S);
             const int rhi = min(n - 1, min(n, wend * Bw) - 1 + C.S);
             const int kcount = rhi + 3 - rlo;  // knots rlo .. rhi+2
+            T* sky = static_cast<T*>(sm.sky);
             __syncthreads();
-            for (int k = tid; k < kcount; k += THREADS) {
-                int ta, tb;
-                double ya, yb;
-                knot2<T>(C, sl, S, env, rlo + k, ta, ya);
-                sm.skt[stage_pad(k)] = ta;
-                if (k + 1 < kcount) {
-                    knot2<T>(C, sl, S, env, rlo + k + 1, tb, yb);
-                    // emd_ref.py:47: (y_{q+1}-y_q)/H_q, the same IEEE division
-                    sm.ssl[stage_pad(k)] = (yb - ya) / (double)(tb - ta);
-                }
+            for (int k = tid; k < kcount; k += THREADS)
+                stage_knot<T>(C, sl, S, env, rlo + k, &sm.skt[stage_pad(k)], &sky[stage_pad(k)]);
+            cp_async_commit();
+            cp_async_wait<0>();
+            __syncthreads();
+            for (int k = tid; k + 1 < kcount; k += THREADS) {
+                const int ta = sm.skt[stage_pad(k)], tb = sm.skt[stage_pad(k + 1)];
+                const double ya = (double)sky[stage_pad(k)], yb = (double)sky[stage_pad(k + 1)];
+                // emd_ref.py:47: (y_{q+1}-y_q)/H_q, the same IEEE division
+                sm.ssl[stage_pad(k)] = (yb - ya) / (double)(tb - ta);
             }
             __syncthreads();
             const int w = wbase + tid;
@@ -522,22 +590,28 @@ __device__ __forceinline__ void block_scan2(int a, int b, int& ea, int& eb, int&
 
 // Envelope value at t from the staged intervals; `cless` = knots strictly
 // before t in mirror space (emd_ref.py:70 searchsorted - 1, clipped).
-template <bool EXACT>
+template <typename T, bool EXACT>
 __device__ __forceinline__ double env_at(const Smem& sm, int env, int cless, int t, int lo2, int p2) {
-    int idx2 = max(0, min(cless - 1, p2 - 2));
+    const int idx2 = max(0, min(cless - 1, p2 - 2));
     const int k = env * sm.cap + (idx2 - lo2);
+    const T* ky = static_cast<const T*>(sm.ky);
     if (EXACT) {
-        return spline_exact((double)t, (double)sm.kt[k], (double)sm.kt[k + 1], sm.c0[k], sm.c0[k + 1],
-                            sm.c1[k], sm.c1[k + 1]);
+        return spline_exact((double)t, (double)sm.kt[k], (double)sm.kt[k + 1], (double)ky[k],
+                            (double)ky[k + 1], sm.M[k], sm.M[k + 1]);
     }
     const double s = (double)(t - sm.kt[k]);
-    return fma(s, fma(s, fma(s, sm.c3[k], sm.c2[k]), sm.c1[k]), sm.c0[k]);
+    return fma(s, fma(s, fma(s, sm.c3[k], sm.c2[k]), sm.c1[k]), (double)ky[k]);
 }
 
 __device__ __forceinline__ int mirror_adj(const TaskSm& S, int env, int t) {
     return S.mir[env] ? (S.tfirst[env] < t ? 1 : 0) + (S.tlast[env] < t ? 1 : 0) : 0;
 }
 
+// The sweep streams the CTA's segment in tiles of TILE samples; thread u owns
+// the run of TILE/THREADS consecutive samples starting at u*TILE/THREADS.
+// The next tile's samples are copied to shared memory (cp.async) while the
+// current one is processed; the knots a tile needs are staged with one batch
+// of asynchronous copies.
 template <typename T, bool EXACT>
 __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, const Smem& sm,
                       cg::cluster_group& cl) {
@@ -548,12 +622,14 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, const Sm
     const int mode = S.mode, n = S.n, s0 = S.s0, s1 = S.s1, rank = S.rank;
     const bool sifting = (mode == TM_SIFT || mode == TM_LAST);
     const bool uses_r = (mode == TM_LAST || mode == TM_TRANS);
+    const bool needs_h = sifting || (mode == TM_TRANS && !S.imf_from_resid);
     const int q = S.step & 1;
     const TaskDesc d = C.td[S.task];
     T* resid = static_cast<T*>(C.resid) + d.s_off;
     T* imf_m = static_cast<T*>(C.imfs) + d.imf_off + (int64_t)min(S.imf, C.max_imf - 1) * n;
     const T* src = (sifting && S.src_resid) ? resid : imf_m;
     const int np = S.kpar ^ 1;
+    T* kyS = static_cast<T*>(sm.ky);
     double num = 0.0, den = 0.0;
 
     if (tid == 0) {
@@ -562,48 +638,80 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, const Sm
         S.hold_m1 = S.hold_m2 = S.rold_m1 = S.hold_p = S.rold_p = 0.0;
         if (mode != TM_INIT) {
             // neighbours' edge samples from their previous step (distributed shared memory)
+            const bool hres = sifting && S.src_resid;
             if (s0 > 0) {
                 const Xchg* xl = cl.map_shared_rank(&X[q ^ 1], rank - 1);
-                S.hold_m1 = S.src_resid ? xl->rl[1] : xl->hl[1];
-                S.hold_m2 = S.src_resid ? xl->rl[0] : xl->hl[0];
+                S.hold_m1 = hres ? xl->rl[1] : xl->hl[1];
+                S.hold_m2 = hres ? xl->rl[0] : xl->hl[0];
                 S.rold_m1 = xl->rl[1];
             }
             if (s1 < n) {
                 const Xchg* xr = cl.map_shared_rank(&X[q ^ 1], rank + 1);
-                S.hold_p = S.src_resid ? xr->rf[0] : xr->hf[0];
+                S.hold_p = hres ? xr->rf[0] : xr->hf[0];
                 S.rold_p = xr->rf[0];
             }
         }
     }
     __syncthreads();
 
-    for (int t0 = s0; t0 < s1; t0 += TILE) {
+    // copies samples [t0p, t0p+tl] (the extra one when it is still this segment's) to buffer b
+    auto prefetch = [&](int t0p, int b) {
+        const int tlp = min(TILE, s1 - t0p);
+        const int cnt = (t0p + tlp < s1) ? tlp + 1 : tlp;
+        T* hb = static_cast<T*>(sm.hT[b]);
+        T* rb = static_cast<T*>(sm.rT[b]);
+        for (int j = tid; j < cnt; j += THREADS) {
+            if (needs_h) cp_async_el<T>(hb + 1 + j, src + t0p + j);
+            if (uses_r) cp_async_el<T>(rb + 1 + j, resid + t0p + j);
+        }
+        cp_async_commit();
+    };
+    const bool streams = needs_h || uses_r;
+    if (streams) prefetch(s0, 0);
+
+    int buf = 0;
+    for (int t0 = s0; t0 < s1; t0 += TILE, buf ^= 1) {
         const int tl = min(TILE, s1 - t0);
         const bool first = (t0 == s0), last = (t0 + tl == s1);
         const int j0 = tid * run;
-        // ---------------- (a) loads ----------------
-        double hv[RUN_MAX], rv[RUN_MAX], fv[RUN_MAX], gv[RUN_MAX];
-#pragma unroll
-        for (int i = 0; i < RUN_MAX; ++i) {
-            hv[i] = rv[i] = fv[i] = gv[i] = 0.0;
-            const int j = j0 + i;
-            if (i < run && j < tl) {
-                if (sifting) { hv[i] = (double)src[t0 + j]; sm.h[1 + j] = hv[i]; }
-                if (uses_r) { rv[i] = (double)resid[t0 + j]; sm.r[1 + j] = rv[i]; }
+        T* hb = static_cast<T*>(sm.hT[buf]);
+        T* rb = static_cast<T*>(sm.rT[buf]);
+        // ---------------- (a) this tile's samples (prefetched), next tile's prefetch ----------------
+        if (streams) {
+            if (!last) {
+                prefetch(t0 + TILE, buf ^ 1);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
             }
         }
         if (tid == 0) {
             if (sifting) {
-                sm.h[0] = S.hold_m1;
-                sm.h[tl + 1] = (t0 + tl < n) ? (last ? S.hold_p : (double)src[t0 + tl]) : 0.0;
+                hb[0] = (T)S.hold_m1;
+                if (last) hb[tl + 1] = (T)((t0 + tl < n) ? S.hold_p : 0.0);
+            } else if (needs_h) {  // TM_TRANS: the closed IMF at the halo samples
+                hb[0] = (first && t0 > 0) ? __ldcg(imf_m + t0 - 1) : (T)0;
+                if (last) hb[tl + 1] = (t0 + tl < n) ? __ldcg(imf_m + t0 + tl) : (T)0;
             }
             if (uses_r) {
-                sm.r[0] = first ? S.rold_m1 : S.g_m1;
-                sm.r[tl + 1] = (t0 + tl < n) ? (last ? S.rold_p : (double)resid[t0 + tl]) : 0.0;
+                if (first) rb[0] = (T)S.rold_m1;
+                if (last) rb[tl + 1] = (T)((t0 + tl < n) ? S.rold_p : 0.0);
             }
-            if (!first) sm.f[0] = S.f_m1;
+            if (!first) {
+                sm.f[0] = S.f_m1;
+                sm.g[0] = S.g_m1;
+            }
         }
         __syncthreads();
+        double hv[RUN_MAX], rv[RUN_MAX], fv[RUN_MAX], gv[RUN_MAX];
+#pragma unroll
+        for (int i = 0; i < RUN_MAX; ++i) {
+            const int j = j0 + i;
+            const bool ok = (i < run && j < tl);
+            hv[i] = (ok && needs_h) ? (double)hb[1 + j] : 0.0;
+            rv[i] = (ok && uses_r) ? (double)rb[1 + j] : 0.0;
+            fv[i] = gv[i] = 0.0;
+        }
 
         // ---------------- (b) current knots: strict extrema of h in the run ----------------
         unsigned kmx = 0u, kmn = 0u;
@@ -613,7 +721,7 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, const Sm
             for (int i = 0; i < RUN_MAX; ++i) {
                 const int j = j0 + i, t = t0 + j;
                 if (i < run && j < tl && t >= 1 && t <= n - 2) {
-                    const double a = sm.h[j], c = sm.h[j + 2], v = hv[i];
+                    const double a = (double)hb[j], c = (double)hb[j + 2], v = hv[i];
                     if (v > a && v > c) kmx |= 1u << i;
                     if (v < a && v < c) kmn |= 1u << i;
                 }
@@ -622,67 +730,63 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, const Sm
             block_scan2(__popc(kmx), __popc(kmn), ex, en, tx, tn, s_w1);
             kc[0] = tx;
             kc[1] = tn;
+            bool bad = false;
 #pragma unroll
             for (int env = 0; env < 2; ++env) {
                 kb[env] = S.pref[env][rank] + S.run_cur[env];
-                const int P = S.P[env];
-                if (P >= 2) {
+                if (S.P[env] >= 2) {
                     lo2[env] = max(0, S.mir[env] + kb[env] - 2);
                     hi2[env] = min(S.p2[env] - 1, S.mir[env] + kb[env] + kc[env] + 1);
                 }
-            }
-            cl0[0] = kb[0] + ex;
-            cl0[1] = kb[1] + en;
-            if (tid == 0) {
-                for (int env = 0; env < 2; ++env) {
-                    if (hi2[env] - lo2[env] + 1 > cap || kb[env] + kc[env] > S.P[env]) {
-                        raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
-                    }
+                if (hi2[env] - lo2[env] + 1 > cap || kb[env] + kc[env] > S.P[env]) {
+                    bad = true;
+                    hi2[env] = lo2[env] - 1;
                 }
             }
-            for (int env = 0; env < 2; ++env)
-                if (hi2[env] - lo2[env] + 1 > cap || kb[env] + kc[env] > S.P[env]) hi2[env] = lo2[env] - 1;
+            if (bad && tid == 0) raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
+            cl0[0] = kb[0] + ex;
+            cl0[1] = kb[1] + en;
             // ---------------- (c) stage the intervals the tile uses ----------------
             const int n0 = hi2[0] - lo2[0] + 1, n1 = hi2[1] - lo2[1] + 1;
             for (int k = tid; k < n0 + n1; k += THREADS) {
                 const int env = (k >= n0) ? 1 : 0;
                 const int kk = k - env * n0;
-                const int cnt = env ? n1 : n0;
                 const int i2 = lo2[env] + kk;
-                const double* M2 = sl.M + (int64_t)env * C.kcap;
-                int ta;
-                double ya;
-                knot2<T>(C, sl, S, env, i2, ta, ya);
-                const double Ma = __ldcg(M2 + i2);
                 const int o = env * cap + kk;
-                sm.kt[o] = ta;
-                sm.c0[o] = ya;
-                if (EXACT) {
-                    sm.c1[o] = Ma;
-                } else if (kk + 1 < cnt) {
-                    // monomial form of interval [i2, i2+1]: y + s(c1 + s(c2 + s c3)), s = t - t_i2,
-                    // c1 = (y'-y)/h - h(2M + M')/6, c2 = M/2, c3 = (M'-M)/(6h)
-                    int tb;
-                    double yb;
-                    knot2<T>(C, sl, S, env, i2 + 1, tb, yb);
-                    const double Mb = __ldcg(M2 + i2 + 1);
-                    const double h = (double)(tb - ta);
-                    const double ih = fast_rcp(h);
-                    sm.c1[o] = fma(yb - ya, ih, -h * fma(2.0, Ma, Mb) * (1.0 / 6.0));
-                    sm.c2[o] = 0.5 * Ma;
-                    sm.c3[o] = (Mb - Ma) * ih * (1.0 / 6.0);
-                }
+                stage_knot<T>(C, sl, S, env, i2, &sm.kt[o], &kyS[o]);
+                cp_async8(&sm.M[o], sl.M + (int64_t)env * C.kcap + i2);
             }
+            cp_async_commit();
             if (tid == 0) {
                 // is t0-1 a knot of each kind? (only the segment's first tile evaluates t0-1)
                 S.left_knot[0] = S.left_knot[1] = 0;
                 if (first && t0 - 1 >= 1 && t0 - 1 <= n - 2) {
-                    const double a = S.hold_m2, b = sm.h[0], c = sm.h[1];
+                    const double a = S.hold_m2, b = (double)hb[0], c = (double)hb[1];
                     S.left_knot[0] = (b > a) && (b > c);
                     S.left_knot[1] = (b < a) && (b < c);
                 }
             }
+            cp_async_wait<0>();
             __syncthreads();
+            if (!EXACT) {
+                // monomial form of interval [k, k+1]: y + s(c1 + s(c2 + s c3)), s = t - t_k,
+                // c1 = (y'-y)/h - h(2M + M')/6, c2 = M/2, c3 = (M'-M)/(6h)
+                for (int k = tid; k < n0 + n1; k += THREADS) {
+                    const int env = (k >= n0) ? 1 : 0;
+                    const int kk = k - env * n0;
+                    if (kk + 1 < (env ? n1 : n0)) {
+                        const int o = env * cap + kk;
+                        const double h = (double)(sm.kt[o + 1] - sm.kt[o]);
+                        const double ih = fast_rcp(h);
+                        const double Ma = sm.M[o], Mb = sm.M[o + 1];
+                        const double ya = (double)kyS[o], yb = (double)kyS[o + 1];
+                        sm.c1[o] = fma(yb - ya, ih, -h * fma(2.0, Ma, Mb) * (1.0 / 6.0));
+                        sm.c2[o] = 0.5 * Ma;
+                        sm.c3[o] = (Mb - Ma) * ih * (1.0 / 6.0);
+                    }
+                }
+                __syncthreads();
+            }
         }
 
         // ---------------- (d) new values ----------------
@@ -694,9 +798,9 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, const Sm
                 if (sifting) {
                     const double h = hv[i];
                     const double eu = (S.P[0] < 2) ? S.cval[0]
-                                      : env_at<EXACT>(sm, 0, cl[0] + mirror_adj(S, 0, t), t, lo2[0], S.p2[0]);
+                                      : env_at<T, EXACT>(sm, 0, cl[0] + mirror_adj(S, 0, t), t, lo2[0], S.p2[0]);
                     const double el = (S.P[1] < 2) ? S.cval[1]
-                                      : env_at<EXACT>(sm, 1, cl[1] + mirror_adj(S, 1, t), t, lo2[1], S.p2[1]);
+                                      : env_at<T, EXACT>(sm, 1, cl[1] + mirror_adj(S, 1, t), t, lo2[1], S.p2[1]);
                     cl[0] += (kmx >> i) & 1u;
                     cl[1] += (kmn >> i) & 1u;
                     const double m = 0.5 * (eu + el);
@@ -711,15 +815,14 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, const Sm
                     den = EXACT ? den + h * h : fma(h, h, den);
                     gv[i] = (mode == TM_LAST) ? rnd<T>(rv[i] - hn) : hn;
                 } else if (mode == TM_TRANS) {
-                    const double hvv = S.imf_from_resid ? rv[i] : (double)imf_m[t];
-                    fv[i] = rnd<T>(rv[i] - hvv);
+                    fv[i] = rnd<T>(rv[i] - (S.imf_from_resid ? rv[i] : hv[i]));
                     gv[i] = fv[i];
                 } else {  // TM_INIT
                     fv[i] = trial_input<T>(C, d, t);
                     gv[i] = fv[i];
                 }
                 sm.f[1 + j] = fv[i];
-                if (mode == TM_LAST) sm.r[1 + j] = gv[i];
+                sm.g[1 + j] = gv[i];
             }
         }
         if (tid == 0) {
@@ -744,27 +847,26 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, const Sm
                         } else {
                             const int c = (side == 0 ? kb[env] - S.left_knot[env] : kb[env] + kc[env]) +
                                           mirror_adj(S, env, t);
-                            e2[env] = env_at<EXACT>(sm, env, c, t, lo2[env], S.p2[env]);
+                            e2[env] = env_at<T, EXACT>(sm, env, c, t, lo2[env], S.p2[env]);
                         }
                     }
                     const double m = 0.5 * (e2[0] + e2[1]);
-                    fn = rnd<T>(sm.h[jj] - m);
-                    gn = (mode == TM_LAST) ? rnd<T>(sm.r[jj] - fn) : fn;
+                    fn = rnd<T>((double)hb[jj] - m);
+                    gn = (mode == TM_LAST) ? rnd<T>((double)rb[jj] - fn) : fn;
                 } else if (mode == TM_TRANS) {
-                    const double ro = sm.r[jj];
-                    const double hvv = S.imf_from_resid ? ro : (double)__ldcg(imf_m + t);
-                    fn = rnd<T>(ro - hvv);
+                    const double ro = (double)rb[jj];
+                    fn = rnd<T>(ro - (S.imf_from_resid ? ro : (double)hb[jj]));
                     gn = fn;
                 } else {
                     fn = trial_input<T>(C, d, t);
                     gn = fn;
                 }
                 sm.f[jj] = fn;
-                if (mode == TM_LAST) sm.r[jj] = gn;
+                sm.g[jj] = gn;
             }
         }
         __syncthreads();
-        const double* G = (mode == TM_LAST) ? sm.r : sm.f;  // signal whose extrema are the next knots
+        const double* G = sm.g;  // signal whose extrema are the next knots
 
         // ---------------- (e) next knots ----------------
         unsigned nmx = 0u, nmn = 0u;
@@ -821,25 +923,24 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, const Sm
         }
         // ---------------- (g) carry to the next tile, segment edges ----------------
         if (tid == 0) {
-            const double* R = (mode == TM_LAST) ? sm.r : sm.f;  // residual after the step (non-SIFT)
             if (first) {
                 S.hf0 = sm.f[1];
                 S.hf1 = (tl >= 2) ? sm.f[2] : 0.0;
-                S.rf0 = R[1];
-                S.rf1 = (tl >= 2) ? R[2] : 0.0;
+                S.rf0 = G[1];
+                S.rf1 = (tl >= 2) ? G[2] : 0.0;
             }
             if (last) {
                 Xchg& xo = X[q];
                 xo.hl[0] = (tl >= 2) ? sm.f[tl - 1] : S.f_m1;
                 xo.hl[1] = sm.f[tl];
-                xo.rl[0] = (tl >= 2) ? R[tl - 1] : S.g_m1;
-                xo.rl[1] = R[tl];
+                xo.rl[0] = (tl >= 2) ? G[tl - 1] : S.g_m1;
+                xo.rl[1] = G[tl];
             }
             S.f_m1 = sm.f[tl];
             S.g_m1 = G[tl];
             if (sifting) {
-                S.hold_m2 = (tl >= 2) ? sm.h[tl - 1] : sm.h[0];
-                S.hold_m1 = sm.h[tl];
+                S.hold_m2 = (tl >= 2) ? (double)hb[tl - 1] : (double)hb[0];
+                S.hold_m1 = (double)hb[tl];
             }
             S.run_cur[0] += kc[0];
             S.run_cur[1] += kc[1];
@@ -1004,6 +1105,8 @@ __device__ void step_setup(const Ctx& C, const Slot& sl, TaskSm& S) {
                 real_knot<T>(C, sl, S, env, P - 2, tb, yb);
                 S.tfirst[env] = 2 * t0 - t1;
                 S.tlast[env] = 2 * ta - tb;
+                S.yfirst[env] = y1;
+                S.ylast[env] = yb;
             }
         }
         if (S.p2[env] > C.kcap) raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
@@ -1025,17 +1128,32 @@ __global__ void __launch_bounds__(THREADS, 2) k_emd(Ctx C) {
     const int csize = (int)cl.num_blocks();
     const int slot = blockIdx.x / csize;
     const int tid = threadIdx.x;
-    const Smem sm = carve(smem_raw, C.tile);
+    const Smem sm = carve<T>(smem_raw, C.tile);
     Slot sl;
     sl.kt = C.kt + (int64_t)slot * C.slot_knots;
     sl.ky = static_cast<T*>(C.ky) + (int64_t)slot * C.slot_knots;
     sl.M = C.M + (int64_t)slot * C.slot_M;
 
+#ifdef EEMD_TRACE
+    unsigned long long cyc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    long long tmark = clock64();
+#define EEMD_PHASE(k)                                   \
+    do {                                                \
+        const long long now_ = clock64();               \
+        cyc[k] += (unsigned long long)(now_ - tmark);   \
+        tmark = now_;                                   \
+    } while (0)
+#else
+#define EEMD_PHASE(k) \
+    do {              \
+    } while (0)
+#endif
     for (;;) {
         if (rank == 0 && tid == 0) s_claim = atomicAdd(&C.hdr->next_task, 1);
         cl.sync();
         const int q = *cl.map_shared_rank(&s_claim, 0);
         cl.sync();
+        EEMD_PHASE(6);
         if (q >= C.n_tasks) break;
         if (tid == 0) {
             const int task = C.order[q];
@@ -1075,12 +1193,18 @@ __global__ void __launch_bounds__(THREADS, 2) k_emd(Ctx C) {
             __syncthreads();
             if (S.mode == TM_SIFT || S.mode == TM_LAST) {
                 step_setup<T>(C, sl, S);
+                EEMD_PHASE(0);
                 solve_task<T, EXACT>(C, sl, S, sm);
+                EEMD_PHASE(1);
                 cl.sync();  // second derivatives of every segment visible
+                EEMD_PHASE(2);
             }
             sweep<T, EXACT>(C, sl, S, X, sm, cl);
+            EEMD_PHASE(3);
             cl.sync();  // segment results published
+            EEMD_PHASE(4);
             decide(C, S, X, cl);
+            EEMD_PHASE(5);
         }
         if (rank == 0 && tid == 0) {
             TaskOut o;
@@ -1093,6 +1217,12 @@ __global__ void __launch_bounds__(THREADS, 2) k_emd(Ctx C) {
         }
         __syncthreads();
     }
+#ifdef EEMD_TRACE
+    if (tid == 0) {
+        for (int k = 0; k < 8; ++k) atomicAdd(&C.hdr->phase_cycles[k], cyc[k]);
+    }
+#endif
+#undef EEMD_PHASE
 }
 
 // ---------------------------------------------------------------------------
@@ -1212,6 +1342,7 @@ int check_params(const eemd_params* p) {
     if (p->tile != 0 && p->tile != 256 && p->tile != 512 && p->tile != 1024) return EEMD_E_BADARG;
     if (p->knots_per_block < 0 || p->knots_per_block > 4096 || p->halo < 0 || p->halo > 256)
         return EEMD_E_BADARG;
+    if (p->cluster_size < 0 || p->cluster_size > 8) return EEMD_E_BADARG;
     return EEMD_OK;
 }
 
@@ -1228,7 +1359,7 @@ int make_layout(const eemd_params* p, const int64_t* lengths, int n_signals, int
         nmax = std::max(nmax, lengths[s]);
         nmin = std::min(nmin, lengths[s]);
     }
-    L.csize = autotune_csize(n_tasks, nmin);
+    L.csize = p->cluster_size ? p->cluster_size : autotune_csize(n_tasks, nmin);
     L.S = p->halo ? p->halo : (p->exact ? 32 : 24);
     L.B = p->knots_per_block ? p->knots_per_block : 64;
     if (p->exact && (2 * L.S + L.B + 8 > SOLVE_CAP)) return EEMD_E_BADARG;
@@ -1343,7 +1474,7 @@ struct Tracer {
 
 template <typename T, bool EXACT>
 int launch_emd(const Ctx& C, const Layout& L, cudaStream_t st, Tracer& tr) {
-    const size_t smem = smem_bytes(L.tile);
+    const size_t smem = smem_bytes(L.tile, (int)sizeof(T));
     if (cudaFuncSetAttribute(k_emd<T, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return EEMD_E_CUDA;

@@ -34,7 +34,7 @@ namespace eemd {
 constexpr int THREADS = 256;      // threads per CTA of k_emd
 constexpr int MAXC = 16;          // largest cluster (non-portable size)
 constexpr int FAST_B = 8;         // owned rows per window, fast solve (register resident)
-constexpr int SOLVE_CAP = 4352;   // knots staged in shared memory per solve pass
+constexpr int SOLVE_CAP = 2176;   // knots staged in shared memory per solve pass
 
 enum Phase : int32_t { PH_DONE = 0, PH_INIT = 1, PH_SIFT = 2, PH_TRANS = 3 };
 enum TileMode : int32_t { TM_INIT = 0, TM_SIFT = 1, TM_LAST = 2, TM_TRANS = 3 };
@@ -46,6 +46,9 @@ struct Header {
     int32_t n_done;       // tasks finished
     int32_t wd_flag;      // the watchdog test mode waits on this word; nothing sets it
     int32_t pad[11];
+    // -DEEMD_TRACE builds: SM cycles spent per phase, summed over CTAs
+    // (0 setup, 1 solve, 2 barrier after solve, 3 sweep, 4 barrier after sweep, 5 decide, 6 claim)
+    unsigned long long phase_cycles[8];
 };
 
 struct TaskDesc {

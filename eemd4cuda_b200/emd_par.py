@@ -78,6 +78,7 @@ class EngineConfig:
     knots_per_block: int = 0
     halo: int = 0
     watchdog: int = 0
+    cluster_size: int = 0
 
 
 _RULES = {"ref": L.EEMD_RULES_REF, "numba": L.EEMD_RULES_NUMBA}
@@ -133,6 +134,7 @@ def make_params(*, dtype=np.float64, noise_mode=L.EEMD_NOISE_NONE, eps=0.2, seed
     p.knots_per_block = int(cfg.knots_per_block)
     p.halo = int(cfg.halo)
     p.watchdog = int(cfg.watchdog)
+    p.cluster_size = int(cfg.cluster_size)
     return p
 
 

@@ -46,7 +46,7 @@ def test_version_and_strerror():
 
 
 def test_struct_layout():
-    assert ctypes.sizeof(L.EemdParams) == 80
+    assert ctypes.sizeof(L.EemdParams) == 88
     assert L.EemdParams.watchdog.offset == 72
     p = L.default_params()
     assert p.dtype == L.EEMD_F64 and p.max_sifts == 50 and p.min_extrema == 4
@@ -67,7 +67,8 @@ def test_workspace_size_scales():
 
 @pytest.mark.parametrize("field,value", [("dtype", 7), ("max_sifts", 0), ("max_imf", 0),
                                          ("end_mode", 5), ("rules", 9), ("tile", 300),
-                                         ("noise_mode", 11), ("tile", 2048)])
+                                         ("noise_mode", 11), ("tile", 2048),
+                                         ("cluster_size", 9)])
 def test_bad_params_rejected(field, value):
     p = L.default_params()
     setattr(p, field, value)
