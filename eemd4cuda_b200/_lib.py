@@ -20,6 +20,8 @@ EEMD_E_KNOT_OVERFLOW = -3
 EEMD_E_TIMEOUT = -4
 EEMD_E_CUDA = -5
 EEMD_E_NOTSUP = -6
+EEMD_E_STATIC_CAPACITY = -7
+STATIC_SCRATCH_BYTES = 64 * 1024 * 1024
 
 EEMD_F64 = 0
 EEMD_F32 = 1
@@ -35,7 +37,8 @@ ABI_VERSION = 1
 
 # every symbol include/eemd_b200.h declares
 EXPORTS = ("eemd_default_params", "eemd_version", "eemd_strerror",
-           "eemd_workspace_size", "eemd_run", "eemd_run_traced", "eemd_finalize")
+           "eemd_workspace_size", "eemd_run", "eemd_run_traced", "eemd_run_static",
+           "eemd_finalize")
 
 KERNEL_KINDS = ("sigma", "emd", "reduce", "outputs", "k4", "k5", "k6", "k7")
 
@@ -124,6 +127,8 @@ def load() -> ctypes.CDLL:
     lib.eemd_run.restype = c_int32
     lib.eemd_run_traced.argtypes = lib.eemd_run.argtypes + [POINTER(KernelTimes)]
     lib.eemd_run_traced.restype = c_int32
+    lib.eemd_run_static.argtypes = lib.eemd_run.argtypes[:16] + [c_void_p]
+    lib.eemd_run_static.restype = c_int32
     lib.eemd_finalize.argtypes = [POINTER(EemdParams), c_void_p, POINTER(c_int64), c_int32,
                                   c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
     lib.eemd_finalize.restype = c_int32
@@ -140,7 +145,8 @@ def strerror(status: int) -> str:
     except Exception:  # library not loadable: still describe the code
         return {0: "ok", -1: "invalid argument", -2: "workspace too small",
                 -3: "knot buffer capacity exceeded", -4: "device wait gave up (watchdog)",
-                -5: "CUDA runtime error", -6: "unsupported parameter combination"}.get(
+                -5: "CUDA runtime error", -6: "unsupported parameter combination",
+                -7: "problem needs more scratch than the static scratch of eemd_run_static"}.get(
                     int(status), "unknown status")
 
 
@@ -197,6 +203,22 @@ def run(p: EemdParams, x, lengths, trial_begin: int, trial_count: int, ws, *, no
     else:
         rc = load().eemd_run_traced(*args, ctypes.byref(times))
     check(rc, "eemd_run")
+
+
+def run_static(p: EemdParams, x, lengths, trial_begin: int, trial_count: int, *, noise=None,
+               imfs=None, resid_out=None, imf_sum=None, mode_count=None, nsift=None, nmode=None,
+               mode_sifts=None, knot_log=None, flags=None, stream=None) -> None:
+    """eemd_run_static: the engine on the library's own static device scratch,
+    for callers that must not allocate device memory (no workspace argument)."""
+    import torch
+
+    la = lengths_array(lengths)
+    st = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    rc = load().eemd_run_static(ctypes.byref(p), _ptr(x), la, len(lengths), int(trial_begin),
+                                int(trial_count), _ptr(noise), _ptr(imfs), _ptr(resid_out),
+                                _ptr(imf_sum), _ptr(mode_count), _ptr(nsift), _ptr(nmode),
+                                _ptr(mode_sifts), _ptr(knot_log), _ptr(flags), c_void_p(st))
+    check(rc, "eemd_run_static")
 
 
 def finalize(p: EemdParams, x, lengths, imf_sum, mode_count, imf_mean, residual, n_modes,

@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <numeric>
@@ -1560,6 +1561,9 @@ const char* eemd_strerror(int32_t status) {
         case EEMD_E_TIMEOUT: return "device wait gave up (watchdog)";
         case EEMD_E_CUDA: return "CUDA runtime error";
         case EEMD_E_NOTSUP: return "unsupported parameter combination";
+        case EEMD_E_STATIC_CAPACITY:
+            return "problem needs more scratch than the static scratch of eemd_run_static "
+                   "(EEMD_STATIC_SCRATCH_BYTES); use eemd_run with a workspace";
         default: return "unknown status";
     }
 }
@@ -1669,6 +1673,51 @@ int32_t eemd_run_traced(const eemd_params* p, const void* x, const int64_t* leng
     if (h.error) return h.error;
     if (h.n_done != C.n_tasks) return EEMD_E_CUDA;
     return EEMD_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point: the engine's scratch is this file-scope device
+// array.  In host code `g_static_scratch` only names the symbol; its device
+// address is looked up once per device with cudaGetSymbolAddress.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_static_scratch[EEMD_STATIC_SCRATCH_BYTES];
+
+namespace {
+constexpr int MAX_DEVICES = 64;
+std::mutex g_static_mu;
+void* g_static_addr[MAX_DEVICES] = {nullptr};
+}  // namespace
+
+extern "C" {
+
+int32_t eemd_run_static(const eemd_params* p, const void* x, const int64_t* lengths, int32_t n_signals,
+                        int32_t trial_begin, int32_t trial_count, const void* noise, void* imfs,
+                        void* resid_out, double* imf_sum, int32_t* mode_count, int32_t* nsift,
+                        int32_t* nmode, int32_t* mode_sifts, int32_t* knot_log, int32_t* flags,
+                        void* stream) {
+    size_t need = 0;
+    int32_t rc = eemd_workspace_size(p, lengths, n_signals, trial_count, imfs != nullptr ? 1 : 0, &need);
+    if (rc) return rc;
+    if (need > (size_t)EEMD_STATIC_SCRATCH_BYTES) return EEMD_E_STATIC_CAPACITY;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return EEMD_E_CUDA;
+    if (dev < 0 || dev >= MAX_DEVICES) return EEMD_E_NOTSUP;
+    void* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_static_mu);
+        if (g_static_addr[dev] == nullptr) {
+            void* addr = nullptr;
+            if (cudaGetSymbolAddress(&addr, g_static_scratch) != cudaSuccess || addr == nullptr)
+                return EEMD_E_CUDA;
+            g_static_addr[dev] = addr;
+        }
+        base = g_static_addr[dev];
+    }
+    return eemd_run(p, x, lengths, n_signals, trial_begin, trial_count, noise, imfs, resid_out, imf_sum,
+                    mode_count, nsift, nmode, mode_sifts, knot_log, flags, base,
+                    (size_t)EEMD_STATIC_SCRATCH_BYTES, stream);
 }
 
 int32_t eemd_finalize(const eemd_params* p, const void* x, const int64_t* lengths, int32_t n_signals,

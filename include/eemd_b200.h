@@ -42,6 +42,8 @@ extern "C" {
 #define EEMD_E_TIMEOUT         -4  /* a bounded device wait gave up (watchdog) */
 #define EEMD_E_CUDA            -5  /* CUDA runtime error */
 #define EEMD_E_NOTSUP          -6  /* unsupported combination (e.g. exact mode with float32) */
+#define EEMD_E_STATIC_CAPACITY -7  /* eemd_run_static(): the problem needs more scratch than
+                                      EEMD_STATIC_SCRATCH_BYTES */
 
 /* storage type of signals, IMFs and working arrays; the spline solve is
  * always float64 */
@@ -162,6 +164,31 @@ int32_t eemd_run_traced(const eemd_params* p, const void* x, const int64_t* leng
                         int32_t* knot_log, int32_t* flags,
                         void* ws, size_t ws_bytes, void* stream,
                         eemd_kernel_times* times);
+
+/* Size of the device scratch eemd_run_static() owns: a file-scope array in the
+ * library, present on every GPU that loads the library until the process exits. */
+#define EEMD_STATIC_SCRATCH_BYTES (64u * 1024u * 1024u)
+
+/* eemd_run() without a workspace argument, for callers that cannot allocate
+ * device memory: code running inside a CUDA-graph capture or a real-time audio
+ * callback (where cudaMalloc would break the capture or block the thread), and
+ * host applications whose device memory is owned by another allocator.  The
+ * engine's scratch is the library's own static device array of
+ * EEMD_STATIC_SCRATCH_BYTES; problems whose eemd_workspace_size() exceeds it are
+ * rejected with EEMD_E_STATIC_CAPACITY before any GPU work.  The caller still
+ * passes x and the outputs.  The first call on each device looks the array up
+ * (cudaGetSymbolAddress with that device current), so make that first call
+ * before any stream capture.  All calls share the one array and it keeps the
+ * previous call's contents (the engine re-initialises what it reads), so calls
+ * that overlap on the GPU -- on different streams or host threads -- race and
+ * must be serialised by the caller.  No cudaMalloc, cudaFree or allocating
+ * library routine is called.  No counterpart in the reference. */
+int32_t eemd_run_static(const eemd_params* p, const void* x, const int64_t* lengths,
+                        int32_t n_signals, int32_t trial_begin, int32_t trial_count,
+                        const void* noise, void* imfs, void* resid_out,
+                        double* imf_sum, int32_t* mode_count,
+                        int32_t* nsift, int32_t* nmode, int32_t* mode_sifts,
+                        int32_t* knot_log, int32_t* flags, void* stream);
 
 /* Ensemble mean and residual from the accumulated sums (emd_par.py:248-250):
  *   imf_mean[s][m][n] = imf_sum[s][m][n] / max(mode_count[s][m], 1)
