@@ -49,6 +49,22 @@ __device__ __forceinline__ double ldv(const void* p, int64_t i) {
 template <typename T>
 __device__ __forceinline__ double rnd(double v) { return (double)(T)v; }
 
+// fused multiply-add in the storage type
+__device__ __forceinline__ float fmat(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmat(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// knot sample index kept in a storage-type record plane as an integer bit pattern
+template <typename T>
+__device__ __forceinline__ T tbits(int t) {
+    if constexpr (sizeof(T) == 4) return __int_as_float(t);
+    else return __longlong_as_double((long long)t);
+}
+template <typename T>
+__device__ __forceinline__ int tint(T v) {
+    if constexpr (sizeof(T) == 4) return __float_as_int(v);
+    else return (int)__double_as_longlong(v);
+}
+
 // 1/x: hardware approximation refined by one Newton step on f(y) = 1/y - x,
 // y <- y + y(1 - xy); relative error about 2^-50 or better.
 __device__ __forceinline__ double fast_rcp(double x) {
@@ -67,6 +83,10 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 template <typename T>
 __device__ __forceinline__ void cp_async_el(T* smem, const T* gmem) {
@@ -197,19 +217,17 @@ struct TaskSm {
     int run_cur[2], run_new[2];
     double hold_m1, hold_m2, rold_m1, rold_p, hold_p, f_m1, g_m1;
     double hf0, hf1, rf0, rf1;
+    double fl, gl, fr, gr;     // new value / new residual at the tile's halo samples
+    double f_last2, g_last2;   // new value / residual at the tile's second-to-last sample
 };
 
 struct Smem {
-    void* hT[2];     // [TILE+2] old h, storage type (double buffer; index j+1 = sample j)
-    void* rT[2];     // [TILE+2] residual, storage type (double buffer)
-    double* f;       // [TILE+2] new values (0 and tl+1 are the halo samples)
-    double* g;       // [TILE+2] new residual (TM_LAST)
-    int* kt;         // [2][cap] staged knot sample index
-    void* ky;        // [2][cap] staged knot value, storage type
-    double* M;       // [2][cap] staged second derivative
-    double* c1;      // [2][cap] fast: monomial c1
-    double* c2;      // [2][cap] fast: monomial c2
-    double* c3;      // [2][cap] fast: monomial c3
+    void* hT[2];     // [TILE+8] old h, storage type (double buffer; the tile's sample 0 sits at
+                     //          index TOFF + (16-byte phase of its global address), so that
+                     //          16-byte copies line up; left halo just before, right halo after)
+    void* rT[2];     // [TILE+8] residual, storage type (double buffer, same placement)
+    void* kt;        // [2][cap] staged interval records, storage type: knot index bit pattern
+    void* c[4];      // [2][cap] fast: monomial c0..c3 of the interval; exact: c[0] = y, c[1] = M
     int* skt;        // solve staging (padded): knot sample index
     void* sky;       // solve staging (padded): knot value, storage type
     double* ssl;     // solve staging (padded): slope of the interval starting at the knot
@@ -218,6 +236,7 @@ struct Smem {
 
 constexpr int RUN_MAX = 4;            // consecutive samples per thread in a tile
 constexpr int NWARP = THREADS / 32;
+constexpr int TOFF = 4;               // tile buffer index of the first 16-byte boundary used
 
 __host__ __device__ inline int stage_pad(int k) { return k + (k >> 4); }
 
@@ -225,9 +244,8 @@ __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t
 
 __host__ __device__ inline size_t smem_bytes(int TILE, int bt) {
     const size_t cap = (size_t)(TILE >> 1) + 8;
-    const size_t tile = align16((size_t)(TILE + 2) * bt);
-    const size_t sweep = 4 * tile + 2 * align16((size_t)(TILE + 2) * 8) + 2 * align16(cap * 4) +
-                         2 * align16(cap * bt) + 8 * align16(cap * 8);
+    const size_t tile = align16((size_t)(TILE + 8) * bt);
+    const size_t sweep = 4 * tile + 10 * align16(cap * bt);
     const size_t sp = (size_t)stage_pad(SOLVE_CAP);
     const size_t solve = align16(sp * 8) + align16(sp * 4) + align16(sp * bt);
     return sweep > solve ? sweep : solve;
@@ -238,20 +256,15 @@ __device__ __forceinline__ Smem carve(unsigned char* base, int TILE) {
     Smem m;
     const size_t cap = (size_t)(TILE >> 1) + 8;
     m.cap = (int)cap;
-    const size_t tile = align16((size_t)(TILE + 2) * sizeof(T));
+    const size_t tile = align16((size_t)(TILE + 8) * sizeof(T));
+    const size_t plane = 2 * align16(cap * sizeof(T));
     unsigned char* p = base;
     m.hT[0] = p; p += tile;
     m.hT[1] = p; p += tile;
     m.rT[0] = p; p += tile;
     m.rT[1] = p; p += tile;
-    m.f = reinterpret_cast<double*>(p); p += align16((size_t)(TILE + 2) * 8);
-    m.g = reinterpret_cast<double*>(p); p += align16((size_t)(TILE + 2) * 8);
-    m.kt = reinterpret_cast<int*>(p); p += 2 * align16(cap * 4);
-    m.ky = p; p += 2 * align16(cap * sizeof(T));
-    m.M = reinterpret_cast<double*>(p); p += 2 * align16(cap * 8);
-    m.c1 = reinterpret_cast<double*>(p); p += 2 * align16(cap * 8);
-    m.c2 = reinterpret_cast<double*>(p); p += 2 * align16(cap * 8);
-    m.c3 = reinterpret_cast<double*>(p);
+    m.kt = p; p += plane;
+    for (int i = 0; i < 4; ++i) { m.c[i] = p; p += plane; }
     // solve staging overlays the sweep buffers (used in a different phase)
     const size_t sp = (size_t)stage_pad(SOLVE_CAP);
     m.ssl = reinterpret_cast<double*>(base);
@@ -265,9 +278,9 @@ __device__ __forceinline__ Smem carve(unsigned char* base, int TILE) {
 // position i - pref[r] of that segment's list
 // ---------------------------------------------------------------------------
 struct Slot {
-    int32_t* kt;   // slot base
+    int32_t* kt;   // knot lists (segmented)
     void* ky;
-    double* M;
+    void* M;       // interval records, mirror space: [2 env][5][kcap] storage type
 };
 
 __device__ __forceinline__ int64_t knot_index(const Ctx& C, int par, int env, int seg, int i) {
@@ -377,10 +390,22 @@ __device__ __forceinline__ Row row_of(int ta, int tb, int tc, double sa, double 
 #define SKT(k) skt[stage_pad(k)]
 #define SSL(k) ssl[stage_pad(k)]
 
+// Interval records of one envelope in mirror space, five storage-type planes
+// of stride kcap: t_k (integer bit pattern), then four coefficient planes.
+template <typename T>
+struct Rec {  // plane 0: t_k; planes 1..4: c0..c3 (fast) or y_k, M_k (exact)
+    T* rc;
+    int64_t stride;
+    __device__ __forceinline__ T& c(int plane, int k) const { return rc[(plane + 1) * stride + k]; }
+    __device__ __forceinline__ T& t(int k) const { return rc[k]; }
+};
+
 // exact: forward elimination from w0 (outer coupling dropped), back
-// substitution from w1; identical recurrences to serial Thomas (emd_ref.py:50-65)
-__device__ void window_exact(const Ctx& C, const int* skt, const double* ssl, int base, int n, int w,
-                             double* M2, int p2) {
+// substitution from w1; identical recurrences to serial Thomas (emd_ref.py:50-65).
+// Writes (t_k, y_k, M_k) of the owned knots k = o0+1 .. o1+1 (+ both end knots).
+template <typename T>
+__device__ void window_exact(const Ctx& C, const int* skt, const T* sky, const double* ssl, int base,
+                             int n, int w, const Rec<T>& R, int p2) {
     const int B = C.B, S = C.S;
     const int o0 = w * B;
     const int o1 = min(n, o0 + B) - 1;
@@ -404,23 +429,29 @@ __device__ void window_exact(const Ctx& C, const int* skt, const double* ssl, in
         tb = tc;
         sa = sb;
     }
+    auto put = [&](int k, double Mk) {
+        R.t(k) = tbits<T>(SKT(k - base));
+        R.c(0, k) = sky[stage_pad(k - base)];
+        R.c(1, k) = (T)Mk;
+    };
     double xv = dp;
-    if (w1 <= o1) M2[w1 + 1] = xv;
+    if (w1 <= o1) put(w1 + 1, xv);
     for (int i = w1 - 1; i >= o0; --i) {
         const double2 cd = sc[(int64_t)(i - o0) * gthreads];
         xv = cd.y - cd.x * xv;
-        if (i <= o1) M2[i + 1] = xv;
+        if (i <= o1) put(i + 1, xv);
     }
-    if (o0 == 0) M2[0] = 0.0;
-    if (o1 == n - 1) M2[p2 - 1] = 0.0;
+    if (o0 == 0) put(0, 0.0);
+    if (o1 == n - 1) put(p2 - 1, 0.0);
 }
 
 // fast: twisted factorisation of the window.  A left sweep (LU, coupling
 // dropped at w0) keeps its (c, d) for the owned rows in registers; a right
 // sweep (UL, coupling dropped at w1) meets it, and each owned unknown is
 //   x_i = (r_i - l_i d_{i-1} - u_i g_{i+1}) / (dg_i - l_i c_{i-1} - u_i e_{i+1}).
-__device__ void window_fast(const Ctx& C, const int* skt, const double* ssl, int base, int n, int w,
-                            double* M2, int p2) {
+template <typename T>
+__device__ void window_fast(const Ctx& C, const int* skt, const T* sky, const double* ssl, int base, int n,
+                            int w, const Rec<T>& R, int p2) {
     const int S = C.S;
     const int o0 = w * FAST_B;
     const int cnt = min(FAST_B, n - o0);
@@ -428,7 +459,7 @@ __device__ void window_fast(const Ctx& C, const int* skt, const double* ssl, int
     const int w0 = max(0, o0 - S);
     const int w1 = min(n - 1, o1 + S);
     double fc[FAST_B], fd[FAST_B];
-    double cp = 0.0, dp = 0.0;
+    double cp = 0.0, dp = 0.0, cq = 0.0, dq = 0.0;  // (cq, dq): forward state after row o0-2
     int ta = SKT(w0 - base), tb = SKT(w0 + 1 - base);
     double sa = SSL(w0 - base);
     for (int i = w0; i <= o0 - 2; ++i) {
@@ -442,6 +473,8 @@ __device__ void window_fast(const Ctx& C, const int* skt, const double* ssl, int
         tb = tc;
         sa = sb;
     }
+    cq = cp;
+    dq = dp;
     // forward state after rows o0-1 .. o1-1 (row -1 does not exist: zero state)
 #pragma unroll
     for (int k = 0; k < FAST_B; ++k) {
@@ -477,6 +510,19 @@ __device__ void window_fast(const Ctx& C, const int* skt, const double* ssl, int
         ub = ua;
         vb = va;
     }
+    // monomial record of interval k (knots k, k+1; M_k = Ma, M_{k+1} = Mb):
+    // y_k + s(c1 + s(c2 + s c3)), s = t - t_k, c1 = slope - h(2Ma + Mb)/6,
+    // c2 = Ma/2, c3 = (Mb - Ma)/(6h)
+    auto put = [&](int k, double Ma, double Mb) {
+        const int t0 = SKT(k - base), t1 = SKT(k + 1 - base);
+        const double h = (double)(t1 - t0);
+        R.t(k) = tbits<T>(t0);
+        R.c(0, k) = sky[stage_pad(k - base)];
+        R.c(1, k) = (T)fma(-h * (1.0 / 6.0), fma(2.0, Ma, Mb), SSL(k - base));
+        R.c(2, k) = (T)(0.5 * Ma);
+        R.c(3, k) = (T)((Mb - Ma) * fast_rcp(h) * (1.0 / 6.0));
+    };
+    double xnext = 0.0;  // x_{i+1} of the previous iteration
 #pragma unroll
     for (int k = FAST_B - 1; k >= 0; --k) {
         if (k < cnt) {
@@ -486,7 +532,10 @@ __device__ void window_fast(const Ctx& C, const int* skt, const double* ssl, int
             const Row rw = row_of(ua, ub, uc, va, vb, i, n);
             const double num = fma(-rw.u, g, fma(-rw.l, fd[k], rw.r));
             const double den = fma(-rw.u, e, fma(-rw.l, fc[k], rw.dg));
-            M2[i + 1] = num * fast_rcp(den);
+            const double xi = num * fast_rcp(den);  // M at mirror knot i+1
+            if (i < o1) put(i + 1, xi, xnext);
+            else if (i == n - 1) put(n, xi, 0.0);   // last interval ends at the M = 0 knot
+            xnext = xi;
             const double inv = fast_rcp(fma(-rw.u, e, rw.dg));
             e = rw.l * inv;
             g = fma(-rw.u, g, rw.r) * inv;
@@ -495,8 +544,18 @@ __device__ void window_fast(const Ctx& C, const int* skt, const double* ssl, int
             vb = va;
         }
     }
-    if (o0 == 0) M2[0] = 0.0;
-    if (o1 == n - 1) M2[p2 - 1] = 0.0;
+    // M at knot o0 (x_{o0-1}) closes interval o0; zero at the natural end
+    double xm = 0.0;
+    if (o0 >= 1) {
+        const int i = o0 - 1;
+        const int ua = SKT(i - base);
+        const double va = SSL(i - base);
+        const Row rw = row_of(ua, ub, uc, va, vb, i, n);
+        const double num = fma(-rw.u, g, fma(-rw.l, dq, rw.r));
+        const double den = fma(-rw.u, e, fma(-rw.l, cq, rw.dg));
+        xm = num * fast_rcp(den);
+    }
+    put(o0, xm, xnext);
 }
 
 #undef SKT
@@ -508,9 +567,25 @@ __device__ void solve_task(const Ctx& C, const Slot& sl, TaskSm& S, const Smem& 
     for (int env = 0; env < 2; ++env) {
         const int p2 = S.p2[env];
         const int n = p2 - 2;
-        double* M2 = sl.M + (int64_t)env * C.kcap;
+        Rec<T> R;
+        R.rc = static_cast<T*>(sl.M) + (int64_t)env * 5 * C.kcap;
+        R.stride = C.kcap;
         if (n <= 0) {
-            if (S.rank == 0 && tid < p2) M2[tid] = 0.0;
+            // one or two knots: a constant or the straight line through them (M = 0)
+            if (S.rank == 0 && tid < p2) {
+                int tk, t1;
+                double yk, y1;
+                knot2<T>(C, sl, S, env, tid, tk, yk);
+                R.t(tid) = tbits<T>(tk);
+                R.c(0, tid) = (T)yk;
+                R.c(1, tid) = (T)0;
+                R.c(2, tid) = (T)0;
+                R.c(3, tid) = (T)0;
+                if (!EXACT && tid + 1 < p2) {
+                    knot2<T>(C, sl, S, env, tid + 1, t1, y1);
+                    R.c(1, tid) = (T)((y1 - yk) / (double)(t1 - tk));
+                }
+            }
             continue;
         }
         const int Bw = EXACT ? C.B : FAST_B;
@@ -540,8 +615,8 @@ __device__ void solve_task(const Ctx& C, const Slot& sl, TaskSm& S, const Smem& 
             __syncthreads();
             const int w = wbase + tid;
             if (w < wend) {
-                if (EXACT) window_exact(C, sm.skt, sm.ssl, rlo, n, w, M2, p2);
-                else window_fast(C, sm.skt, sm.ssl, rlo, n, w, M2, p2);
+                if (EXACT) window_exact<T>(C, sm.skt, sky, sm.ssl, rlo, n, w, R, p2);
+                else window_fast<T>(C, sm.skt, sky, sm.ssl, rlo, n, w, R, p2);
             }
         }
     }
@@ -589,36 +664,95 @@ __device__ __forceinline__ void block_scan2(int a, int b, int& ea, int& eb, int&
     eb = bb + ib - b;
 }
 
-// Envelope value at t from the staged intervals; `cless` = knots strictly
-// before t in mirror space (emd_ref.py:70 searchsorted - 1, clipped).
+// Interval cache of one envelope for a thread's run of consecutive samples:
+// the staged record of interval k is loaded only when k changes.
+template <typename T>
+struct IvCache {
+    int k, t0, t1;
+    T y0, c1, c2, c3, y1, m1;  // fast: monomial c0..c3 of interval k; exact: y0, M0, y1, M1
+};
+
 template <typename T, bool EXACT>
-__device__ __forceinline__ double env_at(const Smem& sm, int env, int cless, int t, int lo2, int p2) {
-    const int idx2 = max(0, min(cless - 1, p2 - 2));
-    const int k = env * sm.cap + (idx2 - lo2);
-    const T* ky = static_cast<const T*>(sm.ky);
-    if (EXACT) {
-        return spline_exact((double)t, (double)sm.kt[k], (double)sm.kt[k + 1], (double)ky[k],
-                            (double)ky[k + 1], sm.M[k], sm.M[k + 1]);
+__device__ __forceinline__ T iv_value(IvCache<T>& cc, const Smem& sm, int env, int idx2, int lo2, int t) {
+    if (idx2 != cc.k) {
+        const T* kt = static_cast<const T*>(sm.kt);
+        const T* c0 = static_cast<const T*>(sm.c[0]);
+        const T* c1 = static_cast<const T*>(sm.c[1]);
+        const int o = env * sm.cap + (idx2 - lo2);
+        cc.k = idx2;
+        cc.t0 = tint<T>(kt[o]);
+        cc.y0 = c0[o];
+        cc.c1 = c1[o];
+        if (EXACT) {
+            cc.t1 = tint<T>(kt[o + 1]);
+            cc.y1 = c0[o + 1];
+            cc.m1 = c1[o + 1];
+        } else {
+            cc.c2 = static_cast<const T*>(sm.c[2])[o];
+            cc.c3 = static_cast<const T*>(sm.c[3])[o];
+        }
     }
-    const double s = (double)(t - sm.kt[k]);
-    return fma(s, fma(s, fma(s, sm.c3[k], sm.c2[k]), sm.c1[k]), (double)ky[k]);
+    if (EXACT)
+        return (T)spline_exact((double)t, (double)cc.t0, (double)cc.t1, (double)cc.y0, (double)cc.y1,
+                               (double)cc.c1, (double)cc.m1);
+    const T s = (T)(t - cc.t0);
+    return fmat(s, fmat(s, fmat(s, cc.c3, cc.c2), cc.c1), cc.y0);
+}
+
+// envelope value at t with `cless` knots strictly before t (mirror space),
+// interval = searchsorted - 1 clipped (emd_ref.py:70)
+template <typename T, bool EXACT>
+__device__ __forceinline__ T env_value(const TaskSm& S, IvCache<T>& cc, const Smem& sm, int env, int cless,
+                                       int t, int lo2) {
+    if (S.P[env] < 2) return (T)S.cval[env];
+    const int idx2 = max(0, min(cless - 1, S.p2[env] - 2));
+    return iv_value<T, EXACT>(cc, sm, env, idx2, lo2, t);
 }
 
 __device__ __forceinline__ int mirror_adj(const TaskSm& S, int env, int t) {
     return S.mir[env] ? (S.tfirst[env] < t ? 1 : 0) + (S.tlast[env] < t ? 1 : 0) : 0;
 }
 
+// element phase of an address within its 16-byte block
+template <typename T>
+__device__ __forceinline__ int phase16(const T* p) {
+    return (int)((reinterpret_cast<uintptr_t>(p) / sizeof(T)) & (16 / sizeof(T) - 1));
+}
+
+// stores a thread's run of samples: one 16-byte-vector pass when the run is
+// full and aligned, element stores otherwise
+template <typename T>
+__device__ __forceinline__ void store_run(T* p, const T (&v)[RUN_MAX], int nv) {
+    if (nv == RUN_MAX && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+        if constexpr (sizeof(T) == 4) {
+            *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+        } else {
+            reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+            reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+        }
+        return;
+    }
+#pragma unroll
+    for (int i = 0; i < RUN_MAX; ++i)
+        if (i < nv) p[i] = v[i];
+}
+
 // The sweep streams the CTA's segment in tiles of TILE samples; thread u owns
-// the run of TILE/THREADS consecutive samples starting at u*TILE/THREADS.
-// The next tile's samples are copied to shared memory (cp.async) while the
-// current one is processed; the knots a tile needs are staged with one batch
-// of asynchronous copies.
+// the run of TILE/THREADS consecutive samples starting at u*TILE/THREADS and
+// keeps its samples in registers.  The next tile is copied to shared memory
+// (cp.async, 16-byte copies where the addresses allow) while the current one
+// is processed; the interval records a tile needs are staged with one batch
+// of asynchronous copies.  Arithmetic runs in the storage type T: the spline
+// solve that produced the records ran in double, and the exact mode (double
+// only) keeps the reference operation order.
 template <typename T, bool EXACT>
 __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, const Smem& sm,
                       cg::cluster_group& cl) {
+    constexpr int VEC = 16 / (int)sizeof(T);
     __shared__ double2 s_red[NWARP];
     __shared__ int s_w1[2 * NWARP], s_w2[2 * NWARP];
-    const int tid = threadIdx.x;
+    __shared__ T s_gfirst[NWARP], s_glast[NWARP];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int TILE = C.tile, run = TILE / THREADS, cap = sm.cap;
     const int mode = S.mode, n = S.n, s0 = S.s0, s1 = S.s1, rank = S.rank;
     const bool sifting = (mode == TM_SIFT || mode == TM_LAST);
@@ -630,8 +764,21 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, const Sm
     T* imf_m = static_cast<T*>(C.imfs) + d.imf_off + (int64_t)min(S.imf, C.max_imf - 1) * n;
     const T* src = (sifting && S.src_resid) ? resid : imf_m;
     const int np = S.kpar ^ 1;
-    T* kyS = static_cast<T*>(sm.ky);
     double num = 0.0, den = 0.0;
+#ifdef EEMD_TRACE
+    unsigned long long scyc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    long long smark = clock64();
+#define SUB(k)                                          \
+    do {                                                \
+        const long long now_ = clock64();               \
+        scyc[k] += (unsigned long long)(now_ - smark);  \
+        smark = now_;                                   \
+    } while (0)
+#else
+#define SUB(k) \
+    do {       \
+    } while (0)
+#endif
 
     if (tid == 0) {
         S.run_cur[0] = S.run_cur[1] = 0;
@@ -655,16 +802,28 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, const Sm
     }
     __syncthreads();
 
+    // copies g[0 .. cnt) to dst[0 .. cnt); dst + j and g + j share their
+    // 16-byte phase, so the body moves in 16-byte copies
+    auto copy_stream = [&](T* dst, const T* g, int cnt) {
+        const int head = min(cnt, (VEC - phase16(g)) & (VEC - 1));
+        const int nvec = (cnt - head) / VEC;
+        const int tail0 = head + nvec * VEC;
+        for (int v = tid; v < nvec; v += THREADS) cp_async16(dst + head + v * VEC, g + head + v * VEC);
+        const int ns = head + (cnt - tail0);
+        for (int k = tid; k < ns; k += THREADS) {
+            const int j = (k < head) ? k : tail0 + (k - head);
+            cp_async_el<T>(dst + j, g + j);
+        }
+    };
+    // tile buffer b positioned for the tile starting at t0p of stream g
+    auto tile_h = [&](int b, int t0p) { return static_cast<T*>(sm.hT[b]) + TOFF + phase16(src + t0p); };
+    auto tile_r = [&](int b, int t0p) { return static_cast<T*>(sm.rT[b]) + TOFF + phase16(resid + t0p); };
     // copies samples [t0p, t0p+tl] (the extra one when it is still this segment's) to buffer b
     auto prefetch = [&](int t0p, int b) {
         const int tlp = min(TILE, s1 - t0p);
         const int cnt = (t0p + tlp < s1) ? tlp + 1 : tlp;
-        T* hb = static_cast<T*>(sm.hT[b]);
-        T* rb = static_cast<T*>(sm.rT[b]);
-        for (int j = tid; j < cnt; j += THREADS) {
-            if (needs_h) cp_async_el<T>(hb + 1 + j, src + t0p + j);
-            if (uses_r) cp_async_el<T>(rb + 1 + j, resid + t0p + j);
-        }
+        if (needs_h) copy_stream(tile_h(b, t0p), src + t0p, cnt);
+        if (uses_r) copy_stream(tile_r(b, t0p), resid + t0p, cnt);
         cp_async_commit();
     };
     const bool streams = needs_h || uses_r;
@@ -675,8 +834,9 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, const Sm
         const int tl = min(TILE, s1 - t0);
         const bool first = (t0 == s0), last = (t0 + tl == s1);
         const int j0 = tid * run;
-        T* hb = static_cast<T*>(sm.hT[buf]);
-        T* rb = static_cast<T*>(sm.rT[buf]);
+        const int nv = max(0, min(run, tl - j0));  // valid samples of this thread's run
+        T* hb = tile_h(buf, t0);  // hb[j] = sample t0+j, hb[-1] / hb[tl] halos
+        T* rb = tile_r(buf, t0);
         // ---------------- (a) this tile's samples (prefetched), next tile's prefetch ----------------
         if (streams) {
             if (!last) {
@@ -688,200 +848,214 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, const Sm
         }
         if (tid == 0) {
             if (sifting) {
-                hb[0] = (T)S.hold_m1;
-                if (last) hb[tl + 1] = (T)((t0 + tl < n) ? S.hold_p : 0.0);
+                hb[-1] = (T)S.hold_m1;
+                if (last) hb[tl] = (T)((t0 + tl < n) ? S.hold_p : 0.0);
             } else if (needs_h) {  // TM_TRANS: the closed IMF at the halo samples
-                hb[0] = (first && t0 > 0) ? __ldcg(imf_m + t0 - 1) : (T)0;
-                if (last) hb[tl + 1] = (t0 + tl < n) ? __ldcg(imf_m + t0 + tl) : (T)0;
+                hb[-1] = (first && t0 > 0) ? __ldcg(imf_m + t0 - 1) : (T)0;
+                if (last) hb[tl] = (t0 + tl < n) ? __ldcg(imf_m + t0 + tl) : (T)0;
             }
             if (uses_r) {
-                if (first) rb[0] = (T)S.rold_m1;
-                if (last) rb[tl + 1] = (T)((t0 + tl < n) ? S.rold_p : 0.0);
-            }
-            if (!first) {
-                sm.f[0] = S.f_m1;
-                sm.g[0] = S.g_m1;
+                if (first) rb[-1] = (T)S.rold_m1;
+                if (last) rb[tl] = (T)((t0 + tl < n) ? S.rold_p : 0.0);
             }
         }
         __syncthreads();
-        double hv[RUN_MAX], rv[RUN_MAX], fv[RUN_MAX], gv[RUN_MAX];
+        SUB(0);
+        T hv[RUN_MAX], rv[RUN_MAX], fv[RUN_MAX], gv[RUN_MAX];
 #pragma unroll
         for (int i = 0; i < RUN_MAX; ++i) {
-            const int j = j0 + i;
-            const bool ok = (i < run && j < tl);
-            hv[i] = (ok && needs_h) ? (double)hb[1 + j] : 0.0;
-            rv[i] = (ok && uses_r) ? (double)rb[1 + j] : 0.0;
-            fv[i] = gv[i] = 0.0;
+            const bool ok = i < nv;
+            hv[i] = (ok && needs_h) ? hb[j0 + i] : (T)0;
+            rv[i] = (ok && uses_r) ? rb[j0 + i] : (T)0;
+            fv[i] = gv[i] = (T)0;
         }
 
         // ---------------- (b) current knots: strict extrema of h in the run ----------------
         unsigned kmx = 0u, kmn = 0u;
-        int kb[2] = {0, 0}, kc[2] = {0, 0}, lo2[2] = {0, 0}, hi2[2] = {-1, -1}, cl0[2] = {0, 0};
+        int kb0 = 0, kb1 = 0, kc0 = 0, kc1 = 0, lo0 = 0, lo1 = 0, hi0 = -1, hi1 = -1;
+        int cl0 = 0, cl1 = 0;
         if (sifting) {
+            if (nv > 0) {
+                const T hl0 = hb[j0 - 1], hr0 = hb[j0 + nv];
 #pragma unroll
-            for (int i = 0; i < RUN_MAX; ++i) {
-                const int j = j0 + i, t = t0 + j;
-                if (i < run && j < tl && t >= 1 && t <= n - 2) {
-                    const double a = (double)hb[j], c = (double)hb[j + 2], v = hv[i];
-                    if (v > a && v > c) kmx |= 1u << i;
-                    if (v < a && v < c) kmn |= 1u << i;
+                for (int i = 0; i < RUN_MAX; ++i) {
+                    const int t = t0 + j0 + i;
+                    if (i < nv && t >= 1 && t <= n - 2) {
+                        const T a = (i == 0) ? hl0 : hv[(i + RUN_MAX - 1) % RUN_MAX];
+                        const T c = (i + 1 == nv) ? hr0 : hv[(i + 1) % RUN_MAX];
+                        const T v = hv[i];
+                        if (v > a && v > c) kmx |= 1u << i;
+                        if (v < a && v < c) kmn |= 1u << i;
+                    }
                 }
             }
             int ex, en, tx, tn;
             block_scan2(__popc(kmx), __popc(kmn), ex, en, tx, tn, s_w1);
-            kc[0] = tx;
-            kc[1] = tn;
-            bool bad = false;
-#pragma unroll
-            for (int env = 0; env < 2; ++env) {
-                kb[env] = S.pref[env][rank] + S.run_cur[env];
-                if (S.P[env] >= 2) {
-                    lo2[env] = max(0, S.mir[env] + kb[env] - 2);
-                    hi2[env] = min(S.p2[env] - 1, S.mir[env] + kb[env] + kc[env] + 1);
-                }
-                if (hi2[env] - lo2[env] + 1 > cap || kb[env] + kc[env] > S.P[env]) {
-                    bad = true;
-                    hi2[env] = lo2[env] - 1;
-                }
+            kc0 = tx;
+            kc1 = tn;
+            kb0 = S.pref[0][rank] + S.run_cur[0];
+            kb1 = S.pref[1][rank] + S.run_cur[1];
+            if (S.P[0] >= 2) {
+                lo0 = max(0, S.mir[0] + kb0 - 2);
+                hi0 = min(S.p2[0] - 1, S.mir[0] + kb0 + kc0 + 1);
             }
-            if (bad && tid == 0) raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
-            cl0[0] = kb[0] + ex;
-            cl0[1] = kb[1] + en;
-            // ---------------- (c) stage the intervals the tile uses ----------------
-            const int n0 = hi2[0] - lo2[0] + 1, n1 = hi2[1] - lo2[1] + 1;
+            if (S.P[1] >= 2) {
+                lo1 = max(0, S.mir[1] + kb1 - 2);
+                hi1 = min(S.p2[1] - 1, S.mir[1] + kb1 + kc1 + 1);
+            }
+            const bool bad0 = hi0 - lo0 + 1 > cap || kb0 + kc0 > S.P[0];
+            const bool bad1 = hi1 - lo1 + 1 > cap || kb1 + kc1 > S.P[1];
+            if ((bad0 || bad1) && tid == 0) raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
+            if (bad0) hi0 = lo0 - 1;
+            if (bad1) hi1 = lo1 - 1;
+            cl0 = kb0 + ex;
+            cl1 = kb1 + en;
+            SUB(1);
+            // ---------------- (c) stage the interval records the tile uses ----------------
+            const int n0 = hi0 - lo0 + 1, n1 = hi1 - lo1 + 1;
             for (int k = tid; k < n0 + n1; k += THREADS) {
                 const int env = (k >= n0) ? 1 : 0;
                 const int kk = k - env * n0;
-                const int i2 = lo2[env] + kk;
+                const int i2 = (env ? lo1 : lo0) + kk;
                 const int o = env * cap + kk;
-                stage_knot<T>(C, sl, S, env, i2, &sm.kt[o], &kyS[o]);
-                cp_async8(&sm.M[o], sl.M + (int64_t)env * C.kcap + i2);
+                const T* rc = static_cast<const T*>(sl.M) + (int64_t)env * 5 * C.kcap + i2;
+                cp_async_el<T>(static_cast<T*>(sm.kt) + o, rc);
+                cp_async_el<T>(static_cast<T*>(sm.c[0]) + o, rc + C.kcap);
+                cp_async_el<T>(static_cast<T*>(sm.c[1]) + o, rc + 2 * (int64_t)C.kcap);
+                if (!EXACT) {
+                    cp_async_el<T>(static_cast<T*>(sm.c[2]) + o, rc + 3 * (int64_t)C.kcap);
+                    cp_async_el<T>(static_cast<T*>(sm.c[3]) + o, rc + 4 * (int64_t)C.kcap);
+                }
             }
             cp_async_commit();
             if (tid == 0) {
                 // is t0-1 a knot of each kind? (only the segment's first tile evaluates t0-1)
                 S.left_knot[0] = S.left_knot[1] = 0;
                 if (first && t0 - 1 >= 1 && t0 - 1 <= n - 2) {
-                    const double a = S.hold_m2, b = (double)hb[0], c = (double)hb[1];
+                    const T a = (T)S.hold_m2, b = hb[-1], c = hb[0];
                     S.left_knot[0] = (b > a) && (b > c);
                     S.left_knot[1] = (b < a) && (b < c);
                 }
             }
             cp_async_wait<0>();
             __syncthreads();
-            if (!EXACT) {
-                // monomial form of interval [k, k+1]: y + s(c1 + s(c2 + s c3)), s = t - t_k,
-                // c1 = (y'-y)/h - h(2M + M')/6, c2 = M/2, c3 = (M'-M)/(6h)
-                for (int k = tid; k < n0 + n1; k += THREADS) {
-                    const int env = (k >= n0) ? 1 : 0;
-                    const int kk = k - env * n0;
-                    if (kk + 1 < (env ? n1 : n0)) {
-                        const int o = env * cap + kk;
-                        const double h = (double)(sm.kt[o + 1] - sm.kt[o]);
-                        const double ih = fast_rcp(h);
-                        const double Ma = sm.M[o], Mb = sm.M[o + 1];
-                        const double ya = (double)kyS[o], yb = (double)kyS[o + 1];
-                        sm.c1[o] = fma(yb - ya, ih, -h * fma(2.0, Ma, Mb) * (1.0 / 6.0));
-                        sm.c2[o] = 0.5 * Ma;
-                        sm.c3[o] = (Mb - Ma) * ih * (1.0 / 6.0);
-                    }
-                }
-                __syncthreads();
-            }
+            SUB(2);
         }
 
         // ---------------- (d) new values ----------------
-        int cl[2] = {cl0[0], cl0[1]};
+        IvCache<T> cc0, cc1;
+        cc0.k = cc1.k = -1;
+        cc0.t0 = cc0.t1 = 0;
+        cc0.y0 = cc0.c1 = cc0.c2 = cc0.c3 = cc0.y1 = cc0.m1 = (T)0;
+        cc1 = cc0;
+        T tnum = (T)0, tden = (T)0;  // fast mode: this tile's SD partial sums
 #pragma unroll
         for (int i = 0; i < RUN_MAX; ++i) {
-            const int j = j0 + i, t = t0 + j;
-            if (i < run && j < tl) {
+            const int t = t0 + j0 + i;
+            if (i < nv) {
                 if (sifting) {
-                    const double h = hv[i];
-                    const double eu = (S.P[0] < 2) ? S.cval[0]
-                                      : env_at<T, EXACT>(sm, 0, cl[0] + mirror_adj(S, 0, t), t, lo2[0], S.p2[0]);
-                    const double el = (S.P[1] < 2) ? S.cval[1]
-                                      : env_at<T, EXACT>(sm, 1, cl[1] + mirror_adj(S, 1, t), t, lo2[1], S.p2[1]);
-                    cl[0] += (kmx >> i) & 1u;
-                    cl[1] += (kmn >> i) & 1u;
-                    const double m = 0.5 * (eu + el);
-                    const double hn = rnd<T>(h - m);
+                    const T h = hv[i];
+                    const T eu = env_value<T, EXACT>(S, cc0, sm, 0, cl0 + mirror_adj(S, 0, t), t, lo0);
+                    const T el = env_value<T, EXACT>(S, cc1, sm, 1, cl1 + mirror_adj(S, 1, t), t, lo1);
+                    cl0 += (kmx >> i) & 1u;
+                    cl1 += (kmn >> i) & 1u;
+                    const T m = (T)0.5 * (eu + el);
+                    const T hn = h - m;
                     fv[i] = hn;
-                    if (C.rules == EEMD_RULES_NUMBA) {
-                        num = EXACT ? num + m * m : fma(m, m, num);
+                    if (EXACT) {
+                        const double dd = (C.rules == EEMD_RULES_NUMBA) ? (double)m : (double)(h - hn);
+                        num = num + dd * dd;
+                        den = den + (double)h * (double)h;
                     } else {
-                        const double dd = h - hn;
-                        num = EXACT ? num + dd * dd : fma(dd, dd, num);
+                        const T dd = (C.rules == EEMD_RULES_NUMBA) ? m : h - hn;
+                        tnum = fmat(dd, dd, tnum);
+                        tden = fmat(h, h, tden);
                     }
-                    den = EXACT ? den + h * h : fma(h, h, den);
-                    gv[i] = (mode == TM_LAST) ? rnd<T>(rv[i] - hn) : hn;
+                    gv[i] = (mode == TM_LAST) ? rv[i] - hn : hn;
                 } else if (mode == TM_TRANS) {
-                    fv[i] = rnd<T>(rv[i] - (S.imf_from_resid ? rv[i] : hv[i]));
+                    fv[i] = rv[i] - (S.imf_from_resid ? rv[i] : hv[i]);
                     gv[i] = fv[i];
                 } else {  // TM_INIT
-                    fv[i] = trial_input<T>(C, d, t);
+                    fv[i] = (T)trial_input<T>(C, d, t);
                     gv[i] = fv[i];
                 }
-                sm.f[1 + j] = fv[i];
-                sm.g[1 + j] = gv[i];
             }
         }
-        if (tid == 0) {
-            // halo samples t0-1 (first tile of the segment) and t0+tl
-            for (int side = 0; side < 2; ++side) {
-                int jj, t;
-                if (side == 0) {
-                    if (!(first && t0 > 0)) continue;
-                    jj = 0;
-                    t = t0 - 1;
-                } else {
-                    if (t0 + tl >= n) continue;
-                    jj = tl + 1;
-                    t = t0 + tl;
-                }
-                double fn, gn;
-                if (sifting) {
-                    double e2[2];
-                    for (int env = 0; env < 2; ++env) {
-                        if (S.P[env] < 2) {
-                            e2[env] = S.cval[env];
-                        } else {
-                            const int c = (side == 0 ? kb[env] - S.left_knot[env] : kb[env] + kc[env]) +
-                                          mirror_adj(S, env, t);
-                            e2[env] = env_at<T, EXACT>(sm, env, c, t, lo2[env], S.p2[env]);
-                        }
-                    }
-                    const double m = 0.5 * (e2[0] + e2[1]);
-                    fn = rnd<T>((double)hb[jj] - m);
-                    gn = (mode == TM_LAST) ? rnd<T>((double)rb[jj] - fn) : fn;
-                } else if (mode == TM_TRANS) {
-                    const double ro = (double)rb[jj];
-                    fn = rnd<T>(ro - (S.imf_from_resid ? ro : (double)hb[jj]));
-                    gn = fn;
-                } else {
-                    fn = trial_input<T>(C, d, t);
-                    gn = fn;
-                }
-                sm.f[jj] = fn;
-                sm.g[jj] = gn;
+        if (!EXACT) {
+            num += (double)tnum;
+            den += (double)tden;
+        }
+        // halo samples: t0-1 (first tile of the segment, thread 0) and t0+tl (last owner)
+        const int u_last = (tl - 1) / run;
+        for (int side = 0; side < 2; ++side) {
+            int t, hj;
+            if (side == 0) {
+                if (!(tid == 0 && first && t0 > 0)) continue;
+                t = t0 - 1;
+                hj = -1;
+            } else {
+                if (!(tid == u_last && t0 + tl < n)) continue;
+                t = t0 + tl;
+                hj = tl;
+            }
+            T fn, gn;
+            if (sifting) {
+                IvCache<T> h0, h1;
+                h0.k = h1.k = -1;
+                const int c0v = (side == 0 ? kb0 - S.left_knot[0] : kb0 + kc0) + mirror_adj(S, 0, t);
+                const int c1v = (side == 0 ? kb1 - S.left_knot[1] : kb1 + kc1) + mirror_adj(S, 1, t);
+                const T eu = env_value<T, EXACT>(S, h0, sm, 0, c0v, t, lo0);
+                const T el = env_value<T, EXACT>(S, h1, sm, 1, c1v, t, lo1);
+                const T m = (T)0.5 * (eu + el);
+                fn = hb[hj] - m;
+                gn = (mode == TM_LAST) ? rb[hj] - fn : fn;
+            } else if (mode == TM_TRANS) {
+                const T ro = rb[hj];
+                fn = ro - (S.imf_from_resid ? ro : hb[hj]);
+                gn = fn;
+            } else {
+                fn = (T)trial_input<T>(C, d, t);
+                gn = fn;
+            }
+            if (side == 0) {
+                S.fl = fn;
+                S.gl = gn;
+            } else {
+                S.fr = fn;
+                S.gr = gn;
             }
         }
+        SUB(3);
+        // run edges for the neighbours' flags
+        const T glast_mine = (run == 1) ? gv[0] : (run == 2) ? gv[1] : gv[RUN_MAX - 1];
+        if (lane == 0) s_gfirst[wid] = gv[0];
+        if (lane == 31) s_glast[wid] = glast_mine;
         __syncthreads();
-        const double* G = sm.g;  // signal whose extrema are the next knots
+        SUB(4);
 
-        // ---------------- (e) next knots ----------------
+        // ---------------- (e) next knots: strict extrema of the new values ----------------
+        const T up = __shfl_up_sync(0xffffffffu, glast_mine, 1);
+        const T dn = __shfl_down_sync(0xffffffffu, gv[0], 1);
+        T gprev, gnext;
+        if (j0 == 0) gprev = first ? (t0 > 0 ? (T)S.gl : (T)0) : (T)S.g_m1;
+        else gprev = (lane > 0) ? up : s_glast[wid - 1];
+        if (j0 + nv == tl) gnext = (t0 + tl < n) ? (T)S.gr : (T)0;
+        else gnext = (lane < 31) ? dn : s_gfirst[wid + 1];
         unsigned nmx = 0u, nmn = 0u;
 #pragma unroll
         for (int i = 0; i < RUN_MAX; ++i) {
-            const int j = j0 + i, t = t0 + j;
-            if (i < run && j < tl && t >= 1 && t <= n - 2) {
-                const double a = G[j], c = G[j + 2], v = gv[i];
+            const int t = t0 + j0 + i;
+            if (i < nv && t >= 1 && t <= n - 2) {
+                const T a = (i == 0) ? gprev : gv[(i + RUN_MAX - 1) % RUN_MAX];
+                const T c = (i + 1 == nv) ? gnext : gv[(i + 1) % RUN_MAX];
+                const T v = gv[i];
                 if (v > a && v > c) nmx |= 1u << i;
                 if (v < a && v < c) nmn |= 1u << i;
             }
         }
         int ex2, en2, tx2, tn2;
         block_scan2(__popc(nmx), __popc(nmn), ex2, en2, tx2, tn2, s_w2);
+        SUB(5);
 
         // ---------------- (f) writes ----------------
         {
@@ -890,12 +1064,12 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, const Sm
             int px = S.run_new[0] + ex2, pn = S.run_new[1] + en2;
 #pragma unroll
             for (int i = 0; i < RUN_MAX; ++i) {
-                const int j = j0 + i, t = t0 + j;
-                if (i < run && j < tl) {
+                const int t = t0 + j0 + i;
+                if (i < nv) {
                     if ((nmx >> i) & 1u) {
                         if (px < C.segcap) {
                             sl.kt[pmx + px] = t;
-                            static_cast<T*>(sl.ky)[pmx + px] = (T)gv[i];
+                            static_cast<T*>(sl.ky)[pmx + px] = gv[i];
                         } else {
                             raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
                         }
@@ -904,52 +1078,72 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, const Sm
                     if ((nmn >> i) & 1u) {
                         if (pn < C.segcap) {
                             sl.kt[pmn + pn] = t;
-                            static_cast<T*>(sl.ky)[pmn + pn] = (T)gv[i];
+                            static_cast<T*>(sl.ky)[pmn + pn] = gv[i];
                         } else {
                             raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
                         }
                         ++pn;
                     }
-                    switch (mode) {
-                        case TM_SIFT: imf_m[t] = (T)fv[i]; break;
-                        case TM_LAST: imf_m[t] = (T)fv[i]; resid[t] = (T)gv[i]; break;
-                        case TM_TRANS:
-                            resid[t] = (T)fv[i];
-                            if (S.imf_from_resid) imf_m[t] = (T)rv[i];
-                            break;
-                        default: resid[t] = (T)fv[i]; break;
+                }
+            }
+            const int tj = t0 + j0;
+            switch (mode) {
+                case TM_SIFT: store_run<T>(imf_m + tj, fv, nv); break;
+                case TM_LAST:
+                    store_run<T>(imf_m + tj, fv, nv);
+                    store_run<T>(resid + tj, gv, nv);
+                    break;
+                case TM_TRANS:
+                    store_run<T>(resid + tj, fv, nv);
+                    if (S.imf_from_resid) store_run<T>(imf_m + tj, rv, nv);
+                    break;
+                default: store_run<T>(resid + tj, fv, nv); break;
+            }
+            // edge and carry values of the tile, written by the threads that hold them
+#pragma unroll
+            for (int i = 0; i < RUN_MAX; ++i) {
+                if (i >= nv) continue;
+                const int j = j0 + i;
+                if (first && j == 0) { S.hf0 = fv[i]; S.rf0 = gv[i]; }
+                if (first && j == 1) { S.hf1 = fv[i]; S.rf1 = gv[i]; }
+                if (j == tl - 2) { S.f_last2 = fv[i]; S.g_last2 = gv[i]; }
+                if (j == tl - 1) {
+                    if (last) {
+                        Xchg& xo = X[q];
+                        xo.hl[0] = (tl >= 2) ? 0.0 : S.f_m1;  // completed below for tl >= 2
+                        xo.hl[1] = fv[i];
+                        xo.rl[0] = (tl >= 2) ? 0.0 : S.g_m1;
+                        xo.rl[1] = gv[i];
+                    }
+                    S.f_m1 = fv[i];
+                    S.g_m1 = gv[i];
+                    if (sifting) {
+                        S.hold_m1 = hv[i];
+                        S.hold_m2 = (tl >= 2) ? (double)hb[tl - 2] : (double)hb[-1];
                     }
                 }
             }
         }
-        // ---------------- (g) carry to the next tile, segment edges ----------------
+        __syncthreads();
         if (tid == 0) {
-            if (first) {
-                S.hf0 = sm.f[1];
-                S.hf1 = (tl >= 2) ? sm.f[2] : 0.0;
-                S.rf0 = G[1];
-                S.rf1 = (tl >= 2) ? G[2] : 0.0;
+            if (last && tl >= 2) {
+                X[q].hl[0] = S.f_last2;
+                X[q].rl[0] = S.g_last2;
             }
-            if (last) {
-                Xchg& xo = X[q];
-                xo.hl[0] = (tl >= 2) ? sm.f[tl - 1] : S.f_m1;
-                xo.hl[1] = sm.f[tl];
-                xo.rl[0] = (tl >= 2) ? G[tl - 1] : S.g_m1;
-                xo.rl[1] = G[tl];
-            }
-            S.f_m1 = sm.f[tl];
-            S.g_m1 = G[tl];
-            if (sifting) {
-                S.hold_m2 = (tl >= 2) ? (double)hb[tl - 1] : (double)hb[0];
-                S.hold_m1 = (double)hb[tl];
-            }
-            S.run_cur[0] += kc[0];
-            S.run_cur[1] += kc[1];
+            S.run_cur[0] += kc0;
+            S.run_cur[1] += kc1;
             S.run_new[0] += tx2;
             S.run_new[1] += tn2;
         }
         __syncthreads();
+        SUB(6);
     }
+#ifdef EEMD_TRACE
+    if (tid == 0) {
+        for (int k = 0; k < 7; ++k) atomicAdd(&C.hdr->sweep_cycles[k], scyc[k]);
+    }
+#endif
+#undef SUB
     // ---------------- publish the segment's results ----------------
     const double2 rs = block_sum2<THREADS>(make_double2(num, den), s_red);
     if (tid == 0) {
@@ -1118,8 +1312,12 @@ __device__ void step_setup(const Ctx& C, const Slot& sl, TaskSm& S) {
 // ---------------------------------------------------------------------------
 // k_emd: the persistent cluster kernel
 // ---------------------------------------------------------------------------
+#ifndef EEMD_MIN_CTAS_PER_SM
+#define EEMD_MIN_CTAS_PER_SM 2
+#endif
+
 template <typename T, bool EXACT>
-__global__ void __launch_bounds__(THREADS, 2) k_emd(Ctx C) {
+__global__ void __launch_bounds__(THREADS, EEMD_MIN_CTAS_PER_SM) k_emd(const __grid_constant__ Ctx C) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ TaskSm S;
     __shared__ Xchg X[2];
@@ -1133,7 +1331,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_emd(Ctx C) {
     Slot sl;
     sl.kt = C.kt + (int64_t)slot * C.slot_knots;
     sl.ky = static_cast<T*>(C.ky) + (int64_t)slot * C.slot_knots;
-    sl.M = C.M + (int64_t)slot * C.slot_M;
+    sl.M = static_cast<T*>(C.M) + (int64_t)slot * C.slot_M;
 
 #ifdef EEMD_TRACE
     unsigned long long cyc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -1407,7 +1605,7 @@ int make_layout(const eemd_params* p, const int64_t* lengths, int n_signals, int
     L.slots = (int)std::max<int64_t>(
         1, std::min<int64_t>(n_tasks, (int64_t)ASSUMED_SMS * ASSUMED_CTAS_PER_SM / L.csize));
     L.slot_knots = (int64_t)2 * 2 * L.csize * L.segcap;
-    L.slot_M = (int64_t)2 * L.kcap;
+    L.slot_M = (int64_t)2 * 5 * L.kcap;
     L.scr_rows = p->exact ? (L.B + L.S) : 0;
     L.NS = so;
     L.NIMF = imo;
@@ -1428,7 +1626,7 @@ int make_layout(const eemd_params* p, const int64_t* lengths, int n_signals, int
     L.o_imfs = imfs_external ? 0 : take(bt * L.NIMF);
     L.o_kt = take(sizeof(int32_t) * L.slot_knots * L.slots);
     L.o_ky = take(bt * L.slot_knots * L.slots);
-    L.o_M = take(sizeof(double) * L.slot_M * L.slots);
+    L.o_M = take(bt * L.slot_M * L.slots);
     L.o_scr = take(sizeof(double2) * (size_t)L.scr_rows * L.slots * L.csize * THREADS);
     L.total = off;
     return EEMD_OK;
@@ -1613,7 +1811,7 @@ int32_t eemd_run_traced(const eemd_params* p, const void* x, const int64_t* leng
     C.imfs = imfs ? imfs : (void*)(base + L.o_imfs);
     C.kt = reinterpret_cast<int32_t*>(base + L.o_kt);
     C.ky = base + L.o_ky;
-    C.M = reinterpret_cast<double*>(base + L.o_M);
+    C.M = base + L.o_M;
     C.scr = reinterpret_cast<double2*>(base + L.o_scr);
     C.x = x;
     C.noise = noise;

@@ -49,6 +49,9 @@ struct Header {
     // -DEEMD_TRACE builds: SM cycles spent per phase, summed over CTAs
     // (0 setup, 1 solve, 2 barrier after solve, 3 sweep, 4 barrier after sweep, 5 decide, 6 claim)
     unsigned long long phase_cycles[8];
+    // sweep sub-phases (thread 0 of each CTA): 0 tile wait+halo, 1 masks+scan,
+    // 2 staging wait, 3 values, 4 edges barrier, 5 flags+scan, 6 writes+barriers
+    unsigned long long sweep_cycles[8];
 };
 
 struct TaskDesc {
@@ -86,14 +89,16 @@ struct Ctx {
     void* imfs;                   // IMF slots per task (dtype)
     int32_t* kt;                  // per slot: [2 parity][2 env][C seg][segcap] knot sample index
     void* ky;                     // per slot: same layout, knot value (dtype)
-    double* M;                    // per slot: [2 env][kcap] second derivatives (mirror space)
+    void* M;                      // per slot: [2 env][5][kcap] interval records (mirror space,
+                                  //   storage type): plane 0 = t_k; fast: monomial c0..c3 of
+                                  //   interval [k, k+1]; exact: y_k, M_k
     double2* scr;                 // exact-mode solve scratch: [rows][grid threads]
     const void* x;
     const void* noise;
     int32_t* knot_log;            // optional [task][max_imf][max_sifts][2]
     int32_t* mode_sifts;          // optional [task][max_imf]
     int64_t slot_knots;           // kt/ky elements per slot
-    int64_t slot_M;               // M doubles per slot
+    int64_t slot_M;               // record elements per slot
     int32_t segcap;               // knots of one kind per segment list
     int32_t kcap;                 // knots per envelope in mirror space (M plane size)
     int32_t n_tasks, n_signals, trial_count, csize;

@@ -9,11 +9,15 @@ from __future__ import annotations
 import numpy as np
 
 PHASES = ("setup", "solve", "barrier_solve", "sweep", "barrier_sweep", "decide", "claim")
+SWEEP_PHASES = ("tile_wait", "masks_scan", "staging_wait", "values", "edges_barrier", "flags_scan",
+                "writes_barriers")
 _HEADER_INTS = 16  # int32 fields before phase_cycles
 
 
 def phase_cycles(ws) -> dict:
     """Cycles per phase summed over CTAs, from a workspace tensor after a traced run."""
-    raw = ws[: _HEADER_INTS * 4 + 8 * 8].cpu().numpy().view(np.uint8)
+    raw = ws[: _HEADER_INTS * 4 + 16 * 8].cpu().numpy().view(np.uint8)
     cyc = raw[_HEADER_INTS * 4:].view(np.uint64)
-    return {name: int(cyc[i]) for i, name in enumerate(PHASES)}
+    out = {name: int(cyc[i]) for i, name in enumerate(PHASES)}
+    out.update({"sweep." + name: int(cyc[8 + i]) for i, name in enumerate(SWEEP_PHASES)})
+    return out
