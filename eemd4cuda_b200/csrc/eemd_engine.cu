@@ -196,11 +196,12 @@ __global__ void __launch_bounds__(1024) k_sigma(const SignalDesc* sdesc, const v
 // ---------------------------------------------------------------------------
 // per-CTA task context (shared memory)
 // ---------------------------------------------------------------------------
+constexpr int NWARP = THREADS / 32;
+constexpr int MAXSEG = 8 * NWARP;  // knot segments per task: one per warp of up to 8 CTAs
+
 struct Xchg {              // one CTA's published segment results (DSMEM-visible)
-    double hf[2], hl[2];   // h after the step: first two / last two samples of the segment
-    double rf[2], rl[2];   // residual after the step: same positions
     double num, den;       // SD partial sums of the segment
-    int cnt[2];            // new knots (maxima, minima) found in the segment
+    int cnt[2][NWARP];     // new knots (maxima, minima) found by each warp
 };
 
 struct TaskSm {
@@ -208,64 +209,50 @@ struct TaskSm {
     int phase, imf, sift, kpar, src_resid, imf_from_resid;
     int nsift_total, nmode, mode_sifts_cur, flags, step, mode;
     int P[2];                  // current knot totals
-    int pref[2][MAXC + 1];     // current knots before each segment
+    int pref[2][2][MAXSEG + 1];  // [list parity][env]: knots before each (CTA, warp) segment
     int mir[2], p2[2], tfirst[2], tlast[2];
     double yfirst[2], ylast[2];  // values of the virtual mirror knots
     double cval[2];            // constant envelope when P == 1
-    // sweep scalars
-    int left_knot[2];
-    int run_cur[2], run_new[2];
-    double hold_m1, hold_m2, rold_m1, rold_p, hold_p, f_m1, g_m1;
-    double hf0, hf1, rf0, rf1;
-    double fl, gl, fr, gr;     // new value / new residual at the tile's halo samples
-    double f_last2, g_last2;   // new value / residual at the tile's second-to-last sample
+    int rcur;                  // current residual: 0 = the task's residual array, 1 = slot scratch
 };
 
+// Per-warp sweep geometry for storage type T.  A warp tile is WT = 32*RUN
+// samples; each warp owns, in dynamic shared memory, two tile buffers per
+// stream (h, residual) and two sets of run records.  Interval records are
+// RS storage-type elements (32 or 48 bytes).
+template <typename T>
+struct Geo {
+    static constexpr int RUN = sizeof(T) == 4 ? 8 : 4;  // consecutive samples per lane
+    static constexpr int WT = 32 * RUN;                 // samples per warp tile
+    static constexpr int TB = WT + 4;                   // tile buffer elements (16-byte phase)
+    static constexpr int RS = sizeof(T) == 4 ? 8 : 6;   // interval record stride
+    static constexpr size_t TB_BYTES = (size_t)2 * 2 * TB * sizeof(T);  // [buf][stream][TB]
+    static constexpr size_t RI_BYTES = (size_t)2 * 32 * 16;             // [buf][lane]
+    static constexpr size_t WARP_BYTES = TB_BYTES + RI_BYTES;
+    static_assert(TB_BYTES % 16 == 0 && (RS * sizeof(T)) % 16 == 0, "16-byte aligned layouts");
+};
+
+
+// solve staging (a different phase from the sweep; overlays the same memory)
 struct Smem {
-    void* hT[2];     // [TILE+8] old h, storage type (double buffer; the tile's sample 0 sits at
-                     //          index TOFF + (16-byte phase of its global address), so that
-                     //          16-byte copies line up; left halo just before, right halo after)
-    void* rT[2];     // [TILE+8] residual, storage type (double buffer, same placement)
-    void* kt;        // [2][cap] staged interval records, storage type: knot index bit pattern
-    void* c[4];      // [2][cap] fast: monomial c0..c3 of the interval; exact: c[0] = y, c[1] = M
     int* skt;        // solve staging (padded): knot sample index
     void* sky;       // solve staging (padded): knot value, storage type
     double* ssl;     // solve staging (padded): slope of the interval starting at the knot
-    int cap;
 };
-
-constexpr int RUN_MAX = 4;            // consecutive samples per thread in a tile
-constexpr int NWARP = THREADS / 32;
-constexpr int TOFF = 4;               // tile buffer index of the first 16-byte boundary used
 
 __host__ __device__ inline int stage_pad(int k) { return k + (k >> 4); }
 
 __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 
-__host__ __device__ inline size_t smem_bytes(int TILE, int bt) {
-    const size_t cap = (size_t)(TILE >> 1) + 8;
-    const size_t tile = align16((size_t)(TILE + 8) * bt);
-    const size_t sweep = 4 * tile + 10 * align16(cap * bt);
+__host__ __device__ inline size_t smem_bytes(int bt) {
+    const size_t sweep = NWARP * (bt == 8 ? Geo<double>::WARP_BYTES : Geo<float>::WARP_BYTES);
     const size_t sp = (size_t)stage_pad(SOLVE_CAP);
     const size_t solve = align16(sp * 8) + align16(sp * 4) + align16(sp * bt);
     return sweep > solve ? sweep : solve;
 }
 
-template <typename T>
-__device__ __forceinline__ Smem carve(unsigned char* base, int TILE) {
+__device__ __forceinline__ Smem carve(unsigned char* base) {
     Smem m;
-    const size_t cap = (size_t)(TILE >> 1) + 8;
-    m.cap = (int)cap;
-    const size_t tile = align16((size_t)(TILE + 8) * sizeof(T));
-    const size_t plane = 2 * align16(cap * sizeof(T));
-    unsigned char* p = base;
-    m.hT[0] = p; p += tile;
-    m.hT[1] = p; p += tile;
-    m.rT[0] = p; p += tile;
-    m.rT[1] = p; p += tile;
-    m.kt = p; p += plane;
-    for (int i = 0; i < 4; ++i) { m.c[i] = p; p += plane; }
-    // solve staging overlays the sweep buffers (used in a different phase)
     const size_t sp = (size_t)stage_pad(SOLVE_CAP);
     m.ssl = reinterpret_cast<double*>(base);
     m.skt = reinterpret_cast<int*>(base + align16(sp * 8));
@@ -281,15 +268,17 @@ struct Slot {
     int32_t* kt;   // knot lists (segmented)
     void* ky;
     void* M;       // interval records, mirror space: [2 env][5][kcap] storage type
+    void* w1;      // scratch h buffer of the running task (storage type)
+    void* r1;      // second residual buffer of the running task (storage type)
+    int4* ri;      // run records [2 parity][runs]: first knot of each kind, knot masks
 };
 
 __device__ __forceinline__ int64_t knot_index(const Ctx& C, int par, int env, int seg, int i) {
-    return ((int64_t)((par * 2 + env) * C.csize + seg)) * C.segcap + i;
+    return ((int64_t)((par * 2 + env) * C.csize * NWARP + seg)) * C.segcap + i;
 }
 
-// segment holding real knot i: largest r with pref[r] <= i
-__device__ __forceinline__ int seg_of(const int* pref, int csize, int i) {
-    int lo = 0, hi = csize;  // pref[lo] <= i < pref[hi]
+// segment holding real knot i: largest r in [lo, hi) with pref[r] <= i
+__device__ __forceinline__ int seg_of(const int* pref, int lo, int hi, int i) {
     while (hi - lo > 1) {
         const int mid = (lo + hi) >> 1;
         if (pref[mid] <= i) lo = mid; else hi = mid;
@@ -297,11 +286,11 @@ __device__ __forceinline__ int seg_of(const int* pref, int csize, int i) {
     return lo;
 }
 
-// element offset of real knot i in the current knot plane
+// element offset of real knot i in the current knot lists
 __device__ __forceinline__ int64_t real_off(const Ctx& C, const TaskSm& S, int env, int i) {
-    const int* pr = S.pref[env];
-    int r = S.rank;  // most lookups fall in the CTA's own segment
-    if (i < pr[r] || i >= pr[r + 1]) r = seg_of(pr, S.csize, i);
+    const int* pr = S.pref[S.kpar][env];
+    const int a = S.rank * NWARP, b = a + NWARP;  // most lookups fall in the CTA's own segments
+    const int r = (i >= pr[a] && i < pr[b]) ? seg_of(pr, a, b, i) : seg_of(pr, 0, S.csize * NWARP, i);
     return knot_index(C, S.kpar, env, r, i - pr[r]);
 }
 
@@ -390,14 +379,13 @@ __device__ __forceinline__ Row row_of(int ta, int tb, int tc, double sa, double 
 #define SKT(k) skt[stage_pad(k)]
 #define SSL(k) ssl[stage_pad(k)]
 
-// Interval records of one envelope in mirror space, five storage-type planes
-// of stride kcap: t_k (integer bit pattern), then four coefficient planes.
+// Interval records of one envelope in mirror space: RS storage-type elements
+// per record: [0] t_k (integer bit pattern), [1] y_k, [2] fast: c1 / exact:
+// M_k, [3] c2, [4] c3.
 template <typename T>
-struct Rec {  // plane 0: t_k; planes 1..4: c0..c3 (fast) or y_k, M_k (exact)
+struct Rec {
     T* rc;
-    int64_t stride;
-    __device__ __forceinline__ T& c(int plane, int k) const { return rc[(plane + 1) * stride + k]; }
-    __device__ __forceinline__ T& t(int k) const { return rc[k]; }
+    __device__ __forceinline__ T& at(int k, int e) const { return rc[(int64_t)k * Geo<T>::RS + e]; }
 };
 
 // exact: forward elimination from w0 (outer coupling dropped), back
@@ -430,9 +418,9 @@ __device__ void window_exact(const Ctx& C, const int* skt, const T* sky, const d
         sa = sb;
     }
     auto put = [&](int k, double Mk) {
-        R.t(k) = tbits<T>(SKT(k - base));
-        R.c(0, k) = sky[stage_pad(k - base)];
-        R.c(1, k) = (T)Mk;
+        R.at(k, 0) = tbits<T>(SKT(k - base));
+        R.at(k, 1) = sky[stage_pad(k - base)];
+        R.at(k, 2) = (T)Mk;
     };
     double xv = dp;
     if (w1 <= o1) put(w1 + 1, xv);
@@ -516,11 +504,11 @@ __device__ void window_fast(const Ctx& C, const int* skt, const T* sky, const do
     auto put = [&](int k, double Ma, double Mb) {
         const int t0 = SKT(k - base), t1 = SKT(k + 1 - base);
         const double h = (double)(t1 - t0);
-        R.t(k) = tbits<T>(t0);
-        R.c(0, k) = sky[stage_pad(k - base)];
-        R.c(1, k) = (T)fma(-h * (1.0 / 6.0), fma(2.0, Ma, Mb), SSL(k - base));
-        R.c(2, k) = (T)(0.5 * Ma);
-        R.c(3, k) = (T)((Mb - Ma) * fast_rcp(h) * (1.0 / 6.0));
+        R.at(k, 0) = tbits<T>(t0);
+        R.at(k, 1) = sky[stage_pad(k - base)];
+        R.at(k, 2) = (T)fma(-h * (1.0 / 6.0), fma(2.0, Ma, Mb), SSL(k - base));
+        R.at(k, 3) = (T)(0.5 * Ma);
+        R.at(k, 4) = (T)((Mb - Ma) * fast_rcp(h) * (1.0 / 6.0));
     };
     double xnext = 0.0;  // x_{i+1} of the previous iteration
 #pragma unroll
@@ -568,22 +556,21 @@ __device__ void solve_task(const Ctx& C, const Slot& sl, TaskSm& S, const Smem& 
         const int p2 = S.p2[env];
         const int n = p2 - 2;
         Rec<T> R;
-        R.rc = static_cast<T*>(sl.M) + (int64_t)env * 5 * C.kcap;
-        R.stride = C.kcap;
+        R.rc = static_cast<T*>(sl.M) + (int64_t)env * C.kcap * Geo<T>::RS;
         if (n <= 0) {
             // one or two knots: a constant or the straight line through them (M = 0)
             if (S.rank == 0 && tid < p2) {
                 int tk, t1;
                 double yk, y1;
                 knot2<T>(C, sl, S, env, tid, tk, yk);
-                R.t(tid) = tbits<T>(tk);
-                R.c(0, tid) = (T)yk;
-                R.c(1, tid) = (T)0;
-                R.c(2, tid) = (T)0;
-                R.c(3, tid) = (T)0;
+                R.at(tid, 0) = tbits<T>(tk);
+                R.at(tid, 1) = (T)yk;
+                R.at(tid, 2) = (T)0;
+                R.at(tid, 3) = (T)0;
+                R.at(tid, 4) = (T)0;
                 if (!EXACT && tid + 1 < p2) {
                     knot2<T>(C, sl, S, env, tid + 1, t1, y1);
-                    R.c(1, tid) = (T)((y1 - yk) / (double)(t1 - tk));
+                    R.at(tid, 2) = (T)((y1 - yk) / (double)(t1 - tk));
                 }
             }
             continue;
@@ -664,53 +651,72 @@ __device__ __forceinline__ void block_scan2(int a, int b, int& ea, int& eb, int&
     eb = bb + ib - b;
 }
 
-// Interval cache of one envelope for a thread's run of consecutive samples:
-// the staged record of interval k is loaded only when k changes.
+// One interval of an envelope (fast: monomial; exact: the two end knots).
 template <typename T>
-struct IvCache {
+struct Iv {
     int k, t0, t1;
-    T y0, c1, c2, c3, y1, m1;  // fast: monomial c0..c3 of interval k; exact: y0, M0, y1, M1
+    T y0, c1, c2, c3, y1, m1;  // fast: y0 + s(c1 + s(c2 + s c3)); exact: y0, M0 = c1, y1, M1
 };
 
+// loads interval record k (and k+1 in exact mode) of an envelope's record array
 template <typename T, bool EXACT>
-__device__ __forceinline__ T iv_value(IvCache<T>& cc, const Smem& sm, int env, int idx2, int lo2, int t) {
-    if (idx2 != cc.k) {
-        const T* kt = static_cast<const T*>(sm.kt);
-        const T* c0 = static_cast<const T*>(sm.c[0]);
-        const T* c1 = static_cast<const T*>(sm.c[1]);
-        const int o = env * sm.cap + (idx2 - lo2);
-        cc.k = idx2;
-        cc.t0 = tint<T>(kt[o]);
-        cc.y0 = c0[o];
-        cc.c1 = c1[o];
+__device__ __forceinline__ void load_iv(Iv<T>& v, const T* R, int k) {
+    constexpr int RS = Geo<T>::RS;
+    v.k = k;
+    const T* p = R + (int64_t)k * RS;
+    if constexpr (sizeof(T) == 4) {
+        const float4 a = *reinterpret_cast<const float4*>(p);
+        v.t0 = __float_as_int(a.x);
+        v.y0 = a.y;
+        v.c1 = a.z;
+        v.c2 = a.w;
+        v.c3 = p[4];
         if (EXACT) {
-            cc.t1 = tint<T>(kt[o + 1]);
-            cc.y1 = c0[o + 1];
-            cc.m1 = c1[o + 1];
-        } else {
-            cc.c2 = static_cast<const T*>(sm.c[2])[o];
-            cc.c3 = static_cast<const T*>(sm.c[3])[o];
+            const float4 c = *reinterpret_cast<const float4*>(p + RS);
+            v.t1 = __float_as_int(c.x);
+            v.y1 = c.y;
+            v.m1 = c.z;
+        }
+    } else {
+        const double2 a = *reinterpret_cast<const double2*>(p);
+        const double2 b = *reinterpret_cast<const double2*>(p + 2);
+        v.t0 = (int)__double_as_longlong(a.x);
+        v.y0 = a.y;
+        v.c1 = b.x;
+        v.c2 = b.y;
+        v.c3 = p[4];
+        if (EXACT) {
+            const double2 c = *reinterpret_cast<const double2*>(p + RS);
+            const double2 e = *reinterpret_cast<const double2*>(p + RS + 2);
+            v.t1 = (int)__double_as_longlong(c.x);
+            v.y1 = c.y;
+            v.m1 = e.x;
         }
     }
-    if (EXACT)
-        return (T)spline_exact((double)t, (double)cc.t0, (double)cc.t1, (double)cc.y0, (double)cc.y1,
-                               (double)cc.c1, (double)cc.m1);
-    const T s = (T)(t - cc.t0);
-    return fmat(s, fmat(s, fmat(s, cc.c3, cc.c2), cc.c1), cc.y0);
 }
 
-// envelope value at t with `cless` knots strictly before t (mirror space),
-// interval = searchsorted - 1 clipped (emd_ref.py:70)
 template <typename T, bool EXACT>
-__device__ __forceinline__ T env_value(const TaskSm& S, IvCache<T>& cc, const Smem& sm, int env, int cless,
-                                       int t, int lo2) {
-    if (S.P[env] < 2) return (T)S.cval[env];
-    const int idx2 = max(0, min(cless - 1, S.p2[env] - 2));
-    return iv_value<T, EXACT>(cc, sm, env, idx2, lo2, t);
+__device__ __forceinline__ T iv_eval(const Iv<T>& v, int t) {
+    if (EXACT)
+        return (T)spline_exact((double)t, (double)v.t0, (double)v.t1, (double)v.y0, (double)v.y1, (double)v.c1,
+                               (double)v.m1);
+    const T s = (T)(t - v.t0);
+    return fmat(s, fmat(s, fmat(s, v.c3, v.c2), v.c1), v.y0);
 }
 
 __device__ __forceinline__ int mirror_adj(const TaskSm& S, int env, int t) {
     return S.mir[env] ? (S.tfirst[env] < t ? 1 : 0) + (S.tlast[env] < t ? 1 : 0) : 0;
+}
+
+// envelope value at t with `cless` real knots strictly before t: mirror-space
+// interval = searchsorted - 1 clipped (emd_ref.py:70); reloads the interval
+// record only when the interval changes
+template <typename T, bool EXACT>
+__device__ __forceinline__ T env_at(const Ctx& C, const TaskSm& S, Iv<T>& v, const T* R, int env, int cless, int t) {
+    if (S.P[env] < 2) return (T)S.cval[env];
+    const int idx2 = max(0, min(cless + mirror_adj(S, env, t) - 1, S.p2[env] - 2));
+    if (idx2 != v.k) load_iv<T, EXACT>(v, R, idx2);
+    return iv_eval<T, EXACT>(v, t);
 }
 
 // element phase of an address within its 16-byte block
@@ -719,51 +725,164 @@ __device__ __forceinline__ int phase16(const T* p) {
     return (int)((reinterpret_cast<uintptr_t>(p) / sizeof(T)) & (16 / sizeof(T) - 1));
 }
 
-// stores a thread's run of samples: one 16-byte-vector pass when the run is
-// full and aligned, element stores otherwise
+// One warp copies g[0 .. cnt) to shared dst[0 .. cnt) asynchronously; dst + j
+// and g + j share their 16-byte phase, so the body moves in 16-byte copies.
 template <typename T>
-__device__ __forceinline__ void store_run(T* p, const T (&v)[RUN_MAX], int nv) {
-    if (nv == RUN_MAX && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+__device__ __forceinline__ void warp_copy(T* dst, const T* g, int cnt, int lane) {
+    constexpr int VEC = 16 / (int)sizeof(T);
+    const int head = min(cnt, (VEC - phase16(g)) & (VEC - 1));
+    const int nvec = (cnt - head) / VEC;
+    const int tail0 = head + nvec * VEC;
+    for (int v = lane; v < nvec; v += 32) cp_async16(dst + head + v * VEC, g + head + v * VEC);
+    const int ns = head + (cnt - tail0);
+    if (lane < ns) {
+        const int j = (lane < head) ? lane : tail0 + (lane - head);
+        cp_async_el<T>(dst + j, g + j);
+    }
+}
+
+// stores a thread's run of samples: 16-byte vectors when the run is full and
+// aligned, element stores otherwise
+template <typename T, int RUN>
+__device__ __forceinline__ void store_run(T* p, const T (&v)[RUN], int nv) {
+    if (nv == RUN && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
         if constexpr (sizeof(T) == 4) {
-            *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+#pragma unroll
+            for (int i = 0; i < RUN; i += 4)
+                *reinterpret_cast<float4*>(p + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
         } else {
-            reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
-            reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+#pragma unroll
+            for (int i = 0; i < RUN; i += 2) *reinterpret_cast<double2*>(p + i) = make_double2(v[i], v[i + 1]);
         }
         return;
     }
 #pragma unroll
-    for (int i = 0; i < RUN_MAX; ++i)
+    for (int i = 0; i < RUN; ++i)
         if (i < nv) p[i] = v[i];
 }
 
-// The sweep streams the CTA's segment in tiles of TILE samples; thread u owns
-// the run of TILE/THREADS consecutive samples starting at u*TILE/THREADS and
-// keeps its samples in registers.  The next tile is copied to shared memory
-// (cp.async, 16-byte copies where the addresses allow) while the current one
-// is processed; the interval records a tile needs are staged with one batch
-// of asynchronous copies.  Arithmetic runs in the storage type T: the spline
-// solve that produced the records ran in double, and the exact mode (double
-// only) keeps the reference operation order.
-template <typename T, bool EXACT>
-__device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, const Smem& sm,
-                      cg::cluster_group& cl) {
-    constexpr int VEC = 16 / (int)sizeof(T);
+// value at tile position pos (lane pos/RUN, element pos%RUN), to every lane
+template <typename T, int RUN>
+__device__ __forceinline__ T tile_at(const T (&v)[RUN], int pos) {
+    const int e = pos % RUN;
+    T x = v[0];
+#pragma unroll
+    for (int i = 1; i < RUN; ++i)
+        if (e == i) x = v[i];
+    return __shfl_sync(0xffffffffu, x, pos / RUN);
+}
+
+// Pointers and flags of one sweep step.
+template <typename T>
+struct StepIo {
+    const T* hsrc;   // h read by the step (sifting, TRANS from a sift)
+    const T* rcur;   // current residual
+    T* rnxt;         // residual written by LAST / TRANS / INIT
+    T* hdst;         // h written by SIFT
+    T* imf_m;        // the IMF slot (written by LAST, and by TRANS when the IMF is elsewhere)
+    bool trans_imf;  // TRANS copies the IMF into its slot
+};
+
+// new value f and next-knot value g of sample t from h / r (not the envelopes)
+template <typename T, int MODE>
+__device__ __forceinline__ void plain_value(const Ctx& C, const TaskSm& S, const TaskDesc& d, int t, T h, T r,
+                                            T& f, T& g) {
+    if (MODE == TM_TRANS) {
+        f = r - (S.imf_from_resid ? r : h);
+        g = f;
+    } else {  // TM_INIT
+        f = (T)trial_input<T>(C, d, t);
+        g = f;
+    }
+}
+
+// next-knot value of a sample outside the warp range (t = range start - 1 or
+// range end), evaluated by one lane from global memory
+template <typename T, bool EXACT, int MODE>
+__device__ T outside_g(const Ctx& C, const TaskSm& S, const TaskDesc& d, const StepIo<T>& io, const T* R0,
+                       const T* R1, int t, int cl0, int cl1) {
+    constexpr bool SIFTING = (MODE == TM_SIFT || MODE == TM_LAST);
+    const T h = (SIFTING || (MODE == TM_TRANS && !S.imf_from_resid)) ? __ldcg(io.hsrc + t) : (T)0;
+    const T r = (MODE == TM_LAST || MODE == TM_TRANS) ? __ldcg(io.rcur + t) : (T)0;
+    if (SIFTING) {
+        Iv<T> v0, v1;
+        v0.k = v1.k = -1;
+        const T eu = env_at<T, EXACT>(C, S, v0, R0, 0, cl0, t);
+        const T el = env_at<T, EXACT>(C, S, v1, R1, 1, cl1, t);
+        const T fn = h - (T)0.5 * (eu + el);
+        return (MODE == TM_LAST) ? r - fn : fn;
+    }
+    T f, g;
+    plain_value<T, MODE>(C, S, d, t, h, r, f, g);
+    return g;
+}
+
+// The sweep.  The CTA's segment [s0, s1) is cut into warp tiles of WT = 32*RUN
+// samples and warp w owns the contiguous tiles [w*NT/8, (w+1)*NT/8); lane u
+// of a tile owns the run of RUN samples at u*RUN.  Each warp works through
+// its range without block-wide barriers and keeps its own knot lists (one
+// knot segment per warp, so no cross-warp prefix is needed).  Per tile:
+//   - the tile's samples of each stream it reads and its run records from
+//     the previous step (per run: position of the run's first current knot
+//     of each kind in the warp's knot lists, and the run's knot masks) are
+//     already in shared memory: cp.async, issued during the previous tile;
+//   - each lane knows the interval of every sample from its run record, and
+//     loads an interval record (32 or 48 bytes) only when the interval
+//     changes; interior tiles take a path without end handling;
+//   - new values and SD partials; strict extrema of the new values with lane
+//     neighbours by shuffle; the tile's last sample is decided with the next
+//     tile (its right neighbour), so only the two samples just outside the
+//     warp's range are ever evaluated twice;
+//   - a warp-shuffle scan places the knots in the warp's lists, and the
+//     samples, knots and this step's run records are written.
+// Every step reads one set of buffers and writes another (ping-pong), so the
+// warps of a step never see each other's writes.
+template <typename T, bool EXACT, int MODE>
+__device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned char* smem) {
+    using G = Geo<T>;
+    constexpr int RUN = G::RUN, WT = G::WT, RS = G::RS;
+    constexpr unsigned FULL = 0xffffffffu;
+    constexpr bool SIFTING = (MODE == TM_SIFT || MODE == TM_LAST);
+    constexpr bool USES_R = (MODE == TM_LAST || MODE == TM_TRANS);
     __shared__ double2 s_red[NWARP];
-    __shared__ int s_w1[2 * NWARP], s_w2[2 * NWARP];
-    __shared__ T s_gfirst[NWARP], s_glast[NWARP];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int TILE = C.tile, run = TILE / THREADS, cap = sm.cap;
-    const int mode = S.mode, n = S.n, s0 = S.s0, s1 = S.s1, rank = S.rank;
-    const bool sifting = (mode == TM_SIFT || mode == TM_LAST);
-    const bool uses_r = (mode == TM_LAST || mode == TM_TRANS);
-    const bool needs_h = sifting || (mode == TM_TRANS && !S.imf_from_resid);
+    const int n = S.n, s0 = S.s0, s1 = S.s1, rank = S.rank;
+    const bool needs_h = SIFTING || (MODE == TM_TRANS && !S.imf_from_resid);
     const int q = S.step & 1;
     const TaskDesc d = C.td[S.task];
-    T* resid = static_cast<T*>(C.resid) + d.s_off;
-    T* imf_m = static_cast<T*>(C.imfs) + d.imf_off + (int64_t)min(S.imf, C.max_imf - 1) * n;
-    const T* src = (sifting && S.src_resid) ? resid : imf_m;
+    StepIo<T> io;
+    {
+        T* const r0 = static_cast<T*>(C.resid) + d.s_off;
+        T* const r1 = static_cast<T*>(sl.r1);
+        T* const w1 = static_cast<T*>(sl.w1);
+        io.imf_m = static_cast<T*>(C.imfs) + d.imf_off + (int64_t)min(S.imf, C.max_imf - 1) * n;
+        io.rcur = S.rcur ? r1 : r0;
+        io.rnxt = S.rcur ? r0 : r1;
+        // h buffers W0 = the IMF slot, W1 = slot scratch: sift k writes W[(max_sifts-1-k) & 1], so
+        // the last sift writes the IMF slot; sift k > 0 reads what sift k-1 wrote
+        const int wd = (C.max_sifts - 1 - S.sift) & 1;
+        io.hdst = wd ? w1 : io.imf_m;
+        io.hsrc = io.rcur;
+        if (SIFTING && !S.src_resid) io.hsrc = wd ? io.imf_m : w1;
+        if (MODE == TM_TRANS && !S.imf_from_resid) io.hsrc = io.hdst;  // the sift that stopped wrote it
+        io.trans_imf = (MODE == TM_TRANS) && (S.imf_from_resid || wd == 1);
+    }
+    const int4* ri_cur = sl.ri + (int64_t)S.kpar * C.slot_runs;
+    int4* ri_nxt = sl.ri + (int64_t)(S.kpar ^ 1) * C.slot_runs;
     const int np = S.kpar ^ 1;
+    const int seg = rank * NWARP + wid;
+    const int64_t pmx = knot_index(C, np, 0, seg, 0);
+    const int64_t pmn = knot_index(C, np, 1, seg, 0);
+    const T* R0 = static_cast<const T*>(sl.M);
+    const T* R1 = R0 + (int64_t)C.kcap * RS;
+    const int kbase0 = S.pref[S.kpar][0][seg], kbase1 = S.pref[S.kpar][1][seg];
+    const int nt = (s1 - s0 + WT - 1) / WT;
+    const int ta = wid * nt / NWARP, tb = (wid + 1) * nt / NWARP;
+    const int r0 = s0 + ta * WT, r1 = min(s1, s0 + tb * WT);  // the warp's range [r0, r1)
+
+    unsigned char* wb = smem + (size_t)wid * G::WARP_BYTES;
+    T* const tbuf = reinterpret_cast<T*>(wb);                      // [2 buf][2 stream][TB]
+    int4* const rib = reinterpret_cast<int4*>(wb + G::TB_BYTES);  // [2 buf][32]
     double num = 0.0, den = 0.0;
 #ifdef EEMD_TRACE
     unsigned long long scyc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -780,391 +899,306 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, const Sm
     } while (0)
 #endif
 
-    if (tid == 0) {
-        S.run_cur[0] = S.run_cur[1] = 0;
-        S.run_new[0] = S.run_new[1] = 0;
-        S.hold_m1 = S.hold_m2 = S.rold_m1 = S.hold_p = S.rold_p = 0.0;
-        if (mode != TM_INIT) {
-            // neighbours' edge samples from their previous step (distributed shared memory)
-            const bool hres = sifting && S.src_resid;
-            if (s0 > 0) {
-                const Xchg* xl = cl.map_shared_rank(&X[q ^ 1], rank - 1);
-                S.hold_m1 = hres ? xl->rl[1] : xl->hl[1];
-                S.hold_m2 = hres ? xl->rl[0] : xl->hl[0];
-                S.rold_m1 = xl->rl[1];
-            }
-            if (s1 < n) {
-                const Xchg* xr = cl.map_shared_rank(&X[q ^ 1], rank + 1);
-                S.hold_p = hres ? xr->rf[0] : xr->hf[0];
-                S.rold_p = xr->rf[0];
-            }
-        }
-    }
-    __syncthreads();
-
-    // copies g[0 .. cnt) to dst[0 .. cnt); dst + j and g + j share their
-    // 16-byte phase, so the body moves in 16-byte copies
-    auto copy_stream = [&](T* dst, const T* g, int cnt) {
-        const int head = min(cnt, (VEC - phase16(g)) & (VEC - 1));
-        const int nvec = (cnt - head) / VEC;
-        const int tail0 = head + nvec * VEC;
-        for (int v = tid; v < nvec; v += THREADS) cp_async16(dst + head + v * VEC, g + head + v * VEC);
-        const int ns = head + (cnt - tail0);
-        for (int k = tid; k < ns; k += THREADS) {
-            const int j = (k < head) ? k : tail0 + (k - head);
-            cp_async_el<T>(dst + j, g + j);
-        }
-    };
-    // tile buffer b positioned for the tile starting at t0p of stream g
-    auto tile_h = [&](int b, int t0p) { return static_cast<T*>(sm.hT[b]) + TOFF + phase16(src + t0p); };
-    auto tile_r = [&](int b, int t0p) { return static_cast<T*>(sm.rT[b]) + TOFF + phase16(resid + t0p); };
-    // copies samples [t0p, t0p+tl] (the extra one when it is still this segment's) to buffer b
-    auto prefetch = [&](int t0p, int b) {
-        const int tlp = min(TILE, s1 - t0p);
-        const int cnt = (t0p + tlp < s1) ? tlp + 1 : tlp;
-        if (needs_h) copy_stream(tile_h(b, t0p), src + t0p, cnt);
-        if (uses_r) copy_stream(tile_r(b, t0p), resid + t0p, cnt);
+    // tile j's samples [t0, t1) and run records into buffer b
+    auto prefetch = [&](int j, int b) {
+        const int t0 = s0 + j * WT, t1 = min(s1, t0 + WT);
+        if (needs_h) warp_copy<T>(tbuf + (b * 2) * G::TB + phase16(io.hsrc + t0), io.hsrc + t0, t1 - t0, lane);
+        if (USES_R) warp_copy<T>(tbuf + (b * 2 + 1) * G::TB + phase16(io.rcur + t0), io.rcur + t0, t1 - t0, lane);
+        if (SIFTING && lane * RUN < t1 - t0) cp_async16(rib + b * 32 + lane, ri_cur + t0 / RUN + lane);
         cp_async_commit();
     };
-    const bool streams = needs_h || uses_r;
-    if (streams) prefetch(s0, 0);
 
-    int buf = 0;
-    for (int t0 = s0; t0 < s1; t0 += TILE, buf ^= 1) {
-        const int tl = min(TILE, s1 - t0);
-        const bool first = (t0 == s0), last = (t0 + tl == s1);
-        const int j0 = tid * run;
-        const int nv = max(0, min(run, tl - j0));  // valid samples of this thread's run
-        T* hb = tile_h(buf, t0);  // hb[j] = sample t0+j, hb[-1] / hb[tl] halos
-        T* rb = tile_r(buf, t0);
-        // ---------------- (a) this tile's samples (prefetched), next tile's prefetch ----------------
-        if (streams) {
-            if (!last) {
-                prefetch(t0 + TILE, buf ^ 1);
-                cp_async_wait<1>();
-            } else {
-                cp_async_wait<0>();
+    int wcx = 0, wcy = 0;  // knots of each kind written to the warp's lists so far
+    T gm1 = (T)0, gm2 = (T)0;  // next-knot values at t0-1 and t0-2 of the current tile
+    int cpx = 0, cpn = 0, cmask = 0, crun = 0, cbit = 0;  // run record awaiting its last sample
+    if (ta < tb) {
+        prefetch(ta, 0);
+        if (r0 > 0) {
+            // the sample before the range: its value is the left neighbour of the range's first sample
+            int c0 = 0, c1 = 0;
+            if (SIFTING && lane == 0) {
+                const unsigned pm = (unsigned)__ldcg(&ri_cur[r0 / RUN - 1].z);
+                c0 = kbase0 - (int)((pm >> (RUN - 1)) & 1u);
+                c1 = kbase1 - (int)((pm >> (16 + RUN - 1)) & 1u);
             }
+            if (lane == 0) gm1 = outside_g<T, EXACT, MODE>(C, S, d, io, R0, R1, r0 - 1, c0, c1);
+            gm1 = __shfl_sync(FULL, gm1, 0);
         }
-        if (tid == 0) {
-            if (sifting) {
-                hb[-1] = (T)S.hold_m1;
-                if (last) hb[tl] = (T)((t0 + tl < n) ? S.hold_p : 0.0);
-            } else if (needs_h) {  // TM_TRANS: the closed IMF at the halo samples
-                hb[-1] = (first && t0 > 0) ? __ldcg(imf_m + t0 - 1) : (T)0;
-                if (last) hb[tl] = (t0 + tl < n) ? __ldcg(imf_m + t0 + tl) : (T)0;
-            }
-            if (uses_r) {
-                if (first) rb[-1] = (T)S.rold_m1;
-                if (last) rb[tl] = (T)((t0 + tl < n) ? S.rold_p : 0.0);
-            }
-        }
-        __syncthreads();
+    }
+
+    int b = 0;
+    for (int j = ta; j < tb; ++j, b ^= 1) {
+        const int t0 = s0 + j * WT, t1 = min(s1, t0 + WT), tl = t1 - t0;
+        const int j0 = lane * RUN;
+        const int nv = max(0, min(RUN, tl - j0));  // valid samples of this lane's run
+        const int last_lane = (tl - 1) / RUN;
+        cp_async_wait<0>();
+        __syncwarp();
+        if (j + 1 < tb) prefetch(j + 1, b ^ 1);
         SUB(0);
-        T hv[RUN_MAX], rv[RUN_MAX], fv[RUN_MAX], gv[RUN_MAX];
+        const T* hb = tbuf + (b * 2) * G::TB + (needs_h ? phase16(io.hsrc + t0) : 0);
+        const T* rb = tbuf + (b * 2 + 1) * G::TB + (USES_R ? phase16(io.rcur + t0) : 0);
+        T hv[RUN], rv[RUN], fv[RUN], gv[RUN];
 #pragma unroll
-        for (int i = 0; i < RUN_MAX; ++i) {
+        for (int i = 0; i < RUN; ++i) {
             const bool ok = i < nv;
             hv[i] = (ok && needs_h) ? hb[j0 + i] : (T)0;
-            rv[i] = (ok && uses_r) ? rb[j0 + i] : (T)0;
+            rv[i] = (ok && USES_R) ? rb[j0 + i] : (T)0;
             fv[i] = gv[i] = (T)0;
         }
 
-        // ---------------- (b) current knots: strict extrema of h in the run ----------------
-        unsigned kmx = 0u, kmn = 0u;
-        int kb0 = 0, kb1 = 0, kc0 = 0, kc1 = 0, lo0 = 0, lo1 = 0, hi0 = -1, hi1 = -1;
-        int cl0 = 0, cl1 = 0;
-        if (sifting) {
+        // ---------------- new values ----------------
+        if (SIFTING) {
+            unsigned kmx = 0u, kmn = 0u;
+            int kb0 = 0, kb1 = 0;
             if (nv > 0) {
-                const T hl0 = hb[j0 - 1], hr0 = hb[j0 + nv];
+                const int4 ri = rib[b * 32 + lane];
+                kmx = (unsigned)ri.z & 0xffffu;
+                kmn = (unsigned)ri.z >> 16;
+                kb0 = kbase0 + ri.x;
+                kb1 = kbase1 + ri.y;
+            }
+            // interior tile: every sample's interval is (knots before it) + mir - 1, no clipping
+            const int ta0 = t0 + j0, ta1 = t0 + j0 + nv - 1;
+            bool ok = S.P[0] >= 2 && S.P[1] >= 2;
 #pragma unroll
-                for (int i = 0; i < RUN_MAX; ++i) {
-                    const int t = t0 + j0 + i;
-                    if (i < nv && t >= 1 && t <= n - 2) {
-                        const T a = (i == 0) ? hl0 : hv[(i + RUN_MAX - 1) % RUN_MAX];
-                        const T c = (i + 1 == nv) ? hr0 : hv[(i + 1) % RUN_MAX];
-                        const T v = hv[i];
-                        if (v > a && v > c) kmx |= 1u << i;
-                        if (v < a && v < c) kmn |= 1u << i;
+            for (int env = 0; env < 2; ++env) {
+                const int kb = env ? kb1 : kb0;
+                const int kc = __popc(env ? kmn : kmx);
+                const int mir = S.mir[env];
+                ok = ok && (!mir || (S.tfirst[env] < ta0 && S.tlast[env] >= ta1));
+                ok = ok && (kb + mir >= 1) && (kb + kc + mir <= S.p2[env] - 1);
+            }
+            const bool fast = __all_sync(FULL, ok || nv == 0);
+            T tnum = (T)0, tden = (T)0;  // fast mode: this tile's SD partial sums
+            // sample i of the run from its envelope mean m: new h, SD terms, next-knot value
+            auto finish = [&](int i, T m) {
+                const T h = hv[i];
+                const T hn = h - m;
+                fv[i] = hn;
+                if (EXACT) {
+                    const double dd = (C.rules == EEMD_RULES_NUMBA) ? (double)m : (double)(h - hn);
+                    num = num + dd * dd;
+                    den = den + (double)h * (double)h;
+                } else {
+                    const T dd = (C.rules == EEMD_RULES_NUMBA) ? m : h - hn;
+                    tnum = fmat(dd, dd, tnum);
+                    tden = fmat(h, h, tden);
+                }
+                gv[i] = (MODE == TM_LAST) ? rv[i] - hn : hn;
+            };
+            if (fast) {
+                // current and next interval of each envelope; the next record is
+                // loaded as soon as the current one is entered
+                Iv<T> c0, n0, c1, n1;
+                c0.t0 = c0.t1 = 0;
+                c0.y0 = c0.c1 = c0.c2 = c0.c3 = c0.y1 = c0.m1 = (T)0;
+                n0 = c1 = n1 = c0;
+                int k0 = kb0 + S.mir[0] - 1, k1 = kb1 + S.mir[1] - 1;
+                if (nv > 0) {
+                    load_iv<T, EXACT>(c0, R0, k0);
+                    load_iv<T, EXACT>(c1, R1, k1);
+                    if (kmx) load_iv<T, EXACT>(n0, R0, k0 + 1);
+                    if (kmn) load_iv<T, EXACT>(n1, R1, k1 + 1);
+                }
+#pragma unroll
+                for (int i = 0; i < RUN; ++i) {
+                    if (i > 0 && ((kmx >> (i - 1)) & 1u)) {
+                        c0 = n0;
+                        ++k0;
+                        if (kmx >> i) load_iv<T, EXACT>(n0, R0, k0 + 1);
                     }
+                    if (i > 0 && ((kmn >> (i - 1)) & 1u)) {
+                        c1 = n1;
+                        ++k1;
+                        if (kmn >> i) load_iv<T, EXACT>(n1, R1, k1 + 1);
+                    }
+                    const int t = t0 + j0 + i;
+                    if (i < nv) finish(i, (T)0.5 * (iv_eval<T, EXACT>(c0, t) + iv_eval<T, EXACT>(c1, t)));
                 }
-            }
-            int ex, en, tx, tn;
-            block_scan2(__popc(kmx), __popc(kmn), ex, en, tx, tn, s_w1);
-            kc0 = tx;
-            kc1 = tn;
-            kb0 = S.pref[0][rank] + S.run_cur[0];
-            kb1 = S.pref[1][rank] + S.run_cur[1];
-            if (S.P[0] >= 2) {
-                lo0 = max(0, S.mir[0] + kb0 - 2);
-                hi0 = min(S.p2[0] - 1, S.mir[0] + kb0 + kc0 + 1);
-            }
-            if (S.P[1] >= 2) {
-                lo1 = max(0, S.mir[1] + kb1 - 2);
-                hi1 = min(S.p2[1] - 1, S.mir[1] + kb1 + kc1 + 1);
-            }
-            const bool bad0 = hi0 - lo0 + 1 > cap || kb0 + kc0 > S.P[0];
-            const bool bad1 = hi1 - lo1 + 1 > cap || kb1 + kc1 > S.P[1];
-            if ((bad0 || bad1) && tid == 0) raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
-            if (bad0) hi0 = lo0 - 1;
-            if (bad1) hi1 = lo1 - 1;
-            cl0 = kb0 + ex;
-            cl1 = kb1 + en;
-            SUB(1);
-            // ---------------- (c) stage the interval records the tile uses ----------------
-            const int n0 = hi0 - lo0 + 1, n1 = hi1 - lo1 + 1;
-            for (int k = tid; k < n0 + n1; k += THREADS) {
-                const int env = (k >= n0) ? 1 : 0;
-                const int kk = k - env * n0;
-                const int i2 = (env ? lo1 : lo0) + kk;
-                const int o = env * cap + kk;
-                const T* rc = static_cast<const T*>(sl.M) + (int64_t)env * 5 * C.kcap + i2;
-                cp_async_el<T>(static_cast<T*>(sm.kt) + o, rc);
-                cp_async_el<T>(static_cast<T*>(sm.c[0]) + o, rc + C.kcap);
-                cp_async_el<T>(static_cast<T*>(sm.c[1]) + o, rc + 2 * (int64_t)C.kcap);
-                if (!EXACT) {
-                    cp_async_el<T>(static_cast<T*>(sm.c[2]) + o, rc + 3 * (int64_t)C.kcap);
-                    cp_async_el<T>(static_cast<T*>(sm.c[3]) + o, rc + 4 * (int64_t)C.kcap);
-                }
-            }
-            cp_async_commit();
-            if (tid == 0) {
-                // is t0-1 a knot of each kind? (only the segment's first tile evaluates t0-1)
-                S.left_knot[0] = S.left_knot[1] = 0;
-                if (first && t0 - 1 >= 1 && t0 - 1 <= n - 2) {
-                    const T a = (T)S.hold_m2, b = hb[-1], c = hb[0];
-                    S.left_knot[0] = (b > a) && (b > c);
-                    S.left_knot[1] = (b < a) && (b < c);
-                }
-            }
-            cp_async_wait<0>();
-            __syncthreads();
-            SUB(2);
-        }
-
-        // ---------------- (d) new values ----------------
-        IvCache<T> cc0, cc1;
-        cc0.k = cc1.k = -1;
-        cc0.t0 = cc0.t1 = 0;
-        cc0.y0 = cc0.c1 = cc0.c2 = cc0.c3 = cc0.y1 = cc0.m1 = (T)0;
-        cc1 = cc0;
-        T tnum = (T)0, tden = (T)0;  // fast mode: this tile's SD partial sums
+            } else {
+                Iv<T> v0, v1;
+                v0.k = v1.k = -1;
+                int cl0 = kb0, cl1 = kb1;
 #pragma unroll
-        for (int i = 0; i < RUN_MAX; ++i) {
-            const int t = t0 + j0 + i;
-            if (i < nv) {
-                if (sifting) {
-                    const T h = hv[i];
-                    const T eu = env_value<T, EXACT>(S, cc0, sm, 0, cl0 + mirror_adj(S, 0, t), t, lo0);
-                    const T el = env_value<T, EXACT>(S, cc1, sm, 1, cl1 + mirror_adj(S, 1, t), t, lo1);
+                for (int i = 0; i < RUN; ++i) {
+                    const int t = t0 + j0 + i;
+                    if (i < nv) {
+                        const T eu = env_at<T, EXACT>(C, S, v0, R0, 0, cl0, t);
+                        const T el = env_at<T, EXACT>(C, S, v1, R1, 1, cl1, t);
+                        finish(i, (T)0.5 * (eu + el));
+                    }
                     cl0 += (kmx >> i) & 1u;
                     cl1 += (kmn >> i) & 1u;
-                    const T m = (T)0.5 * (eu + el);
-                    const T hn = h - m;
-                    fv[i] = hn;
-                    if (EXACT) {
-                        const double dd = (C.rules == EEMD_RULES_NUMBA) ? (double)m : (double)(h - hn);
-                        num = num + dd * dd;
-                        den = den + (double)h * (double)h;
-                    } else {
-                        const T dd = (C.rules == EEMD_RULES_NUMBA) ? m : h - hn;
-                        tnum = fmat(dd, dd, tnum);
-                        tden = fmat(h, h, tden);
-                    }
-                    gv[i] = (mode == TM_LAST) ? rv[i] - hn : hn;
-                } else if (mode == TM_TRANS) {
-                    fv[i] = rv[i] - (S.imf_from_resid ? rv[i] : hv[i]);
-                    gv[i] = fv[i];
-                } else {  // TM_INIT
-                    fv[i] = (T)trial_input<T>(C, d, t);
-                    gv[i] = fv[i];
                 }
             }
-        }
-        if (!EXACT) {
-            num += (double)tnum;
-            den += (double)tden;
-        }
-        // halo samples: t0-1 (first tile of the segment, thread 0) and t0+tl (last owner)
-        const int u_last = (tl - 1) / run;
-        for (int side = 0; side < 2; ++side) {
-            int t, hj;
-            if (side == 0) {
-                if (!(tid == 0 && first && t0 > 0)) continue;
-                t = t0 - 1;
-                hj = -1;
-            } else {
-                if (!(tid == u_last && t0 + tl < n)) continue;
-                t = t0 + tl;
-                hj = tl;
+            if (!EXACT) {
+                num += (double)tnum;
+                den += (double)tden;
             }
-            T fn, gn;
-            if (sifting) {
-                IvCache<T> h0, h1;
-                h0.k = h1.k = -1;
-                const int c0v = (side == 0 ? kb0 - S.left_knot[0] : kb0 + kc0) + mirror_adj(S, 0, t);
-                const int c1v = (side == 0 ? kb1 - S.left_knot[1] : kb1 + kc1) + mirror_adj(S, 1, t);
-                const T eu = env_value<T, EXACT>(S, h0, sm, 0, c0v, t, lo0);
-                const T el = env_value<T, EXACT>(S, h1, sm, 1, c1v, t, lo1);
-                const T m = (T)0.5 * (eu + el);
-                fn = hb[hj] - m;
-                gn = (mode == TM_LAST) ? rb[hj] - fn : fn;
-            } else if (mode == TM_TRANS) {
-                const T ro = rb[hj];
-                fn = ro - (S.imf_from_resid ? ro : hb[hj]);
-                gn = fn;
-            } else {
-                fn = (T)trial_input<T>(C, d, t);
-                gn = fn;
-            }
-            if (side == 0) {
-                S.fl = fn;
-                S.gl = gn;
-            } else {
-                S.fr = fn;
-                S.gr = gn;
-            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < RUN; ++i)
+                if (i < nv) plain_value<T, MODE>(C, S, d, t0 + j0 + i, hv[i], rv[i], fv[i], gv[i]);
         }
-        SUB(3);
-        // run edges for the neighbours' flags
-        const T glast_mine = (run == 1) ? gv[0] : (run == 2) ? gv[1] : gv[RUN_MAX - 1];
-        if (lane == 0) s_gfirst[wid] = gv[0];
-        if (lane == 31) s_glast[wid] = glast_mine;
-        __syncthreads();
-        SUB(4);
+        SUB(1);
 
-        // ---------------- (e) next knots: strict extrema of the new values ----------------
-        const T up = __shfl_up_sync(0xffffffffu, glast_mine, 1);
-        const T dn = __shfl_down_sync(0xffffffffu, gv[0], 1);
-        T gprev, gnext;
-        if (j0 == 0) gprev = first ? (t0 > 0 ? (T)S.gl : (T)0) : (T)S.g_m1;
-        else gprev = (lane > 0) ? up : s_glast[wid - 1];
-        if (j0 + nv == tl) gnext = (t0 + tl < n) ? (T)S.gr : (T)0;
-        else gnext = (lane < 31) ? dn : s_gfirst[wid + 1];
+        // ---------------- strict extrema of the new values ----------------
+        // lanes decide their own samples except the tile's last one (its right
+        // neighbour is the next tile's first sample); lane 0 decides the
+        // previous tile's last sample
+        const T up = __shfl_up_sync(FULL, gv[RUN - 1], 1);
+        const T dn = __shfl_down_sync(FULL, gv[0], 1);
+        const T gprev = (lane == 0) ? gm1 : up;
         unsigned nmx = 0u, nmn = 0u;
 #pragma unroll
-        for (int i = 0; i < RUN_MAX; ++i) {
-            const int t = t0 + j0 + i;
-            if (i < nv && t >= 1 && t <= n - 2) {
-                const T a = (i == 0) ? gprev : gv[(i + RUN_MAX - 1) % RUN_MAX];
-                const T c = (i + 1 == nv) ? gnext : gv[(i + 1) % RUN_MAX];
+        for (int i = 0; i < RUN; ++i) {
+            const int pos = j0 + i, t = t0 + pos;
+            if (i < nv && pos != tl - 1 && t >= 1 && t <= n - 2) {
+                const T a = (i == 0) ? gprev : gv[(i + RUN - 1) % RUN];
+                const T c = (i + 1 < RUN) ? gv[(i + 1) % RUN] : dn;
                 const T v = gv[i];
                 if (v > a && v > c) nmx |= 1u << i;
                 if (v < a && v < c) nmn |= 1u << i;
             }
         }
-        int ex2, en2, tx2, tn2;
-        block_scan2(__popc(nmx), __popc(nmn), ex2, en2, tx2, tn2, s_w2);
-        SUB(5);
+        unsigned dmx = 0u, dmn = 0u;  // the previous tile's last sample (lane 0)
+        if (lane == 0 && j > ta && t0 - 1 >= 1 && t0 - 1 <= n - 2) {
+            dmx = (gm1 > gm2 && gm1 > gv[0]) ? 1u : 0u;
+            dmn = (gm1 < gm2 && gm1 < gv[0]) ? 1u : 0u;
+        }
+        const int cnt = (int)(__popc(nmx) + dmx) | ((int)(__popc(nmn) + dmn) << 16);
+        int inc = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int x = __shfl_up_sync(FULL, inc, o);
+            if (lane >= o) inc += x;
+        }
+        const int tot = __shfl_sync(FULL, inc, 31);
+        const int exc = inc - cnt;
+        SUB(2);
 
-        // ---------------- (f) writes ----------------
-        {
-            const int64_t pmx = knot_index(C, np, 0, rank, 0);
-            const int64_t pmn = knot_index(C, np, 1, rank, 0);
-            int px = S.run_new[0] + ex2, pn = S.run_new[1] + en2;
-#pragma unroll
-            for (int i = 0; i < RUN_MAX; ++i) {
-                const int t = t0 + j0 + i;
-                if (i < nv) {
-                    if ((nmx >> i) & 1u) {
-                        if (px < C.segcap) {
-                            sl.kt[pmx + px] = t;
-                            static_cast<T*>(sl.ky)[pmx + px] = gv[i];
-                        } else {
-                            raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
-                        }
-                        ++px;
-                    }
-                    if ((nmn >> i) & 1u) {
-                        if (pn < C.segcap) {
-                            sl.kt[pmn + pn] = t;
-                            static_cast<T*>(sl.ky)[pmn + pn] = gv[i];
-                        } else {
-                            raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
-                        }
-                        ++pn;
-                    }
+        // ---------------- writes ----------------
+        int px = wcx + (exc & 0xffff), pn = wcy + (exc >> 16);
+        if (lane == 0 && j > ta) {
+            // the previous tile's last sample and the run record that waited for it
+            if (dmx) {
+                if (px < C.segcap) {
+                    sl.kt[pmx + px] = t0 - 1;
+                    static_cast<T*>(sl.ky)[pmx + px] = gm1;
+                } else {
+                    raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
                 }
             }
-            const int tj = t0 + j0;
-            switch (mode) {
-                case TM_SIFT: store_run<T>(imf_m + tj, fv, nv); break;
-                case TM_LAST:
-                    store_run<T>(imf_m + tj, fv, nv);
-                    store_run<T>(resid + tj, gv, nv);
-                    break;
-                case TM_TRANS:
-                    store_run<T>(resid + tj, fv, nv);
-                    if (S.imf_from_resid) store_run<T>(imf_m + tj, rv, nv);
-                    break;
-                default: store_run<T>(resid + tj, fv, nv); break;
-            }
-            // edge and carry values of the tile, written by the threads that hold them
-#pragma unroll
-            for (int i = 0; i < RUN_MAX; ++i) {
-                if (i >= nv) continue;
-                const int j = j0 + i;
-                if (first && j == 0) { S.hf0 = fv[i]; S.rf0 = gv[i]; }
-                if (first && j == 1) { S.hf1 = fv[i]; S.rf1 = gv[i]; }
-                if (j == tl - 2) { S.f_last2 = fv[i]; S.g_last2 = gv[i]; }
-                if (j == tl - 1) {
-                    if (last) {
-                        Xchg& xo = X[q];
-                        xo.hl[0] = (tl >= 2) ? 0.0 : S.f_m1;  // completed below for tl >= 2
-                        xo.hl[1] = fv[i];
-                        xo.rl[0] = (tl >= 2) ? 0.0 : S.g_m1;
-                        xo.rl[1] = gv[i];
-                    }
-                    S.f_m1 = fv[i];
-                    S.g_m1 = gv[i];
-                    if (sifting) {
-                        S.hold_m1 = hv[i];
-                        S.hold_m2 = (tl >= 2) ? (double)hb[tl - 2] : (double)hb[-1];
-                    }
+            if (dmn) {
+                if (pn < C.segcap) {
+                    sl.kt[pmn + pn] = t0 - 1;
+                    static_cast<T*>(sl.ky)[pmn + pn] = gm1;
+                } else {
+                    raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
                 }
             }
+            ri_nxt[crun] = make_int4(cpx, cpn, cmask | (int)(dmx << cbit) | (int)(dmn << (16 + cbit)), 0);
+            px += (int)dmx;
+            pn += (int)dmn;
         }
-        __syncthreads();
-        if (tid == 0) {
-            if (last && tl >= 2) {
-                X[q].hl[0] = S.f_last2;
-                X[q].rl[0] = S.g_last2;
+        const int rpx = px, rpn = pn, rmask = (int)(nmx | (nmn << 16));
+        if (nv > 0 && lane != last_lane) ri_nxt[t0 / RUN + lane] = make_int4(rpx, rpn, rmask, 0);
+#pragma unroll
+        for (int i = 0; i < RUN; ++i) {
+            const int t = t0 + j0 + i;
+            if ((nmx >> i) & 1u) {
+                if (px < C.segcap) {
+                    sl.kt[pmx + px] = t;
+                    static_cast<T*>(sl.ky)[pmx + px] = gv[i];
+                } else {
+                    raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
+                }
+                ++px;
             }
-            S.run_cur[0] += kc0;
-            S.run_cur[1] += kc1;
-            S.run_new[0] += tx2;
-            S.run_new[1] += tn2;
+            if ((nmn >> i) & 1u) {
+                if (pn < C.segcap) {
+                    sl.kt[pmn + pn] = t;
+                    static_cast<T*>(sl.ky)[pmn + pn] = gv[i];
+                } else {
+                    raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
+                }
+                ++pn;
+            }
         }
-        __syncthreads();
-        SUB(6);
+        const int tj = t0 + j0;
+        if (MODE == TM_SIFT) {
+            store_run<T, RUN>(io.hdst + tj, fv, nv);
+        } else if (MODE == TM_LAST) {
+            store_run<T, RUN>(io.imf_m + tj, fv, nv);
+            store_run<T, RUN>(io.rnxt + tj, gv, nv);
+        } else if (MODE == TM_TRANS) {
+            store_run<T, RUN>(io.rnxt + tj, fv, nv);
+            if (io.trans_imf) {
+                if (S.imf_from_resid) store_run<T, RUN>(io.imf_m + tj, rv, nv);
+                else store_run<T, RUN>(io.imf_m + tj, hv, nv);
+            }
+        } else {
+            store_run<T, RUN>(io.rnxt + tj, fv, nv);
+        }
+        // carry to the next tile: the last sample's neighbours and its run record
+        cpx = __shfl_sync(FULL, rpx, last_lane);
+        cpn = __shfl_sync(FULL, rpn, last_lane);
+        cmask = __shfl_sync(FULL, rmask, last_lane);
+        crun = t0 / RUN + last_lane;
+        cbit = tl - 1 - last_lane * RUN;
+        gm2 = (tl >= 2) ? tile_at<T, RUN>(gv, tl - 2) : gm1;
+        gm1 = tile_at<T, RUN>(gv, tl - 1);
+        wcx += tot & 0xffff;
+        wcy += tot >> 16;
+        SUB(3);
+    }
+    if (ta < tb) {
+        // the range's last sample r1-1: its right neighbour lies outside the range
+        unsigned dmx = 0u, dmn = 0u;
+        if (lane == 0 && r1 < n && r1 - 1 >= 1) {
+            const T gr = outside_g<T, EXACT, MODE>(C, S, d, io, R0, R1, r1, S.pref[S.kpar][0][seg + 1],
+                                                  S.pref[S.kpar][1][seg + 1]);
+            dmx = (gm1 > gm2 && gm1 > gr) ? 1u : 0u;
+            dmn = (gm1 < gm2 && gm1 < gr) ? 1u : 0u;
+        }
+        if (lane == 0) {
+            if (dmx) {
+                if (wcx < C.segcap) {
+                    sl.kt[pmx + wcx] = r1 - 1;
+                    static_cast<T*>(sl.ky)[pmx + wcx] = gm1;
+                } else {
+                    raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
+                }
+            }
+            if (dmn) {
+                if (wcy < C.segcap) {
+                    sl.kt[pmn + wcy] = r1 - 1;
+                    static_cast<T*>(sl.ky)[pmn + wcy] = gm1;
+                } else {
+                    raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
+                }
+            }
+            ri_nxt[crun] = make_int4(cpx, cpn, cmask | (int)(dmx << cbit) | (int)(dmn << (16 + cbit)), 0);
+        }
+        wcx += (int)__shfl_sync(FULL, dmx, 0);
+        wcy += (int)__shfl_sync(FULL, dmn, 0);
+    }
+    if (lane == 0) {
+        X[q].cnt[0][wid] = wcx;
+        X[q].cnt[1][wid] = wcy;
     }
 #ifdef EEMD_TRACE
-    if (tid == 0) {
-        for (int k = 0; k < 7; ++k) atomicAdd(&C.hdr->sweep_cycles[k], scyc[k]);
+    if (lane == 0) {
+        for (int k = 0; k < 4; ++k) atomicAdd(&C.hdr->sweep_cycles[k], scyc[k]);
     }
 #endif
 #undef SUB
-    // ---------------- publish the segment's results ----------------
+    // ---------------- publish the segment's SD partials ----------------
     const double2 rs = block_sum2<THREADS>(make_double2(num, den), s_red);
     if (tid == 0) {
-        Xchg& xo = X[q];
-        xo.hf[0] = S.hf0;
-        xo.hf[1] = S.hf1;
-        if (mode == TM_SIFT) {
-            // the residual is unchanged by a plain sift: carry the previous edges
-            const Xchg& xp = X[q ^ 1];
-            xo.rf[0] = xp.rf[0];
-            xo.rf[1] = xp.rf[1];
-            xo.rl[0] = xp.rl[0];
-            xo.rl[1] = xp.rl[1];
-        } else {
-            xo.rf[0] = S.rf0;
-            xo.rf[1] = S.rf1;
-        }
-        xo.num = rs.x;
-        xo.den = rs.y;
-        xo.cnt[0] = S.run_new[0];
-        xo.cnt[1] = S.run_new[1];
+        X[q].num = rs.x;
+        X[q].den = rs.y;
     }
 }
 
@@ -1186,23 +1220,14 @@ __device__ __forceinline__ void close_imf(const Ctx& C, TaskSm& S) {
     S.mode_sifts_cur = 0;
 }
 
-// adopt the knots the last sweep produced (segment counts nc[env][r])
-__device__ __forceinline__ void adopt(TaskSm& S, const int nc[2][MAXC], int cmax, int cmin) {
+// adopt the knots the last sweep produced (their segment prefixes are in pref[kpar ^ 1])
+__device__ __forceinline__ void adopt(TaskSm& S, int cmax, int cmin) {
     S.kpar ^= 1;
     S.P[0] = cmax;
     S.P[1] = cmin;
-    for (int env = 0; env < 2; ++env) {
-        int acc = 0;
-        for (int r = 0; r < S.csize; ++r) {
-            S.pref[env][r] = acc;
-            acc += nc[env][r];
-        }
-        S.pref[env][S.csize] = acc;
-    }
 }
 
-__device__ __forceinline__ void imf_level(const Ctx& C, TaskSm& S, const int nc[2][MAXC], int cmax,
-                                          int cmin) {
+__device__ __forceinline__ void imf_level(const Ctx& C, TaskSm& S, int cmax, int cmin) {
     bool stop = (cmax + cmin < C.min_extrema);
     if (C.rules == EEMD_RULES_NUMBA) stop = stop || cmax < 2 || cmin < 2;
     if (stop) { S.phase = PH_DONE; return; }
@@ -1218,59 +1243,91 @@ __device__ __forceinline__ void imf_level(const Ctx& C, TaskSm& S, const int nc[
     S.sift = 0;
     S.src_resid = 1;
     S.imf_from_resid = 0;
-    adopt(S, nc, cmax, cmin);
+    adopt(S, cmax, cmin);
 }
 
+// Warp 0 gathers the knot counts of every (CTA, warp) segment through
+// distributed shared memory and writes their prefixes for the new lists;
+// thread 0 then takes the step decision, identical in every CTA.
 __device__ void decide(const Ctx& C, TaskSm& S, Xchg* X, cg::cluster_group& cl) {
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
         const int q = S.step & 1;
-        double num = 0.0, den = 0.0;
-        int nc[2][MAXC];
-        int cmax = 0, cmin = 0;
-        for (int r = 0; r < S.csize; ++r) {
-            const Xchg* xr = cl.map_shared_rank(&X[q], r);
-            num += xr->num;
-            den += xr->den;
-            nc[0][r] = xr->cnt[0];
-            nc[1][r] = xr->cnt[1];
-            cmax += nc[0][r];
-            cmin += nc[1][r];
-        }
-        const int mode = S.mode;
-        if (mode == TM_SIFT) {
-            log_sift(C, S);
-            S.mode_sifts_cur += 1;
-            S.nsift_total += 1;
-            const double sdv = den > 0.0 ? num / den : 0.0;
-            bool stop = (S.sift >= 1) && (sdv < C.tau);
-            if (!stop) stop = (C.rules == EEMD_RULES_NUMBA) ? (cmax < 2 || cmin < 2) : (cmax < 1 || cmin < 1);
-            if (stop) {
-                S.phase = PH_TRANS;
-                S.imf_from_resid = 0;
-            } else {
-                S.sift += 1;
-                S.src_resid = 0;
-                adopt(S, nc, cmax, cmin);
+        const int nseg = S.csize * NWARP;
+        int c[2][2] = {{0, 0}, {0, 0}};  // [env][segment 2*lane + k]
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int sg = 2 * lane + k;
+            if (sg < nseg) {
+                const Xchg* xr = cl.map_shared_rank(&X[q], sg / NWARP);
+                c[0][k] = xr->cnt[0][sg % NWARP];
+                c[1][k] = xr->cnt[1][sg % NWARP];
             }
-        } else if (mode == TM_LAST) {
-            log_sift(C, S);
-            S.mode_sifts_cur += 1;
-            S.nsift_total += 1;
-            close_imf(C, S);
-            imf_level(C, S, nc, cmax, cmin);
-        } else if (mode == TM_TRANS) {
-            close_imf(C, S);
-            imf_level(C, S, nc, cmax, cmin);
-        } else {
-            S.imf = 0;
-            S.nmode = 0;
-            imf_level(C, S, nc, cmax, cmin);
         }
-        S.step += 1;
-        // every IMF ends after at most max_sifts sifts plus one closing step
-        if (S.phase != PH_DONE && S.step > 2 + C.max_imf * (C.max_sifts + 1)) {
-            raise_error(C.hdr, EEMD_E_TIMEOUT, S.task);
-            S.phase = PH_DONE;
+        int tot[2];
+#pragma unroll
+        for (int env = 0; env < 2; ++env) {
+            const int v = c[env][0] + c[env][1];
+            int inc = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int x = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += x;
+            }
+            tot[env] = __shfl_sync(0xffffffffu, inc, 31);
+            int* pr = S.pref[S.kpar ^ 1][env];
+            const int e = inc - v;
+            if (2 * lane < nseg) pr[2 * lane] = e;
+            if (2 * lane + 1 < nseg) pr[2 * lane + 1] = e + c[env][0];
+            if (lane == 0) pr[nseg] = tot[env];
+        }
+        if (lane == 0) {
+            double num = 0.0, den = 0.0;
+            for (int r = 0; r < S.csize; ++r) {
+                const Xchg* xr = cl.map_shared_rank(&X[q], r);
+                num += xr->num;
+                den += xr->den;
+            }
+            const int cmax = tot[0], cmin = tot[1];
+            const int mode = S.mode;
+            if (mode == TM_SIFT) {
+                log_sift(C, S);
+                S.mode_sifts_cur += 1;
+                S.nsift_total += 1;
+                const double sdv = den > 0.0 ? num / den : 0.0;
+                bool stop = (S.sift >= 1) && (sdv < C.tau);
+                if (!stop) stop = (C.rules == EEMD_RULES_NUMBA) ? (cmax < 2 || cmin < 2) : (cmax < 1 || cmin < 1);
+                if (stop) {
+                    S.phase = PH_TRANS;
+                    S.imf_from_resid = 0;
+                } else {
+                    S.sift += 1;
+                    S.src_resid = 0;
+                    adopt(S, cmax, cmin);
+                }
+            } else if (mode == TM_LAST) {
+                log_sift(C, S);
+                S.mode_sifts_cur += 1;
+                S.nsift_total += 1;
+                S.rcur ^= 1;
+                close_imf(C, S);
+                imf_level(C, S, cmax, cmin);
+            } else if (mode == TM_TRANS) {
+                S.rcur ^= 1;
+                close_imf(C, S);
+                imf_level(C, S, cmax, cmin);
+            } else {
+                S.rcur ^= 1;
+                S.imf = 0;
+                S.nmode = 0;
+                imf_level(C, S, cmax, cmin);
+            }
+            S.step += 1;
+            // every IMF ends after at most max_sifts sifts plus one closing step
+            if (S.phase != PH_DONE && S.step > 2 + C.max_imf * (C.max_sifts + 1)) {
+                raise_error(C.hdr, EEMD_E_TIMEOUT, S.task);
+                S.phase = PH_DONE;
+            }
         }
     }
     __syncthreads();
@@ -1327,11 +1384,14 @@ __global__ void __launch_bounds__(THREADS, EEMD_MIN_CTAS_PER_SM) k_emd(const __g
     const int csize = (int)cl.num_blocks();
     const int slot = blockIdx.x / csize;
     const int tid = threadIdx.x;
-    const Smem sm = carve<T>(smem_raw, C.tile);
+    const Smem sm = carve(smem_raw);
     Slot sl;
     sl.kt = C.kt + (int64_t)slot * C.slot_knots;
     sl.ky = static_cast<T*>(C.ky) + (int64_t)slot * C.slot_knots;
     sl.M = static_cast<T*>(C.M) + (int64_t)slot * C.slot_M;
+    sl.w1 = static_cast<T*>(C.w1) + (int64_t)slot * C.slot_n;
+    sl.r1 = static_cast<T*>(C.r1) + (int64_t)slot * C.slot_n;
+    sl.ri = C.ri + (int64_t)slot * 2 * C.slot_runs;
 
 #ifdef EEMD_TRACE
     unsigned long long cyc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -1367,9 +1427,10 @@ __global__ void __launch_bounds__(THREADS, EEMD_MIN_CTAS_PER_SM) k_emd(const __g
             S.imf = S.sift = S.kpar = S.src_resid = S.imf_from_resid = 0;
             S.nsift_total = S.nmode = S.mode_sifts_cur = S.flags = S.step = 0;
             S.P[0] = S.P[1] = 0;
-            for (int r = 0; r <= MAXC; ++r) S.pref[0][r] = S.pref[1][r] = 0;
+            for (int r = 0; r <= MAXSEG; ++r)
+                S.pref[0][0][r] = S.pref[0][1][r] = S.pref[1][0][r] = S.pref[1][1][r] = 0;
             S.mir[0] = S.mir[1] = 0;
-            S.f_m1 = S.g_m1 = 0.0;
+            S.rcur = 1;  // the first step writes the residual array
             if (C.watchdog < 0 && rank == 0) {
                 // watchdog test mode: a bounded wait on a flag nothing sets
                 long long spins = 0;
@@ -1398,12 +1459,24 @@ __global__ void __launch_bounds__(THREADS, EEMD_MIN_CTAS_PER_SM) k_emd(const __g
                 cl.sync();  // second derivatives of every segment visible
                 EEMD_PHASE(2);
             }
-            sweep<T, EXACT>(C, sl, S, X, sm, cl);
+            switch (S.mode) {
+                case TM_SIFT: sweep<T, EXACT, TM_SIFT>(C, sl, S, X, smem_raw); break;
+                case TM_LAST: sweep<T, EXACT, TM_LAST>(C, sl, S, X, smem_raw); break;
+                case TM_TRANS: sweep<T, EXACT, TM_TRANS>(C, sl, S, X, smem_raw); break;
+                default: sweep<T, EXACT, TM_INIT>(C, sl, S, X, smem_raw); break;
+            }
             EEMD_PHASE(3);
             cl.sync();  // segment results published
             EEMD_PHASE(4);
             decide(C, S, X, cl);
             EEMD_PHASE(5);
+        }
+        if (S.rcur) {
+            // the final residual sits in the slot scratch: move this segment to the task's array
+            const TaskDesc d = C.td[S.task];
+            T* r0 = static_cast<T*>(C.resid) + d.s_off;
+            const T* r1 = static_cast<const T*>(sl.r1);
+            for (int t = S.s0 + tid; t < S.s1; t += THREADS) r0[t] = r1[t];
         }
         if (rank == 0 && tid == 0) {
             TaskOut o;
@@ -1511,18 +1584,17 @@ struct Layout {
     std::vector<TaskDesc> td;
     std::vector<SignalDesc> sd;
     std::vector<int32_t> order;
-    int64_t NS = 0, NIMF = 0, slot_knots = 0, slot_M = 0;
-    int tile = 0, B = 0, S = 0, csize = 1, slots = 1, segcap = 0, kcap = 0, scr_rows = 0;
-    size_t o_hdr, o_td, o_order, o_tout, o_sd, o_sigma, o_resid, o_imfs, o_kt, o_ky, o_M, o_scr;
+    int64_t NS = 0, NIMF = 0, slot_knots = 0, slot_M = 0, slot_n = 0, slot_runs = 0;
+    int B = 0, S = 0, csize = 1, slots = 1, segcap = 0, kcap = 0, scr_rows = 0;
+    size_t o_hdr, o_td, o_order, o_tout, o_sd, o_sigma, o_resid, o_imfs, o_kt, o_ky, o_M, o_w1, o_r1, o_ri,
+        o_scr;
     size_t total = 0;
 };
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-// Launch shapes by length bucket.  The cluster spreads one task over several
-// SMs when there are fewer tasks than CTA slots; tiles live inside a segment.
-int autotune_tile(int64_t seg) { return seg <= 4096 ? 512 : 1024; }
-
+// The cluster spreads one task over several SMs when there are fewer tasks
+// than CTA slots.
 int autotune_csize(int64_t n_tasks, int64_t nmin) {
     const int64_t budget = (int64_t)ASSUMED_SMS * ASSUMED_CTAS_PER_SM;
     int c = (int)std::max<int64_t>(1, std::min<int64_t>(8, budget / std::max<int64_t>(n_tasks, 1)));
@@ -1538,7 +1610,9 @@ int check_params(const eemd_params* p) {
     if (p->end_mode != EEMD_END_NATURAL && p->end_mode != EEMD_END_MIRROR) return EEMD_E_BADARG;
     if (p->rules != EEMD_RULES_REF && p->rules != EEMD_RULES_NUMBA) return EEMD_E_BADARG;
     if (p->noise_mode < EEMD_NOISE_NONE || p->noise_mode > EEMD_NOISE_PREPERTURBED) return EEMD_E_BADARG;
-    if (p->tile != 0 && p->tile != 256 && p->tile != 512 && p->tile != 1024) return EEMD_E_BADARG;
+    // warp tile: 32 lanes x 8 float32 samples or x 4 float64 samples
+    const int wt = (p->dtype == EEMD_F64) ? Geo<double>::WT : Geo<float>::WT;
+    if (p->tile != 0 && p->tile != wt) return EEMD_E_BADARG;
     if (p->knots_per_block < 0 || p->knots_per_block > 4096 || p->halo < 0 || p->halo > 256)
         return EEMD_E_BADARG;
     if (p->cluster_size < 0 || p->cluster_size > 8) return EEMD_E_BADARG;
@@ -1599,13 +1673,19 @@ int make_layout(const eemd_params* p, const int64_t* lengths, int n_signals, int
     L.order.resize(n_tasks);
     std::iota(L.order.begin(), L.order.end(), 0);
     std::stable_sort(L.order.begin(), L.order.end(), [&](int a, int b) { return L.td[a].n > L.td[b].n; });
-    L.tile = p->tile ? p->tile : autotune_tile(segmax);
-    L.segcap = (int)(segmax / 2 + 2);
+    const int run = (p->dtype == EEMD_F64) ? Geo<double>::RUN : Geo<float>::RUN;
+    const int wt = 32 * run;
+    // knots of one kind in one warp's range: at most half its samples (+ends)
+    const int64_t tiles_per_warp = ((segmax + wt - 1) / wt + NWARP - 1) / NWARP;
+    L.segcap = (int)(tiles_per_warp * wt / 2 + 2);
     L.kcap = (int)(nmax / 2 + 4);
+    const int rs = (p->dtype == EEMD_F64) ? Geo<double>::RS : Geo<float>::RS;
+    L.slot_n = (nmax + 3) / 4 * 4;
+    L.slot_runs = (nmax + run - 1) / run + 1;
     L.slots = (int)std::max<int64_t>(
         1, std::min<int64_t>(n_tasks, (int64_t)ASSUMED_SMS * ASSUMED_CTAS_PER_SM / L.csize));
-    L.slot_knots = (int64_t)2 * 2 * L.csize * L.segcap;
-    L.slot_M = (int64_t)2 * 5 * L.kcap;
+    L.slot_knots = (int64_t)2 * 2 * L.csize * NWARP * L.segcap;
+    L.slot_M = (int64_t)2 * L.kcap * rs;
     L.scr_rows = p->exact ? (L.B + L.S) : 0;
     L.NS = so;
     L.NIMF = imo;
@@ -1627,6 +1707,9 @@ int make_layout(const eemd_params* p, const int64_t* lengths, int n_signals, int
     L.o_kt = take(sizeof(int32_t) * L.slot_knots * L.slots);
     L.o_ky = take(bt * L.slot_knots * L.slots);
     L.o_M = take(bt * L.slot_M * L.slots);
+    L.o_w1 = take(bt * L.slot_n * L.slots);
+    L.o_r1 = take(bt * L.slot_n * L.slots);
+    L.o_ri = take(16 * 2 * L.slot_runs * L.slots);
     L.o_scr = take(sizeof(double2) * (size_t)L.scr_rows * L.slots * L.csize * THREADS);
     L.total = off;
     return EEMD_OK;
@@ -1673,7 +1756,7 @@ struct Tracer {
 
 template <typename T, bool EXACT>
 int launch_emd(const Ctx& C, const Layout& L, cudaStream_t st, Tracer& tr) {
-    const size_t smem = smem_bytes(L.tile, (int)sizeof(T));
+    const size_t smem = smem_bytes((int)sizeof(T));
     if (cudaFuncSetAttribute(k_emd<T, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return EEMD_E_CUDA;
@@ -1706,7 +1789,12 @@ int run_typed(const eemd_params* p, const Layout& L, Ctx& C, double* imf_sum, in
         k_sigma<T><<<(int)L.sd.size(), 1024, 0, st>>>(C.sd, C.x, p->eps, const_cast<double*>(C.sigma));
         tr.end();
     }
-    int rc = p->exact ? launch_emd<T, true>(C, L, st, tr) : launch_emd<T, false>(C, L, st, tr);
+    int rc;
+    if constexpr (sizeof(T) == 8) {
+        rc = p->exact ? launch_emd<T, true>(C, L, st, tr) : launch_emd<T, false>(C, L, st, tr);
+    } else {
+        rc = launch_emd<T, false>(C, L, st, tr);  // exact mode is float64 only
+    }
     if (rc) return rc;
     if (imf_sum || mode_count) {
         int64_t nmax = 0;
@@ -1812,6 +1900,9 @@ int32_t eemd_run_traced(const eemd_params* p, const void* x, const int64_t* leng
     C.kt = reinterpret_cast<int32_t*>(base + L.o_kt);
     C.ky = base + L.o_ky;
     C.M = base + L.o_M;
+    C.w1 = base + L.o_w1;
+    C.r1 = base + L.o_r1;
+    C.ri = reinterpret_cast<int4*>(base + L.o_ri);
     C.scr = reinterpret_cast<double2*>(base + L.o_scr);
     C.x = x;
     C.noise = noise;
@@ -1819,6 +1910,8 @@ int32_t eemd_run_traced(const eemd_params* p, const void* x, const int64_t* leng
     C.mode_sifts = mode_sifts;
     C.slot_knots = L.slot_knots;
     C.slot_M = L.slot_M;
+    C.slot_n = L.slot_n;
+    C.slot_runs = L.slot_runs;
     C.segcap = L.segcap;
     C.kcap = L.kcap;
     C.n_tasks = (int32_t)L.td.size();
@@ -1831,7 +1924,6 @@ int32_t eemd_run_traced(const eemd_params* p, const void* x, const int64_t* leng
     C.end_mode = p->end_mode;
     C.rules = p->rules;
     C.noise_mode = p->noise_mode;
-    C.tile = L.tile;
     C.B = L.B;
     C.S = L.S;
     C.scr_rows = L.scr_rows;

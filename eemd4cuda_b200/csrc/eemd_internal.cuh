@@ -32,7 +32,7 @@
 namespace eemd {
 
 constexpr int THREADS = 256;      // threads per CTA of k_emd
-constexpr int MAXC = 16;          // largest cluster (non-portable size)
+constexpr int MAXC = 8;           // largest cluster
 constexpr int FAST_B = 8;         // owned rows per window, fast solve (register resident)
 constexpr int SOLVE_CAP = 2176;   // knots staged in shared memory per solve pass
 
@@ -49,8 +49,8 @@ struct Header {
     // -DEEMD_TRACE builds: SM cycles spent per phase, summed over CTAs
     // (0 setup, 1 solve, 2 barrier after solve, 3 sweep, 4 barrier after sweep, 5 decide, 6 claim)
     unsigned long long phase_cycles[8];
-    // sweep sub-phases (thread 0 of each CTA): 0 tile wait+halo, 1 masks+scan,
-    // 2 staging wait, 3 values, 4 edges barrier, 5 flags+scan, 6 writes+barriers
+    // sweep sub-phases (lane 0 of each warp): 0 tile wait, 1 values, 2 extrema +
+    // warp scan, 3 writes
     unsigned long long sweep_cycles[8];
 };
 
@@ -92,6 +92,9 @@ struct Ctx {
     void* M;                      // per slot: [2 env][5][kcap] interval records (mirror space,
                                   //   storage type): plane 0 = t_k; fast: monomial c0..c3 of
                                   //   interval [k, k+1]; exact: y_k, M_k
+    void* w1;                     // per slot: scratch h buffer [slot_n] (storage type)
+    void* r1;                     // per slot: second residual buffer [slot_n] (storage type)
+    int4* ri;                     // per slot: run records [2 parity][slot_runs]
     double2* scr;                 // exact-mode solve scratch: [rows][grid threads]
     const void* x;
     const void* noise;
@@ -99,11 +102,13 @@ struct Ctx {
     int32_t* mode_sifts;          // optional [task][max_imf]
     int64_t slot_knots;           // kt/ky elements per slot
     int64_t slot_M;               // record elements per slot
+    int64_t slot_n;               // w1 / r1 elements per slot
+    int64_t slot_runs;            // run records per slot and parity
     int32_t segcap;               // knots of one kind per segment list
     int32_t kcap;                 // knots per envelope in mirror space (M plane size)
     int32_t n_tasks, n_signals, trial_count, csize;
     int32_t max_sifts, max_imf, min_extrema, end_mode, rules, noise_mode;
-    int32_t tile, B, S, scr_rows;
+    int32_t B, S, scr_rows;
     double tau;
     uint64_t seed;
     long long watchdog;

@@ -73,7 +73,12 @@ class EMDResult:
 
 @dataclass
 class EngineConfig:
-    """Engine knobs beyond the reference's signature (0 = autotune)."""
+    """Engine knobs beyond the reference's signature (0 = default / autotune).
+
+    tile: samples per warp tile; only 32 x 8 (float32) or 32 x 4 (float64).
+    knots_per_block, halo: exact-mode solve window and decay halo.
+    watchdog: spin limit of the device waits (negative: test mode).
+    cluster_size: CTAs sharing one signal (1..8)."""
     tile: int = 0
     knots_per_block: int = 0
     halo: int = 0

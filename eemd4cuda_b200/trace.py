@@ -1,16 +1,16 @@
 """Per-phase cycle counters of a -DEEMD_TRACE build (libeemd_b200_trace.so).
 
 The persistent kernel's thread 0 of every CTA sums clock64() deltas per phase
-and adds them to the workspace header at exit; `phase_cycles(ws)` reads them
-back (the header sits at offset 0 of the workspace).
+(lane 0 of every warp for the sweep's sub-phases) and adds them to the
+workspace header at exit; `phase_cycles(ws)` reads them back (the header sits
+at offset 0 of the workspace).
 """
 from __future__ import annotations
 
 import numpy as np
 
 PHASES = ("setup", "solve", "barrier_solve", "sweep", "barrier_sweep", "decide", "claim")
-SWEEP_PHASES = ("tile_wait", "masks_scan", "staging_wait", "values", "edges_barrier", "flags_scan",
-                "writes_barriers")
+SWEEP_PHASES = ("tile_wait", "values", "extrema_scan", "writes")
 _HEADER_INTS = 16  # int32 fields before phase_cycles
 
 

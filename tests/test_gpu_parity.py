@@ -190,13 +190,14 @@ def test_determinism_and_seed(sweep):
     assert np.max(np.abs(a.imfs[:m] - c.imfs[:m])) > 0
 
 
-@pytest.mark.parametrize("tile", [256, 512, 1024])
-def test_tile_size_invariance(sweep, tile):
-    """Launch shape must not change results: the per-sample arithmetic is
-    tile-independent (only the SD sum order moves)."""
+@pytest.mark.parametrize("cluster_size", [1, 2, 4])
+def test_cluster_size_invariance(sweep, cluster_size):
+    """Launch shape must not change results: the knot lists, the solve windows
+    and the per-sample arithmetic do not depend on how many CTAs share a
+    signal (only the SD sum order moves)."""
     x = sweep[:50000]
-    base = raw_run(x[None, :], exact=True, config=M.EngineConfig(tile=512))
-    res = raw_run(x[None, :], exact=True, config=M.EngineConfig(tile=tile))
+    base = raw_run(x[None, :], exact=True, config=M.EngineConfig(cluster_size=2))
+    res = raw_run(x[None, :], exact=True, config=M.EngineConfig(cluster_size=cluster_size))
     assert res["nmode"].tolist() == base["nmode"].tolist()
     assert res["nsift"].tolist() == base["nsift"].tolist()
     for a, b in zip(res["imfs"][0], base["imfs"][0]):
@@ -262,7 +263,7 @@ def test_batched_uneven_signals_equal_single_runs():
     """Many signals of different length in one launch == one launch each."""
     lengths = [4096, 9000, 3000]
     xs = [signals.harmonic_clicks(n, seed=1000 + i) for i, n in enumerate(lengths)]
-    cfg = M.EngineConfig(tile=512)
+    cfg = M.EngineConfig()
     E = 3
     batched = raw_run(None, x=np.concatenate(xs), lengths=lengths, trial_count=E,
                       noise_mode=L.EEMD_NOISE_PHILOX, eps=0.2, seed=5, exact=False, tau=0.0,
@@ -282,7 +283,7 @@ def test_watchdog_reports_timeout_and_context_survives(small):
     run on the same context succeeds."""
     x = np.tile(small["a1_x"], 4)
     with pytest.raises(L.EngineError) as ei:
-        M.decompose(x, E=1, max_sifts=2, max_imf=2, config=M.EngineConfig(tile=256, watchdog=-2000))
+        M.decompose(x, E=1, max_sifts=2, max_imf=2, config=M.EngineConfig(watchdog=-2000))
     assert ei.value.status == L.EEMD_E_TIMEOUT
     r = M.decompose(x, E=1, max_sifts=2, max_imf=2)
     assert r.n_modes == 2
