@@ -233,31 +233,21 @@ struct Geo {
 };
 
 
-// solve staging (a different phase from the sweep; overlays the same memory)
-struct Smem {
-    int* skt;        // solve staging (padded): knot sample index
-    void* sky;       // solve staging (padded): knot value, storage type
-    double* ssl;     // solve staging (padded): slope of the interval starting at the knot
-};
-
 __host__ __device__ inline int stage_pad(int k) { return k + (k >> 4); }
 
 __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 
-__host__ __device__ inline size_t smem_bytes(int bt) {
-    const size_t sweep = NWARP * (bt == 8 ? Geo<double>::WARP_BYTES : Geo<float>::WARP_BYTES);
-    const size_t sp = (size_t)stage_pad(SOLVE_CAP);
-    const size_t solve = align16(sp * 8) + align16(sp * 4) + align16(sp * bt);
-    return sweep > solve ? sweep : solve;
+// per-warp solve staging: slopes (double), knot times (int), knot values (storage type)
+__host__ __device__ inline size_t wsolve_bytes(size_t bt) {
+    const size_t sp = (size_t)stage_pad(WSCAP);
+    return align16(sp * 8) + align16(sp * 4) + align16(sp * bt);
 }
 
-__device__ __forceinline__ Smem carve(unsigned char* base) {
-    Smem m;
-    const size_t sp = (size_t)stage_pad(SOLVE_CAP);
-    m.ssl = reinterpret_cast<double*>(base);
-    m.skt = reinterpret_cast<int*>(base + align16(sp * 8));
-    m.sky = base + align16(sp * 8) + align16(sp * 4);
-    return m;
+// dynamic shared memory of k_emd: the sweep's and the solve's per-warp areas overlay
+__host__ __device__ inline size_t smem_bytes(int bt) {
+    const size_t sweep = NWARP * (bt == 8 ? Geo<double>::WARP_BYTES : Geo<float>::WARP_BYTES);
+    const size_t solve = NWARP * wsolve_bytes((size_t)bt);
+    return sweep > solve ? sweep : solve;
 }
 
 // ---------------------------------------------------------------------------
@@ -550,64 +540,98 @@ __device__ void window_fast(const Ctx& C, const int* skt, const T* sky, const do
 #undef SSL
 
 template <typename T, bool EXACT>
-__device__ void solve_task(const Ctx& C, const Slot& sl, TaskSm& S, const Smem& sm) {
-    const int tid = threadIdx.x;
+__device__ void solve_task(const Ctx& C, const Slot& sl, TaskSm& S, unsigned char* smem) {
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+#ifdef EEMD_TRACE
+    unsigned long long scyc[3] = {0, 0, 0};
+    long long smark = clock64();
+#define SUB(k)                                          \
+    do {                                                \
+        const long long now_ = clock64();               \
+        scyc[k] += (unsigned long long)(now_ - smark);  \
+        smark = now_;                                   \
+    } while (0)
+#else
+#define SUB(k) \
+    do {       \
+    } while (0)
+#endif
+    // one or two knots: a constant or the straight line through them (M = 0)
     for (int env = 0; env < 2; ++env) {
         const int p2 = S.p2[env];
-        const int n = p2 - 2;
+        if (p2 - 2 > 0 || S.rank != 0 || tid >= p2) continue;
         Rec<T> R;
         R.rc = static_cast<T*>(sl.M) + (int64_t)env * C.kcap * Geo<T>::RS;
-        if (n <= 0) {
-            // one or two knots: a constant or the straight line through them (M = 0)
-            if (S.rank == 0 && tid < p2) {
-                int tk, t1;
-                double yk, y1;
-                knot2<T>(C, sl, S, env, tid, tk, yk);
-                R.at(tid, 0) = tbits<T>(tk);
-                R.at(tid, 1) = (T)yk;
-                R.at(tid, 2) = (T)0;
-                R.at(tid, 3) = (T)0;
-                R.at(tid, 4) = (T)0;
-                if (!EXACT && tid + 1 < p2) {
-                    knot2<T>(C, sl, S, env, tid + 1, t1, y1);
-                    R.at(tid, 2) = (T)((y1 - yk) / (double)(t1 - tk));
-                }
-            }
-            continue;
-        }
-        const int Bw = EXACT ? C.B : FAST_B;
-        const int nwin = (n + Bw - 1) / Bw;
-        const int wa = (int)((int64_t)S.rank * nwin / S.csize);
-        const int wb = (int)((int64_t)(S.rank + 1) * nwin / S.csize);
-        int wpp = (SOLVE_CAP - 2 * C.S - 8) / Bw;
-        wpp = max(1, min(wpp, THREADS));
-        for (int wbase = wa; wbase < wb; wbase += wpp) {
-            const int wend = min(wb, wbase + wpp);
-            const int rlo = max(0, wbase * Bw - C.S);
-            const int rhi = min(n - 1, min(n, wend * Bw) - 1 + C.S);
-            const int kcount = rhi + 3 - rlo;  // knots rlo .. rhi+2
-            T* sky = static_cast<T*>(sm.sky);
-            __syncthreads();
-            for (int k = tid; k < kcount; k += THREADS)
-                stage_knot<T>(C, sl, S, env, rlo + k, &sm.skt[stage_pad(k)], &sky[stage_pad(k)]);
-            cp_async_commit();
-            cp_async_wait<0>();
-            __syncthreads();
-            for (int k = tid; k + 1 < kcount; k += THREADS) {
-                const int ta = sm.skt[stage_pad(k)], tb = sm.skt[stage_pad(k + 1)];
-                const double ya = (double)sky[stage_pad(k)], yb = (double)sky[stage_pad(k + 1)];
-                // emd_ref.py:47: (y_{q+1}-y_q)/H_q, the same IEEE division
-                sm.ssl[stage_pad(k)] = (yb - ya) / (double)(tb - ta);
-            }
-            __syncthreads();
-            const int w = wbase + tid;
-            if (w < wend) {
-                if (EXACT) window_exact<T>(C, sm.skt, sky, sm.ssl, rlo, n, w, R, p2);
-                else window_fast<T>(C, sm.skt, sky, sm.ssl, rlo, n, w, R, p2);
-            }
+        int tk, t1;
+        double yk, y1;
+        knot2<T>(C, sl, S, env, tid, tk, yk);
+        R.at(tid, 0) = tbits<T>(tk);
+        R.at(tid, 1) = (T)yk;
+        R.at(tid, 2) = (T)0;
+        R.at(tid, 3) = (T)0;
+        R.at(tid, 4) = (T)0;
+        if (!EXACT && tid + 1 < p2) {
+            knot2<T>(C, sl, S, env, tid + 1, t1, y1);
+            R.at(tid, 2) = (T)((y1 - yk) / (double)(t1 - tk));
         }
     }
+    // The windows of both envelopes form one list (envelope 0 first); CTA r
+    // takes an even share of it and each warp a contiguous part of the CTA's
+    // share, solved 32 windows (one per lane) at a time from the warp's own
+    // knot staging area: no block-wide barriers.
+    const int Bw = EXACT ? C.B : FAST_B;
+    const int n0 = max(0, S.p2[0] - 2), n1 = max(0, S.p2[1] - 2);
+    const int nw0 = (n0 + Bw - 1) / Bw, nw1 = (n1 + Bw - 1) / Bw;
+    const int nwt = nw0 + nw1;
+    const int ca = (int)((int64_t)S.rank * nwt / S.csize), cb = (int)((int64_t)(S.rank + 1) * nwt / S.csize);
+    const int wa = ca + (int)((int64_t)wid * (cb - ca) / NWARP);
+    const int wb = ca + (int)((int64_t)(wid + 1) * (cb - ca) / NWARP);
+    const int per = min(32, (WSCAP - 2 * C.S - 8) / Bw);  // windows per pass
+    unsigned char* ws = smem + (size_t)wid * wsolve_bytes(sizeof(T));
+    double* ssl = reinterpret_cast<double*>(ws);
+    int* skt = reinterpret_cast<int*>(ws + align16(stage_pad(WSCAP) * 8));
+    T* sky = reinterpret_cast<T*>(ws + align16(stage_pad(WSCAP) * 8) + align16(stage_pad(WSCAP) * 4));
+    for (int g = wa; g < wb;) {
+        const int env = (g < nw0) ? 0 : 1;
+        const int w0 = env ? g - nw0 : g;  // first window of the pass (within its envelope)
+        const int wend = min(w0 + per, min(env ? nw1 : nw0, w0 + (wb - g)));  // one past the last
+        const int n = env ? n1 : n0;
+        const int p2 = S.p2[env];
+        const int rlo = max(0, w0 * Bw - C.S);
+        const int rhi = min(n - 1, min(n, wend * Bw) - 1 + C.S);
+        const int kcount = rhi + 3 - rlo;  // knots rlo .. rhi+2
+        for (int k = lane; k < kcount; k += 32)
+            stage_knot<T>(C, sl, S, env, rlo + k, &skt[stage_pad(k)], &sky[stage_pad(k)]);
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncwarp();
+        SUB(0);
+        for (int k = lane; k + 1 < kcount; k += 32) {
+            const int ta = skt[stage_pad(k)], tb = skt[stage_pad(k + 1)];
+            const double ya = (double)sky[stage_pad(k)], yb = (double)sky[stage_pad(k + 1)];
+            // emd_ref.py:47: (y_{q+1}-y_q)/H_q (the same IEEE division in exact mode)
+            ssl[stage_pad(k)] = EXACT ? (yb - ya) / (double)(tb - ta) : (yb - ya) * fast_rcp((double)(tb - ta));
+        }
+        __syncwarp();
+        SUB(1);
+        Rec<T> R;
+        R.rc = static_cast<T*>(sl.M) + (int64_t)env * C.kcap * Geo<T>::RS;
+        const int w = w0 + lane;
+        if (w < wend) {
+            if (EXACT) window_exact<T>(C, skt, sky, ssl, rlo, n, w, R, p2);
+            else window_fast<T>(C, skt, sky, ssl, rlo, n, w, R, p2);
+        }
+        __syncwarp();
+        SUB(2);
+        g += wend - w0;
+    }
     __syncthreads();
+#ifdef EEMD_TRACE
+    if (lane == 0) {
+        for (int k = 0; k < 3; ++k) atomicAdd(&C.hdr->sweep_cycles[4 + k], scyc[k]);
+    }
+#endif
+#undef SUB
 }
 
 // ---------------------------------------------------------------------------
@@ -1370,7 +1394,7 @@ __device__ void step_setup(const Ctx& C, const Slot& sl, TaskSm& S) {
 // k_emd: the persistent cluster kernel
 // ---------------------------------------------------------------------------
 #ifndef EEMD_MIN_CTAS_PER_SM
-#define EEMD_MIN_CTAS_PER_SM 2
+#define EEMD_MIN_CTAS_PER_SM CTAS_PER_SM
 #endif
 
 template <typename T, bool EXACT>
@@ -1384,7 +1408,6 @@ __global__ void __launch_bounds__(THREADS, EEMD_MIN_CTAS_PER_SM) k_emd(const __g
     const int csize = (int)cl.num_blocks();
     const int slot = blockIdx.x / csize;
     const int tid = threadIdx.x;
-    const Smem sm = carve(smem_raw);
     Slot sl;
     sl.kt = C.kt + (int64_t)slot * C.slot_knots;
     sl.ky = static_cast<T*>(C.ky) + (int64_t)slot * C.slot_knots;
@@ -1454,7 +1477,7 @@ __global__ void __launch_bounds__(THREADS, EEMD_MIN_CTAS_PER_SM) k_emd(const __g
             if (S.mode == TM_SIFT || S.mode == TM_LAST) {
                 step_setup<T>(C, sl, S);
                 EEMD_PHASE(0);
-                solve_task<T, EXACT>(C, sl, S, sm);
+                solve_task<T, EXACT>(C, sl, S, smem_raw);
                 EEMD_PHASE(1);
                 cl.sync();  // second derivatives of every segment visible
                 EEMD_PHASE(2);
@@ -1578,7 +1601,7 @@ using namespace eemd;
 namespace {
 
 constexpr int ASSUMED_SMS = 148;        // B200
-constexpr int ASSUMED_CTAS_PER_SM = 2;  // resident k_emd CTAs per SM the grid is sized for
+constexpr int ASSUMED_CTAS_PER_SM = CTAS_PER_SM;  // resident k_emd CTAs per SM the grid is sized for
 
 struct Layout {
     std::vector<TaskDesc> td;
@@ -1596,7 +1619,9 @@ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // The cluster spreads one task over several SMs when there are fewer tasks
 // than CTA slots.
 int autotune_csize(int64_t n_tasks, int64_t nmin) {
-    const int64_t budget = (int64_t)ASSUMED_SMS * ASSUMED_CTAS_PER_SM;
+    // leave a fifth of the CTA slots free: clusters must fit inside a GPC,
+    // and the last clusters to be placed would otherwise wait for a second wave
+    const int64_t budget = (int64_t)ASSUMED_SMS * ASSUMED_CTAS_PER_SM * 4 / 5;
     int c = (int)std::max<int64_t>(1, std::min<int64_t>(8, budget / std::max<int64_t>(n_tasks, 1)));
     while (c > 1 && nmin / c < 2048) --c;
     return c;
@@ -1634,9 +1659,9 @@ int make_layout(const eemd_params* p, const int64_t* lengths, int n_signals, int
     }
     L.csize = p->cluster_size ? p->cluster_size : autotune_csize(n_tasks, nmin);
     L.S = p->halo ? p->halo : (p->exact ? 32 : 24);
-    L.B = p->knots_per_block ? p->knots_per_block : 64;
-    if (p->exact && (2 * L.S + L.B + 8 > SOLVE_CAP)) return EEMD_E_BADARG;
-    if (!p->exact && 2 * L.S + FAST_B + 8 > SOLVE_CAP) return EEMD_E_BADARG;
+    L.B = p->knots_per_block ? p->knots_per_block : 16;
+    // a solve pass stages its windows' knots plus both halos in the warp's area
+    if (2 * L.S + L.B + 8 > WSCAP || 2 * L.S + FAST_B + 8 > WSCAP) return EEMD_E_BADARG;
     int64_t segmax = 0;
     L.td.resize(n_tasks);
     L.sd.resize(n_signals);

@@ -31,10 +31,14 @@
 
 namespace eemd {
 
-constexpr int THREADS = 256;      // threads per CTA of k_emd
+#ifndef EEMD_CTA_WARPS
+#define EEMD_CTA_WARPS 4
+#endif
+constexpr int THREADS = 32 * EEMD_CTA_WARPS;  // threads per CTA of k_emd
+constexpr int CTAS_PER_SM = 16 / EEMD_CTA_WARPS;  // 16 warps of 128 registers fill an SM
 constexpr int MAXC = 8;           // largest cluster
 constexpr int FAST_B = 8;         // owned rows per window, fast solve (register resident)
-constexpr int SOLVE_CAP = 2176;   // knots staged in shared memory per solve pass
+constexpr int WSCAP = 576;        // knots staged in shared memory per warp and solve pass
 
 enum Phase : int32_t { PH_DONE = 0, PH_INIT = 1, PH_SIFT = 2, PH_TRANS = 3 };
 enum TileMode : int32_t { TM_INIT = 0, TM_SIFT = 1, TM_LAST = 2, TM_TRANS = 3 };
@@ -50,7 +54,8 @@ struct Header {
     // (0 setup, 1 solve, 2 barrier after solve, 3 sweep, 4 barrier after sweep, 5 decide, 6 claim)
     unsigned long long phase_cycles[8];
     // sweep sub-phases (lane 0 of each warp): 0 tile wait, 1 values, 2 extrema +
-    // warp scan, 3 writes
+    // warp scan, 3 writes; solve sub-phases (lane 0 of each warp): 4 knot
+    // staging, 5 slopes, 6 windows
     unsigned long long sweep_cycles[8];
 };
 

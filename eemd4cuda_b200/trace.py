@@ -10,7 +10,8 @@ from __future__ import annotations
 import numpy as np
 
 PHASES = ("setup", "solve", "barrier_solve", "sweep", "barrier_sweep", "decide", "claim")
-SWEEP_PHASES = ("tile_wait", "values", "extrema_scan", "writes")
+SWEEP_PHASES = ("tile_wait", "values", "extrema_scan", "writes", "solve_staging", "solve_slopes",
+                "solve_windows")
 _HEADER_INTS = 16  # int32 fields before phase_cycles
 
 
