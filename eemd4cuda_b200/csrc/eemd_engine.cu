@@ -749,19 +749,39 @@ __device__ __forceinline__ int phase16(const T* p) {
     return (int)((reinterpret_cast<uintptr_t>(p) / sizeof(T)) & (16 / sizeof(T) - 1));
 }
 
-// One warp copies g[0 .. cnt) to shared dst[0 .. cnt) asynchronously; dst + j
-// and g + j share their 16-byte phase, so the body moves in 16-byte copies.
+// One warp copies g[0 .. cnt) to the 16-byte aligned shared dst[0 .. cnt):
+// 16-byte copies when g is 16-byte aligned too, element copies otherwise.
 template <typename T>
-__device__ __forceinline__ void warp_copy(T* dst, const T* g, int cnt, int lane) {
+__device__ __forceinline__ void tile_copy(T* dst, const T* g, int cnt, int lane) {
     constexpr int VEC = 16 / (int)sizeof(T);
-    const int head = min(cnt, (VEC - phase16(g)) & (VEC - 1));
-    const int nvec = (cnt - head) / VEC;
-    const int tail0 = head + nvec * VEC;
-    for (int v = lane; v < nvec; v += 32) cp_async16(dst + head + v * VEC, g + head + v * VEC);
-    const int ns = head + (cnt - tail0);
-    if (lane < ns) {
-        const int j = (lane < head) ? lane : tail0 + (lane - head);
-        cp_async_el<T>(dst + j, g + j);
+    if (phase16(g) == 0) {
+        const int nvec = cnt / VEC;
+        for (int v = lane; v < nvec; v += 32) cp_async16(dst + v * VEC, g + v * VEC);
+        for (int j = nvec * VEC + lane; j < cnt; j += 32) cp_async_el<T>(dst + j, g + j);
+    } else {
+        for (int j = lane; j < cnt; j += 32) cp_async_el<T>(dst + j, g + j);
+    }
+}
+
+// a lane's run of RUN samples from a 16-byte aligned shared tile position
+template <typename T, int RUN>
+__device__ __forceinline__ void load_run(const T* p, T (&v)[RUN]) {
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int i = 0; i < RUN; i += 4) {
+            const float4 a = *reinterpret_cast<const float4*>(p + i);
+            v[i] = a.x;
+            v[i + 1] = a.y;
+            v[i + 2] = a.z;
+            v[i + 3] = a.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < RUN; i += 2) {
+            const double2 a = *reinterpret_cast<const double2*>(p + i);
+            v[i] = a.x;
+            v[i + 1] = a.y;
+        }
     }
 }
 
@@ -926,8 +946,8 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
     // tile j's samples [t0, t1) and run records into buffer b
     auto prefetch = [&](int j, int b) {
         const int t0 = s0 + j * WT, t1 = min(s1, t0 + WT);
-        if (needs_h) warp_copy<T>(tbuf + (b * 2) * G::TB + phase16(io.hsrc + t0), io.hsrc + t0, t1 - t0, lane);
-        if (USES_R) warp_copy<T>(tbuf + (b * 2 + 1) * G::TB + phase16(io.rcur + t0), io.rcur + t0, t1 - t0, lane);
+        if (needs_h) tile_copy<T>(tbuf + (b * 2) * G::TB, io.hsrc + t0, t1 - t0, lane);
+        if (USES_R) tile_copy<T>(tbuf + (b * 2 + 1) * G::TB, io.rcur + t0, t1 - t0, lane);
         if (SIFTING && lane * RUN < t1 - t0) cp_async16(rib + b * 32 + lane, ri_cur + t0 / RUN + lane);
         cp_async_commit();
     };
@@ -960,15 +980,15 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
         __syncwarp();
         if (j + 1 < tb) prefetch(j + 1, b ^ 1);
         SUB(0);
-        const T* hb = tbuf + (b * 2) * G::TB + (needs_h ? phase16(io.hsrc + t0) : 0);
-        const T* rb = tbuf + (b * 2 + 1) * G::TB + (USES_R ? phase16(io.rcur + t0) : 0);
+        const T* hb = tbuf + (b * 2) * G::TB;
+        const T* rb = tbuf + (b * 2 + 1) * G::TB;
+        // (samples past the run's end are read but never used)
         T hv[RUN], rv[RUN], fv[RUN], gv[RUN];
 #pragma unroll
-        for (int i = 0; i < RUN; ++i) {
-            const bool ok = i < nv;
-            hv[i] = (ok && needs_h) ? hb[j0 + i] : (T)0;
-            rv[i] = (ok && USES_R) ? rb[j0 + i] : (T)0;
-            fv[i] = gv[i] = (T)0;
+        for (int i = 0; i < RUN; ++i) hv[i] = rv[i] = fv[i] = gv[i] = (T)0;
+        if (nv > 0) {
+            if (needs_h) load_run<T, RUN>(hb + j0, hv);
+            if (USES_R) load_run<T, RUN>(rb + j0, rv);
         }
 
         // ---------------- new values ----------------
@@ -1658,7 +1678,9 @@ int make_layout(const eemd_params* p, const int64_t* lengths, int n_signals, int
         nmin = std::min(nmin, lengths[s]);
     }
     L.csize = p->cluster_size ? p->cluster_size : autotune_csize(n_tasks, nmin);
-    L.S = p->halo ? p->halo : (p->exact ? 32 : 24);
+    // decay halo of the seam windows: the truncation error falls like
+    // (2 - sqrt 3)^S; 16 rows put it far below float32 rounding
+    L.S = p->halo ? p->halo : (p->exact ? 32 : (p->dtype == EEMD_F32 ? 16 : 24));
     L.B = p->knots_per_block ? p->knots_per_block : 16;
     // a solve pass stages its windows' knots plus both halos in the warp's area
     if (2 * L.S + L.B + 8 > WSCAP || 2 * L.S + FAST_B + 8 > WSCAP) return EEMD_E_BADARG;
