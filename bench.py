@@ -1,13 +1,22 @@
 #!/usr/bin/env python
 """EEMD throughput on one B200 (or N independent replicas), one JSON line.
 
-Workload (one "step"): full EEMD of 1 s of 48 kHz synthetic audio -- harmonic
-tone f0=220 Hz with 8 partials (1/k), pink noise at -30 dB, 5 decaying clicks,
-seed 1 -- N=48000 samples, 100 trials, Philox noise 0.2*std(x), 8 IMFs,
-fixed 10 sifts per IMF, float32 storage with float64 spline solve.
-Metric: Msamples*trials/s = N*E / step time (whole job: summed over ranks).
+Default workload (one "step"): full EEMD of 1 s of 48 kHz synthetic audio --
+harmonic tone f0=220 Hz with 8 partials (1/k), pink noise at -30 dB, 5
+decaying clicks, seed 1 -- N=48000 samples, 100 trials, Philox noise
+0.2*std(x), 8 IMFs, fixed 10 sifts per IMF, float32 storage with float64
+spline solve.  Metric: Msamples*trials/s = sum(N)*E / step time (whole job:
+summed over ranks).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload harmonic48k|plain8k|amfm4m|uneven512]
+
+The other workloads measure the remaining configurations of the path:
+plain8k (single-trial plain EMD, float64, mirror ends, N=8192), amfm4m (N=2^22
+AM/FM signal, float64, 256 trials in launches of 64, 12 IMFs, SD<0.2 capped
+at 20 sifts, seam halo 30) and uneven512 (512 signals of log-uniform length
+4096..262144, 64 trials in launches of 16, 10 IMFs, float32 storage; the line
+also times the same work as one launch sequence per signal).
 
 --impl reference times the reference's CPU algorithm (the numpy port in
 oracle/, emd_ref.py semantics, float64) on the host cores with a spawn process
@@ -23,6 +32,7 @@ import subprocess
 import sys
 import threading
 import time
+from dataclasses import dataclass, field
 from pathlib import Path
 
 import numpy as np
@@ -30,20 +40,93 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-N = 48000
-E = 100
-EPS = 0.2
-MAX_IMF = 8
-MAX_SIFTS = 10
-TAU = 0.0          # SD < 0 never holds: every IMF gets exactly MAX_SIFTS sifts
-SEED = 1
 METRIC = "EEMD Msamples*trials/s"
 UNIT = "Msamples*trials/s"
 L2_BYTES = 126 * 1024 * 1024
-CONFIG = {"workload": "harmonic_clicks_48k_eemd", "N": N, "trials": E, "eps": EPS,
-          "max_imf": MAX_IMF, "sifts_per_imf": MAX_SIFTS, "storage": "float32",
-          "solve": "float64", "noise": "philox", "signals": 1,
-          "l2": "flushed between timed steps (256 MiB write)"}
+
+
+@dataclass
+class Workload:
+    name: str
+    config: dict
+    E: int
+    eps: float
+    max_imf: int
+    max_sifts: int
+    tau: float            # SD threshold; 0 never holds, so every IMF takes max_sifts sifts
+    dtype: str            # "f32" or "f64" storage (the spline solve is float64 either way)
+    seed: int
+    end: str = "natural"
+    halo: int = 0         # seam-window halo (0: the engine's default)
+    trial_batch: int = 0  # trials per launch (0: all at once)
+    per_signal: bool = False  # also time the same work as one launch sequence per signal
+    cpu_tasks: int = 0        # CPU-baseline sample: tasks (0: one per core, at most 32)
+    cpu_max_imf: int = 0      # CPU-baseline sample: IMFs per task (0: all)
+    cpu_max_sifts: int = 0    # CPU-baseline sample: sift cap (0: the workload's)
+    signals_fn: object = None
+    _signals: list = field(default=None, repr=False)
+
+    def signals(self) -> list:
+        if self._signals is None:
+            self._signals = [np.asarray(s, dtype=np.float64) for s in self.signals_fn()]
+        return self._signals
+
+    @property
+    def np_dtype(self):
+        return np.float32 if self.dtype == "f32" else np.float64
+
+
+def _harmonic():
+    from eemd4cuda_b200 import signals
+    return [signals.harmonic_clicks(48000, seed=1)]
+
+
+def _plain8k():
+    from eemd4cuda_b200 import signals
+    return [signals.plain_emd_8k()]
+
+
+def _amfm():
+    from eemd4cuda_b200 import signals
+    return [signals.amfm_long(1 << 22, seed=2)]
+
+
+def _uneven():
+    from eemd4cuda_b200 import signals
+    return signals.uneven_batch(512, seed=4)
+
+
+WORKLOADS = {
+    "harmonic48k": Workload(
+        "harmonic48k",
+        {"workload": "harmonic_clicks_48k_eemd", "N": 48000, "trials": 100, "eps": 0.2,
+         "max_imf": 8, "sifts_per_imf": 10, "storage": "float32", "solve": "float64",
+         "noise": "philox", "signals": 1},
+        E=100, eps=0.2, max_imf=8, max_sifts=10, tau=0.0, dtype="f32", seed=1,
+        signals_fn=_harmonic),
+    "plain8k": Workload(
+        "plain8k",
+        {"workload": "plain_emd_8k", "N": 8192, "trials": 1, "max_imf": 10, "tau": 0.2,
+         "max_sifts": 10, "ends": "mirror", "storage": "float64", "solve": "float64",
+         "signals": 1},
+        E=1, eps=0.0, max_imf=10, max_sifts=10, tau=0.2, dtype="f64", seed=0, end="mirror",
+        cpu_tasks=8, signals_fn=_plain8k),
+    "amfm4m": Workload(
+        "amfm4m",
+        {"workload": "amfm_2^22_eemd", "N": 1 << 22, "trials": 256, "eps": 0.2, "max_imf": 12,
+         "tau": 0.2, "max_sifts": 20, "storage": "float64", "solve": "float64",
+         "seam_halo": 30, "noise": "philox", "signals": 1, "trials_per_launch": 64},
+        E=256, eps=0.2, max_imf=12, max_sifts=20, tau=0.2, dtype="f64", seed=2, halo=30,
+        trial_batch=64, cpu_tasks=16, cpu_max_imf=1, cpu_max_sifts=2, signals_fn=_amfm),
+    "uneven512": Workload(
+        "uneven512",
+        {"workload": "uneven_512_signals_eemd", "signals": 512,
+         "lengths": "log-uniform 4096..262144", "trials": 64, "eps": 0.2, "max_imf": 10,
+         "sifts_per_imf": 10, "storage": "float32", "solve": "float64", "noise": "philox",
+         "trials_per_launch": 16},
+        E=64, eps=0.2, max_imf=10, max_sifts=10, tau=0.0, dtype="f32", seed=1, trial_batch=16,
+        per_signal=True, cpu_tasks=32, signals_fn=_uneven),
+}
 
 
 def rank_env():
@@ -51,69 +134,94 @@ def rank_env():
             int(os.environ.get("WORLD_SIZE", 1)))
 
 
-def workload_signal():
-    from eemd4cuda_b200 import signals
-    return signals.harmonic_clicks(N, seed=SEED)
-
-
 # ---------------------------------------------------------------------------
 # CPU side (reference algorithm, numpy port)
 # ---------------------------------------------------------------------------
 class CpuBaseline:
-    """emd_1d of x + noise_e for a bounded number of trials in a spawn pool."""
+    """emd_1d of (signal, trial) tasks of the workload in a spawn process pool.
 
-    def __init__(self, trials: int | None = None):
+    The sample is a bounded set of tasks (x + its trial noise, float64) so that
+    one step takes seconds.  With cpu_max_imf / cpu_max_sifts the sample runs
+    only the first sifts, and `value` scales the time per sift to a full
+    task's sift count."""
+
+    def __init__(self, wl: Workload):
         import multiprocessing as mp
         from concurrent.futures import ProcessPoolExecutor
 
-        self.cores = os.cpu_count() or 1
-        self.trials = trials or max(4, min(self.cores, 32))
-        self.x = workload_signal().astype(np.float32).astype(np.float64)
-        sigma = EPS * np.std(self.x)
-        rng = np.random.default_rng(SEED)
-        self.noises = rng.standard_normal((self.trials, N)) * sigma
+        self.wl = wl
+        self.cores = 1 if wl.E == 1 else (os.cpu_count() or 1)
+        sig = wl.signals()
+        rng = np.random.default_rng(wl.seed)
+        n_tasks = wl.cpu_tasks or max(4, min(self.cores, 32))
+        self.tasks = []
+        for _ in range(n_tasks):
+            s = int(rng.integers(len(sig))) if len(sig) > 1 else 0
+            x = sig[s].astype(wl.np_dtype).astype(np.float64)
+            if wl.E > 1:
+                noise = rng.standard_normal(len(x)) * (wl.eps * np.std(x))
+            else:
+                noise = np.zeros(len(x))
+            self.tasks.append((x, noise))
+        self.kw = dict(tau=wl.tau, max_sifts=wl.cpu_max_sifts or wl.max_sifts,
+                       max_imf=wl.cpu_max_imf or wl.max_imf, end=wl.end)
         self.pool = ProcessPoolExecutor(max_workers=self.cores, mp_context=mp.get_context("spawn"))
+        self.sifts_done = 0
+        self.full_sifts = None
 
     def step(self) -> float:
         from concurrent.futures import as_completed
         from oracle import emd_oracle as O
 
-        kw = dict(tau=TAU, max_sifts=MAX_SIFTS, max_imf=MAX_IMF)
         t0 = time.perf_counter()
-        futs = [self.pool.submit(O._trial_worker, (self.x, self.noises[e], kw))
-                for e in range(self.trials)]
+        futs = [self.pool.submit(O._trial_worker, (x, nz, self.kw)) for x, nz in self.tasks]
+        sifts = 0
         for f in as_completed(futs):
-            f.result()
+            sifts += f.result()[1]
+        self.sifts_done = sifts
         return time.perf_counter() - t0
 
-    def value(self, seconds: float) -> float:
-        return self.trials * N / seconds / 1e6
+    def value(self, seconds: float, full_sifts_per_task: float | None = None) -> float:
+        samples = sum(len(x) for x, _ in self.tasks)
+        if self.wl.cpu_max_imf or self.wl.cpu_max_sifts:
+            self.full_sifts = full_sifts_per_task or self.wl.max_imf * self.wl.max_sifts / 2
+            seconds *= self.full_sifts / max(self.sifts_done / len(self.tasks), 1e-9)
+        return samples / seconds / 1e6
 
     def describe(self, v: float) -> dict:
+        wl = self.wl
+        what = (f"{len(self.tasks)} (signal, trial) tasks of the workload (emd_1d, float64, "
+                f"tau={wl.tau}, max_sifts={self.kw['max_sifts']}, max_imf={self.kw['max_imf']}, "
+                f"{wl.end} ends) in a {self.cores}-process pool")
+        if wl.cpu_max_imf or wl.cpu_max_sifts:
+            what += (f"; the time per sift of IMF 1 scaled to {self.full_sifts:.1f} sifts per task "
+                     "(IMF-1 sifts are the slowest, so this bounds the CPU time from above)")
         return {"value": round(v, 4), "unit": UNIT, "cores": self.cores, "kind": "port",
-                "sample": f"{self.trials} of the {E} trials of the workload (emd_1d, float64, "
-                          f"tau=0 / {MAX_SIFTS} sifts, {MAX_IMF} IMFs) in a {self.cores}-process pool"}
+                "sample": what}
 
     def close(self):
         self.pool.shutdown()
 
 
-def run_reference(args):
+def run_reference(args, wl: Workload):
     rank, _, world = rank_env()
     if rank != 0:
         return 0
-    cb = CpuBaseline()
-    for _ in range(args.warmup):
+    cb = CpuBaseline(wl)
+    big = wl.name in ("amfm4m", "uneven512")
+    steps = max(1, min(args.steps, 2)) if big else args.steps
+    warm = 1 if big else args.warmup
+    for _ in range(warm):
         cb.step()
-    ts = [cb.step() for _ in range(args.steps)]
+    ts = [cb.step() for _ in range(steps)]
     cb.close()
     sec = sum(ts) / len(ts)
     v = cb.value(sec)
     line = {"impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT,
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "n_gpus": args.gpus, "steps": steps, "warmup": warm,
             "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(CONFIG, storage="float64", sample_trials=cb.trials),
+            "config": dict(wl.config, storage="float64", sample_tasks=len(cb.tasks)),
             "cpu_baseline": cb.describe(v),
             "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -208,38 +316,79 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
-def emd_algorithmic_bytes(klog: np.ndarray, nmode: np.ndarray, bytes_el: int) -> float:
+def emd_algorithmic_bytes(klog: np.ndarray, nmode: np.ndarray, lengths, trials: int,
+                          bytes_el: int) -> float:
     """Algorithmic bytes of one k_emd launch, from the per-sift knot log.
 
-    Per trial: read x and write the residual (2*N*b) and the first knot list
-    (P0*(4+b)).  Per sift with P = maxima+minima knots: the solve reads the knots
-    (P*(4+b)) and writes the second derivatives (8*P); the sweep reads and writes
-    h (2*N*b), reads knots and second derivatives (P*(4+b+8)) and writes the
-    next knot list (P'*(4+b)).  The sift that closes an IMF also reads and
-    writes the residual (2*N*b)."""
+    Per task of a signal of n samples (b bytes per sample; P = maxima + minima
+    knots of a sift): per sift 3*n*b + P*(3*(4+b) + 2*8) -- extrema pass
+    (reads h, writes the knots), solve (reads the knots, writes the second
+    derivatives), evaluation pass (reads and writes h, reads knots and second
+    derivatives); per IMF 4*n*b (residual read and write, IMF read, the next
+    count's read); per task 2*n*b (input read, perturbed-input write).  The
+    float64 ensemble accumulator belongs to k_reduce and is not counted."""
     total = 0.0
     kb = 4 + bytes_el
-    for e in range(klog.shape[0]):
-        seq = []
-        for m in range(int(nmode[e])):
+    for t in range(klog.shape[0]):
+        n = int(lengths[t // trials])
+        total += 2 * n * bytes_el
+        for m in range(int(nmode[t])):
             for k in range(klog.shape[2]):
-                a, b = klog[e, m, k]
+                a, b = klog[t, m, k]
                 if a < 0:
                     break
-                seq.append((m, int(a) + int(b)))
-        total += 2 * N * bytes_el
-        if seq:
-            total += seq[0][1] * kb
-        for i, (m, P) in enumerate(seq):
-            Pn = seq[i + 1][1] if i + 1 < len(seq) else P
-            total += P * kb + 8 * P                      # solve
-            total += 2 * N * bytes_el + P * (kb + 8) + Pn * kb   # sweep
-            if i + 1 == len(seq) or seq[i + 1][0] != m:
-                total += 2 * N * bytes_el                # residual update at the IMF close
+                total += 3 * n * bytes_el + (int(a) + int(b)) * (3 * kb + 16)
+            total += 4 * n * bytes_el
     return total
 
 
-def run_ours(args):
+class Engine:
+    """Device buffers and one EEMD step of a workload (all signals, all trials)."""
+
+    def __init__(self, wl: Workload, dev, seed: int, signals=None):
+        import torch
+        from eemd4cuda_b200 import _lib as L
+        from eemd4cuda_b200 import emd_par as M
+
+        self.L, self.wl = L, wl
+        sig = signals if signals is not None else wl.signals()
+        self.lengths = [len(s) for s in sig]
+        self.n_total = sum(self.lengths)
+        noise = L.EEMD_NOISE_PHILOX if wl.E > 1 else L.EEMD_NOISE_NONE
+        cfg = M.EngineConfig(halo=wl.halo) if wl.halo else None
+        self.p = M.make_params(dtype=wl.np_dtype, noise_mode=noise, eps=wl.eps, seed=seed,
+                               tau=wl.tau, max_sifts=wl.max_sifts, max_imf=wl.max_imf, end=wl.end,
+                               config=cfg)
+        self.batch = wl.trial_batch or wl.E
+        self.host = np.concatenate([s.astype(wl.np_dtype) for s in sig])
+        self.xd = torch.from_numpy(self.host).to(dev)
+        self.ws = torch.empty((L.workspace_size(self.p, self.lengths, self.batch, False),),
+                              dtype=torch.uint8, device=dev)
+        m = wl.max_imf
+        self.imf_sum = torch.zeros((m * self.n_total,), dtype=torch.float64, device=dev)
+        self.mode_count = torch.zeros((len(sig) * m,), dtype=torch.int32, device=dev)
+        self.imf_mean = torch.empty((m * self.n_total,), dtype=torch.float64, device=dev)
+        self.resid = torch.empty((self.n_total,), dtype=torch.float64, device=dev)
+        self.n_modes = torch.empty((len(sig),), dtype=torch.int32, device=dev)
+
+    def step(self, times=None, klog=None, nmode=None, nsift=None):
+        self.imf_sum.zero_()
+        self.mode_count.zero_()
+        for b0 in range(0, self.wl.E, self.batch):
+            eb = min(self.batch, self.wl.E - b0)
+            first = b0 == 0
+            self.L.run(self.p, self.xd, self.lengths, b0, eb, self.ws, imf_sum=self.imf_sum,
+                       mode_count=self.mode_count, times=times if first else None,
+                       knot_log=klog if first else None, nmode=nmode if first else None,
+                       nsift=nsift if first else None)
+        self.L.finalize(self.p, self.xd, self.lengths, self.imf_sum, self.mode_count,
+                        self.imf_mean, self.resid, self.n_modes)
+
+    def launch_batches(self) -> int:
+        return (self.wl.E + self.batch - 1) // self.batch
+
+
+def run_ours(args, wl: Workload):
     import torch
 
     rank, local_rank, world = rank_env()
@@ -252,33 +401,18 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
                                 device_id=dev)
 
-    from eemd4cuda_b200 import _lib as L
     from eemd4cuda_b200 import emd_par as M
 
     # the CPU baseline pool is started before any GPU work (spawn context)
-    cb = CpuBaseline() if (rank == 0 and world == 1) else None
+    cb = CpuBaseline(wl) if (rank == 0 and world == 1) else None
 
-    x = workload_signal().astype(np.float32)
-    p = M.make_params(dtype=np.float32, noise_mode=L.EEMD_NOISE_PHILOX, eps=EPS, seed=SEED + rank,
-                      tau=TAU, max_sifts=MAX_SIFTS, max_imf=MAX_IMF)
-    xd = torch.from_numpy(x).to(dev)
-    ws = torch.empty((L.workspace_size(p, [N], E, False),), dtype=torch.uint8, device=dev)
-    imf_sum = torch.zeros((MAX_IMF, N), dtype=torch.float64, device=dev)
-    mode_count = torch.zeros((MAX_IMF,), dtype=torch.int32, device=dev)
-    imf_mean = torch.empty((MAX_IMF, N), dtype=torch.float64, device=dev)
-    resid = torch.empty((N,), dtype=torch.float64, device=dev)
-    nmodes = torch.empty((1,), dtype=torch.int32, device=dev)
+    eng = Engine(wl, dev, wl.seed + rank)
+    L = eng.L
     flush = torch.empty((2 * L2_BYTES,), dtype=torch.uint8, device=dev)
-
-    def step(times=None, klog=None, nmode=None):
-        imf_sum.zero_()
-        mode_count.zero_()
-        L.run(p, xd, [N], 0, E, ws, imf_sum=imf_sum, mode_count=mode_count, times=times,
-              knot_log=klog, nmode=nmode)
-        L.finalize(p, xd, [N], imf_sum, mode_count, imf_mean, resid, nmodes)
+    samples_trials = eng.n_total * wl.E
 
     for _ in range(args.warmup):
-        step()
+        eng.step()
     torch.cuda.synchronize()
 
     # ---- timed region: K steps, device time per step with CUDA events ----
@@ -294,7 +428,7 @@ def run_ours(args):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        step()
+        eng.step()
         e1.record(stream)
         e1.synchronize()
         total_ms += e0.elapsed_time(e1)
@@ -307,62 +441,115 @@ def run_ours(args):
         t = torch.tensor([ms], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    value = world * N * E / (ms / 1e3) / 1e6
+    value = world * samples_trials / (ms / 1e3) / 1e6
 
-    # ---- per-kernel split (traced step, event pair around every launch) ----
+    # ---- per-kernel split (traced step: event pair around every launch of the first batch) ----
     times = L.KernelTimes()
-    klog = torch.full((E, MAX_IMF, MAX_SIFTS, 2), -1, dtype=torch.int32, device=dev)
-    nmode = torch.zeros((E,), dtype=torch.int32, device=dev)
+    n_first = len(eng.lengths) * eng.batch
+    klog = torch.full((n_first, wl.max_imf, wl.max_sifts, 2), -1, dtype=torch.int32, device=dev)
+    nmode = torch.zeros((n_first,), dtype=torch.int32, device=dev)
+    nsift = torch.zeros((n_first,), dtype=torch.int32, device=dev)
     flush.fill_(1)
-    step(times=times, klog=klog, nmode=nmode)
+    eng.step(times=times, klog=klog, nmode=nmode, nsift=nsift)
     torch.cuda.synchronize()
     kt = times.as_dict()
-    launches_per_step = sum(v["launches"] for v in kt.values()) + 1  # + k_finalize
+    launches_per_step = sum(v["launches"] for v in kt.values()) * eng.launch_batches() + 1
     ev = kt["emd"]
-    emd_bytes = emd_algorithmic_bytes(klog.cpu().numpy(), nmode.cpu().numpy(), 4)
+    bytes_el = 4 if wl.dtype == "f32" else 8
+    emd_bytes = emd_algorithmic_bytes(klog.cpu().numpy(), nmode.cpu().numpy(), eng.lengths,
+                                      eng.batch, bytes_el)
     emd_gbs = emd_bytes / (ev["ms"] / 1e3) / 1e9 if ev["ms"] > 0 else 0.0
+    gpu_sifts_per_task = float(nsift.float().mean().item())
     peak, peak_kind = measured_peak_hbm()
     traffic = None
     tf = ROOT / "profiles" / "emd_traffic.json"
-    if tf.exists():
+    if wl.name == "harmonic48k" and tf.exists():
         try:
             traffic = json.loads(tf.read_text()).get("bytes_per_launch")
         except ValueError:
             traffic = None
 
     # ---- end to end through the public API (host buffers) ----
-    def e2e_call():
-        return M.decompose(x, E=E, eps=EPS, tau=TAU, max_sifts=MAX_SIFTS, max_imf=MAX_IMF,
-                           seed=SEED + rank, dtype=np.float32)
+    if wl.name in ("harmonic48k", "plain8k"):
+        x = wl.signals()[0].astype(wl.np_dtype)
+        cfg = M.EngineConfig(halo=wl.halo) if wl.halo else None
 
-    for _ in range(args.warmup):
+        def e2e_call():
+            r = M.decompose(x, E=wl.E, eps=wl.eps, tau=wl.tau, max_sifts=wl.max_sifts,
+                            max_imf=wl.max_imf, seed=wl.seed + rank, end=wl.end,
+                            dtype=wl.np_dtype, config=cfg)
+            return r.n_modes
+        h2d = x.nbytes
+        e2e_warm = args.warmup
+    else:
+        # the batched C ABI: pinned host input in, ensemble means and residuals out
+        pin_in = torch.from_numpy(eng.host).pin_memory()
+        pin_out = torch.empty((wl.max_imf * eng.n_total,), dtype=torch.float64).pin_memory()
+        pin_res = torch.empty((eng.n_total,), dtype=torch.float64).pin_memory()
+
+        def e2e_call():
+            eng.xd.copy_(pin_in, non_blocking=True)
+            eng.step()
+            pin_out.copy_(eng.imf_mean, non_blocking=True)
+            pin_res.copy_(eng.resid, non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+            return wl.max_imf
+        h2d = eng.host.nbytes
+        e2e_warm = 1
+
+    for _ in range(e2e_warm):
         e2e_call()
     torch.cuda.synchronize()
     e2e_ms = []
-    n_modes_e2e = MAX_IMF
-    for i in range(max(args.steps, 1)):
+    n_modes_e2e = wl.max_imf
+    for _ in range(max(args.steps, 1)):
         flush.fill_(1)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        r = e2e_call()
+        n_modes_e2e = e2e_call()
         e1.record(stream)
         e1.synchronize()
         e2e_ms.append(e0.elapsed_time(e1))
-        n_modes_e2e = r.n_modes
     e2e = statistics.median(e2e_ms)
     if dist:
         t = torch.tensor([e2e], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e = float(t.item())
-    e2e_value = world * N * E / (e2e / 1e3) / 1e6
+    e2e_value = world * samples_trials / (e2e / 1e3) / 1e6
+    d2h = n_modes_e2e * eng.n_total * 8 + eng.n_total * 8
+    if wl.name in ("harmonic48k", "plain8k"):
+        d2h += 3 * wl.E * 4  # per-trial sift, mode and flag counters
+
+    # ---- the same work as one launch sequence per signal ----
+    per_signal = None
+    if wl.per_signal and rank == 0:
+        engs = [Engine(wl, dev, wl.seed + rank, signals=[s]) for s in wl.signals()]
+        for e in engs:
+            e.step()
+        torch.cuda.synchronize()
+        flush.fill_(1)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for e in engs:
+            e.step()
+        e1.record(stream)
+        e1.synchronize()
+        ps_ms = e0.elapsed_time(e1)
+        per_signal = {"ms_per_step": round(ps_ms, 3),
+                      "value": round(samples_trials / (ps_ms / 1e3) / 1e6, 3),
+                      "launch_sequences": len(engs),
+                      "batched_speedup": round(ps_ms / ms, 3)}
+        del engs
+        torch.cuda.empty_cache()
 
     cpu = None
     if cb is not None:
         cb.step()  # warm the pool's imports
         cs = cb.step()
-        cpu = cb.describe(cb.value(cs))
+        cpu = cb.describe(cb.value(cs, gpu_sifts_per_task))
         cb.close()
 
     if dist:
@@ -370,14 +557,15 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank != 0:
         return 0
+    config = dict(wl.config, parallelism=f"replicas{world}",
+                  l2="flushed between timed steps (256 MiB write)")
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": dict(CONFIG, parallelism=f"replicas{world}"),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl.dtype,
+        "data": "synthetic", "config": config,
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "ms_per_step": round(e2e, 4),
-                "h2d_bytes_per_step": N * 4,
-                "d2h_bytes_per_step": n_modes_e2e * N * 8 + N * 8 + 3 * E * 4},
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches_per_step * args.steps,
         "roofline": {"bound": "hbm", "kernel": "k_emd", "achieved": round(emd_gbs, 2),
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
@@ -389,6 +577,8 @@ def run_ours(args):
         "kernel_launches": {k: v["launches"] for k, v in kt.items()},
         "clocks": clocks,
     }
+    if per_signal is not None:
+        line["per_signal_launches"] = per_signal
     if cpu is not None:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
@@ -401,12 +591,14 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="harmonic48k")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    wl = WORKLOADS[args.workload]
     if args.impl == "reference":
-        return run_reference(args)
-    return run_ours(args)
+        return run_reference(args, wl)
+    return run_ours(args, wl)
 
 
 if __name__ == "__main__":
