@@ -228,8 +228,11 @@ struct Geo {
     static constexpr int RS = sizeof(T) == 4 ? 8 : 6;   // interval record stride
     static constexpr size_t TB_BYTES = (size_t)2 * 2 * TB * sizeof(T);  // [buf][stream][TB]
     static constexpr size_t RI_BYTES = (size_t)2 * 32 * 16;             // [buf][lane]
-    static constexpr size_t WARP_BYTES = TB_BYTES + RI_BYTES;
-    static_assert(TB_BYTES % 16 == 0 && (RS * sizeof(T)) % 16 == 0, "16-byte aligned layouts");
+    static constexpr int KCAP = WT / 2 + 4;                              // knots of one kind in a tile
+    static constexpr size_t KN_BYTES = (size_t)2 * KCAP * (4 + sizeof(T));  // [kind][KCAP] index, value
+    static constexpr size_t WARP_BYTES = TB_BYTES + RI_BYTES + KN_BYTES;
+    static_assert(TB_BYTES % 16 == 0 && (RS * sizeof(T)) % 16 == 0 && KN_BYTES % 16 == 0,
+                  "16-byte aligned layouts");
 };
 
 
@@ -927,6 +930,9 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
     unsigned char* wb = smem + (size_t)wid * G::WARP_BYTES;
     T* const tbuf = reinterpret_cast<T*>(wb);                      // [2 buf][2 stream][TB]
     int4* const rib = reinterpret_cast<int4*>(wb + G::TB_BYTES);  // [2 buf][32]
+    // the tile's new knots, compacted in time order before one coalesced copy out
+    int* const kts = reinterpret_cast<int*>(wb + G::TB_BYTES + G::RI_BYTES);  // [kind][KCAP]
+    T* const kvs = reinterpret_cast<T*>(wb + G::TB_BYTES + G::RI_BYTES + 2 * G::KCAP * 4);
     double num = 0.0, den = 0.0;
 #ifdef EEMD_TRACE
     unsigned long long scyc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -1123,51 +1129,54 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
         SUB(2);
 
         // ---------------- writes ----------------
-        int px = wcx + (exc & 0xffff), pn = wcy + (exc >> 16);
+        // knots go to shared memory at their tile position, then to the warp's
+        // lists with one coalesced copy per kind
+        int px = exc & 0xffff, pn = exc >> 16;  // tile positions
         if (lane == 0 && j > ta) {
             // the previous tile's last sample and the run record that waited for it
             if (dmx) {
-                if (px < C.segcap) {
-                    sl.kt[pmx + px] = t0 - 1;
-                    static_cast<T*>(sl.ky)[pmx + px] = gm1;
-                } else {
-                    raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
-                }
+                kts[px] = t0 - 1;
+                kvs[px] = gm1;
             }
             if (dmn) {
-                if (pn < C.segcap) {
-                    sl.kt[pmn + pn] = t0 - 1;
-                    static_cast<T*>(sl.ky)[pmn + pn] = gm1;
-                } else {
-                    raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
-                }
+                kts[G::KCAP + pn] = t0 - 1;
+                kvs[G::KCAP + pn] = gm1;
             }
             ri_nxt[crun] = make_int4(cpx, cpn, cmask | (int)(dmx << cbit) | (int)(dmn << (16 + cbit)), 0);
             px += (int)dmx;
             pn += (int)dmn;
         }
-        const int rpx = px, rpn = pn, rmask = (int)(nmx | (nmn << 16));
+        const int rpx = wcx + px, rpn = wcy + pn, rmask = (int)(nmx | (nmn << 16));
         if (nv > 0 && lane != last_lane) ri_nxt[t0 / RUN + lane] = make_int4(rpx, rpn, rmask, 0);
 #pragma unroll
         for (int i = 0; i < RUN; ++i) {
             const int t = t0 + j0 + i;
             if ((nmx >> i) & 1u) {
-                if (px < C.segcap) {
-                    sl.kt[pmx + px] = t;
-                    static_cast<T*>(sl.ky)[pmx + px] = gv[i];
-                } else {
-                    raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
-                }
+                kts[px] = t;
+                kvs[px] = gv[i];
                 ++px;
             }
             if ((nmn >> i) & 1u) {
-                if (pn < C.segcap) {
-                    sl.kt[pmn + pn] = t;
-                    static_cast<T*>(sl.ky)[pmn + pn] = gv[i];
-                } else {
-                    raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
-                }
+                kts[G::KCAP + pn] = t;
+                kvs[G::KCAP + pn] = gv[i];
                 ++pn;
+            }
+        }
+        __syncwarp();
+        {
+            const int nx = tot & 0xffff, nn = tot >> 16;
+            if (wcx + nx > C.segcap || wcy + nn > C.segcap || nx > G::KCAP || nn > G::KCAP) {
+                if (lane == 0) raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
+            } else {
+                T* const ky = static_cast<T*>(sl.ky);
+                for (int k = lane; k < nx; k += 32) {
+                    sl.kt[pmx + wcx + k] = kts[k];
+                    ky[pmx + wcx + k] = kvs[k];
+                }
+                for (int k = lane; k < nn; k += 32) {
+                    sl.kt[pmn + wcy + k] = kts[G::KCAP + k];
+                    ky[pmn + wcy + k] = kvs[G::KCAP + k];
+                }
             }
         }
         const int tj = t0 + j0;
