@@ -295,27 +295,39 @@ __device__ __forceinline__ void real_knot(const Ctx& C, const Slot& sl, const Ta
     y = (double)__ldcg(static_cast<const T*>(sl.ky) + o);
 }
 
-// Stage mirror-space knot i2 into shared memory: an asynchronous copy for a
-// real knot, a direct store for a virtual mirror knot.
+// Stage the mirror-space knots rlo .. rlo+kcount-1 (lane-strided); each lane
+// finds the segment of its first real knot by binary search and then walks
+// forward, since its later knots follow in the same or later segments.
 template <typename T>
-__device__ __forceinline__ void stage_knot(const Ctx& C, const Slot& sl, const TaskSm& S, int env, int i2,
-                                           int* kt_s, T* ky_s) {
-    if (S.mir[env]) {
-        if (i2 == 0) {
-            *kt_s = S.tfirst[env];
-            *ky_s = (T)S.yfirst[env];
-            return;
+__device__ __forceinline__ void stage_range(const Ctx& C, const Slot& sl, const TaskSm& S, int env, int rlo,
+                                            int kcount, int* skt, T* sky, int lane) {
+    const int* pr = S.pref[S.kpar][env];
+    const int nseg = S.csize * NWARP;
+    const int mir = S.mir[env], P = S.P[env];
+    int r = -1;
+    for (int k = lane; k < kcount; k += 32) {
+        int i2 = rlo + k;
+        int* kt_s = &skt[stage_pad(k)];
+        T* ky_s = &sky[stage_pad(k)];
+        if (mir) {
+            if (i2 == 0) {
+                *kt_s = S.tfirst[env];
+                *ky_s = (T)S.yfirst[env];
+                continue;
+            }
+            if (i2 == P + 1) {
+                *kt_s = S.tlast[env];
+                *ky_s = (T)S.ylast[env];
+                continue;
+            }
+            i2 -= 1;
         }
-        if (i2 == S.P[env] + 1) {
-            *kt_s = S.tlast[env];
-            *ky_s = (T)S.ylast[env];
-            return;
-        }
-        i2 -= 1;
+        if (r < 0) r = seg_of(pr, 0, nseg, i2);
+        while (r + 1 < nseg && i2 >= pr[r + 1]) ++r;
+        const int64_t o = knot_index(C, S.kpar, env, r, i2 - pr[r]);
+        cp_async4(kt_s, sl.kt + o);
+        cp_async_el<T>(ky_s, static_cast<const T*>(sl.ky) + o);
     }
-    const int64_t o = real_off(C, S, env, i2);
-    cp_async4(kt_s, sl.kt + o);
-    cp_async_el<T>(ky_s, static_cast<const T*>(sl.ky) + o);
 }
 
 // Knot i2 in "mirror space" (emd_ref.py:92-96): with mir=1 the list is
@@ -603,8 +615,7 @@ __device__ void solve_task(const Ctx& C, const Slot& sl, TaskSm& S, unsigned cha
         const int rlo = max(0, w0 * Bw - C.S);
         const int rhi = min(n - 1, min(n, wend * Bw) - 1 + C.S);
         const int kcount = rhi + 3 - rlo;  // knots rlo .. rhi+2
-        for (int k = lane; k < kcount; k += 32)
-            stage_knot<T>(C, sl, S, env, rlo + k, &skt[stage_pad(k)], &sky[stage_pad(k)]);
+        stage_range<T>(C, sl, S, env, rlo, kcount, skt, sky, lane);
         cp_async_commit();
         cp_async_wait<0>();
         __syncwarp();
