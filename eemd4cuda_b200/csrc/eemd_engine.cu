@@ -819,6 +819,19 @@ __device__ __forceinline__ void store_run(T* p, const T (&v)[RUN], int nv) {
         if (i < nv) p[i] = v[i];
 }
 
+// a lane's run of RUN values into a 16-byte aligned shared position
+template <typename T, int RUN>
+__device__ __forceinline__ void store_run_smem(T* p, const T (&v)[RUN]) {
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int i = 0; i < RUN; i += 4)
+            *reinterpret_cast<float4*>(p + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < RUN; i += 2) *reinterpret_cast<double2*>(p + i) = make_double2(v[i], v[i + 1]);
+    }
+}
+
 // value at tile position pos (lane pos/RUN, element pos%RUN), to every lane
 template <typename T, int RUN>
 __device__ __forceinline__ T tile_at(const T (&v)[RUN], int pos) {
@@ -1111,18 +1124,26 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
         const T up = __shfl_up_sync(FULL, gv[RUN - 1], 1);
         const T dn = __shfl_down_sync(FULL, gv[0], 1);
         const T gprev = (lane == 0) ? gm1 : up;
+        // samples of the run that may be knots: inside the run, not the tile's
+        // last sample, and 1 <= t <= n-2
+        unsigned valid = (1u << nv) - 1u;
+        if (j0 + nv == tl && nv > 0) valid &= ~(1u << (nv - 1));
+        if (t0 + j0 == 0) valid &= ~1u;
+        {
+            const int lim = n - 2 - (t0 + j0);  // largest run index with t <= n-2
+            if (lim < RUN - 1) valid &= (lim < 0) ? 0u : ((2u << lim) - 1u);
+        }
         unsigned nmx = 0u, nmn = 0u;
 #pragma unroll
         for (int i = 0; i < RUN; ++i) {
-            const int pos = j0 + i, t = t0 + pos;
-            if (i < nv && pos != tl - 1 && t >= 1 && t <= n - 2) {
-                const T a = (i == 0) ? gprev : gv[(i + RUN - 1) % RUN];
-                const T c = (i + 1 < RUN) ? gv[(i + 1) % RUN] : dn;
-                const T v = gv[i];
-                if (v > a && v > c) nmx |= 1u << i;
-                if (v < a && v < c) nmn |= 1u << i;
-            }
+            const T a = (i == 0) ? gprev : gv[(i + RUN - 1) % RUN];
+            const T c = (i + 1 < RUN) ? gv[(i + 1) % RUN] : dn;
+            const T v = gv[i];
+            nmx |= (unsigned)((v > a) & (v > c)) << i;
+            nmn |= (unsigned)((v < a) & (v < c)) << i;
         }
+        nmx &= valid;
+        nmn &= valid;
         unsigned dmx = 0u, dmn = 0u;  // the previous tile's last sample (lane 0)
         if (lane == 0 && j > ta && t0 - 1 >= 1 && t0 - 1 <= n - 2) {
             dmx = (gm1 > gm2 && gm1 > gv[0]) ? 1u : 0u;
@@ -1159,17 +1180,21 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
         }
         const int rpx = wcx + px, rpn = wcy + pn, rmask = (int)(nmx | (nmn << 16));
         if (nv > 0 && lane != last_lane) ri_nxt[t0 / RUN + lane] = make_int4(rpx, rpn, rmask, 0);
-#pragma unroll
-        for (int i = 0; i < RUN; ++i) {
-            const int t = t0 + j0 + i;
-            if ((nmx >> i) & 1u) {
-                kts[px] = t;
-                kvs[px] = gv[i];
+        {
+            // the run's new values go to the (already consumed) h tile buffer, so a
+            // knot's value is read by index; only the set bits are visited
+            T* const gsm = tbuf + (b * 2) * G::TB + j0;
+            store_run_smem<T, RUN>(gsm, gv);
+            for (unsigned m = nmx; m; m &= m - 1u) {
+                const int i = __ffs(m) - 1;
+                kts[px] = t0 + j0 + i;
+                kvs[px] = gsm[i];
                 ++px;
             }
-            if ((nmn >> i) & 1u) {
-                kts[G::KCAP + pn] = t;
-                kvs[G::KCAP + pn] = gv[i];
+            for (unsigned m = nmn; m; m &= m - 1u) {
+                const int i = __ffs(m) - 1;
+                kts[G::KCAP + pn] = t0 + j0 + i;
+                kvs[G::KCAP + pn] = gsm[i];
                 ++pn;
             }
         }
