@@ -38,7 +38,10 @@ constexpr int THREADS = 32 * EEMD_CTA_WARPS;  // threads per CTA of k_emd
 constexpr int CTAS_PER_SM = 16 / EEMD_CTA_WARPS;  // 16 warps of 128 registers fill an SM
 constexpr int MAXC = 8;           // largest cluster
 constexpr int FAST_B = 8;         // owned rows per window, fast solve (register resident)
-constexpr int WSCAP = 576;        // knots staged in shared memory per warp and solve pass
+#ifndef EEMD_WSCAP
+#define EEMD_WSCAP 352
+#endif
+constexpr int WSCAP = EEMD_WSCAP;  // knots staged in shared memory per warp and solve pass
 
 enum Phase : int32_t { PH_DONE = 0, PH_INIT = 1, PH_SIFT = 2, PH_TRANS = 3 };
 enum TileMode : int32_t { TM_INIT = 0, TM_SIFT = 1, TM_LAST = 2, TM_TRANS = 3 };

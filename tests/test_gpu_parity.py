@@ -204,7 +204,7 @@ def test_cluster_size_invariance(sweep, cluster_size):
         assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("B,S", [(16, 32), (250, 30), (480, 32), (64, 48)])
+@pytest.mark.parametrize("B,S", [(16, 32), (250, 30), (272, 32), (64, 48)])
 def test_block_thomas_windows(sweep, B, S):
     """Decay-seamed windows of any size agree with the exact serial result."""
     x = sweep[:50000]
