@@ -10,6 +10,7 @@ Outputs (git-ignored, shipped next to the sources):
     eemd4cuda_b200/lib/libeemd_b200_trace.so    -DEEMD_TRACE: the persistent
         kernel sums clock64() cycles per phase into the workspace header
         (eemd4cuda_b200.trace reads them)
+    eemd4cuda_b200/lib/libeemd_surrogate.so     the learned surrogate's kernels
 """
 from __future__ import annotations
 
@@ -47,10 +48,25 @@ def _stale(out: Path, deps) -> bool:
     return any(p.stat().st_mtime > t for p in deps)
 
 
+SG_SOURCES = ["surrogate.cu"]
+
+
 def build(force: bool = False, verbose: bool = False) -> list[Path]:
     LIB.mkdir(exist_ok=True)
     deps = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
     outs = []
+    # the surrogate's kernels (a library of their own; default float contraction)
+    out = LIB / "libeemd_surrogate.so"
+    outs.append(out)
+    sg_deps = [CSRC / s for s in SG_SOURCES] + [INCLUDE / "eemd_surrogate.h"]
+    if force or _stale(out, sg_deps):
+        tmp = out.with_suffix(".so.tmp")
+        cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+               "-I", str(INCLUDE), "-o", str(tmp), *[str(CSRC / s) for s in SG_SOURCES]]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+        os.replace(tmp, out)
     for name, extra in (("libeemd_b200.so", []), ("libeemd_b200_checked.so", ["-DEEMD_CHECKED"]),
                         ("libeemd_b200_trace.so", ["-DEEMD_TRACE"])):
         out = LIB / name
