@@ -2,7 +2,7 @@
 from __future__ import annotations
 
 import ctypes
-from ctypes import c_float, c_int32, c_int64, c_void_p
+from ctypes import c_double, c_float, c_int32, c_int64, c_void_p
 from pathlib import Path
 
 LIB_DIR = Path(__file__).resolve().parent / "lib"
@@ -10,8 +10,9 @@ SG_OK = 0
 SG_E_BADARG = -1
 SG_E_TIMEOUT = -4
 SG_E_CUDA = -5
-ABI_VERSION = 1
-EXPORTS = ("eemd_sg_version", "eemd_sg_conv", "eemd_sg_pack", "eemd_sg_wgrad", "eemd_sg_loss", "eemd_sg_adam")
+ABI_VERSION = 2
+EXPORTS = ("eemd_sg_version", "eemd_sg_conv", "eemd_sg_pack", "eemd_sg_wgrad", "eemd_sg_loss", "eemd_sg_adam",
+           "eemd_sg_bias", "eemd_sg_scale", "eemd_sg_prepare", "eemd_sg_combine", "eemd_sg_stat_count")
 
 _lib = None
 
@@ -39,11 +40,20 @@ def load() -> ctypes.CDLL:
         raise RuntimeError("libeemd_surrogate.so ABI version mismatch")
     lib.eemd_sg_conv.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32,
                                  c_int32, c_int32, c_int32, c_void_p, c_int32, c_void_p, c_int64, c_void_p]
-    lib.eemd_sg_pack.argtypes = [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_void_p]
+    lib.eemd_sg_pack.argtypes = [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_int32,
+                                 c_void_p]
+    lib.eemd_sg_bias.argtypes = [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p]
+    lib.eemd_sg_scale.argtypes = [c_void_p, c_void_p, c_int32, c_int32, c_void_p]
+    lib.eemd_sg_prepare.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                    c_int32, c_int32, c_int32, c_int32, c_void_p]
+    lib.eemd_sg_combine.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                    c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_int32, c_double,
+                                    c_double, c_void_p, c_void_p, c_void_p]
+    lib.eemd_sg_stat_count.restype = c_int32
     lib.eemd_sg_wgrad.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32,
                                   c_int32, c_int32, c_int32, c_void_p]
     lib.eemd_sg_loss.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32,
-                                 c_int32, c_int32, c_void_p]
+                                 c_int32, c_int32, c_int32, c_float, c_void_p, c_void_p]
     lib.eemd_sg_adam.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_float, c_float, c_float,
                                  c_float, c_int32, c_void_p]
     for f in EXPORTS[1:]:
@@ -72,8 +82,33 @@ def conv(x, wpk, bias, y, B, T, cin, cout, dil, direction=1, relu=False, mask=No
                                _p(mask), int(tensor_cores), _p(err), spin_limit, _stream()), "eemd_sg_conv")
 
 
-def pack(w, wpk, n_rows, c, nv, cv, transpose=False):
-    _check(load().eemd_sg_pack(_p(w), _p(wpk), n_rows, c, nv, cv, int(transpose), _stream()), "eemd_sg_pack")
+def pack(w, wpk, n_rows, c, nv, cv, transpose=False, project=False):
+    _check(load().eemd_sg_pack(_p(w), _p(wpk), n_rows, c, nv, cv, int(transpose), int(project), _stream()),
+           "eemd_sg_pack")
+
+
+def bias(b, out, n_rows, nv, project=False):
+    _check(load().eemd_sg_bias(_p(b), _p(out), n_rows, nv, int(project), _stream()), "eemd_sg_bias")
+
+
+def scale(x, out, S, N):
+    _check(load().eemd_sg_scale(_p(x), _p(out), S, N, _stream()), "eemd_sg_scale")
+
+
+def prepare(imf_sum, mode_count, x, scl, out, S, N, K, C, imf_sum2=None, mode_count2=None):
+    _check(load().eemd_sg_prepare(_p(imf_sum), _p(mode_count), _p(imf_sum2), _p(mode_count2), _p(x), _p(scl),
+                                  _p(out), S, N, K, C, _stream()), "eemd_sg_prepare")
+
+
+def stat_count() -> int:
+    return int(load().eemd_sg_stat_count())
+
+
+def combine(imf_sum, mode_count, x, scl, net_out, imfs_out, resid_out, partial, chunks, S, N, K, C, P,
+            recon_bound, io_bound, metrics, fallback):
+    _check(load().eemd_sg_combine(_p(imf_sum), _p(mode_count), _p(x), _p(scl), _p(net_out), _p(imfs_out),
+                                  _p(resid_out), _p(partial), chunks, S, N, K, C, P, float(recon_bound),
+                                  float(io_bound), _p(metrics), _p(fallback), _stream()), "eemd_sg_combine")
 
 
 def wgrad(dy, x, dw, db, B, T, n_rows, c, nv, cv, dil):
@@ -81,9 +116,9 @@ def wgrad(dy, x, dw, db, B, T, n_rows, c, nv, cv, dil):
            "eemd_sg_wgrad")
 
 
-def loss(out, base, target, dout, acc, B, T, c, cv, margin):
+def loss(out, base, target, dout, acc, B, T, c, cv, margin, project=False, delta=0.0, weights=None):
     _check(load().eemd_sg_loss(_p(out), _p(base), _p(target), _p(dout), _p(acc), B, T, c, cv, margin,
-                               _stream()), "eemd_sg_loss")
+                               int(project), float(delta), _p(weights), _stream()), "eemd_sg_loss")
 
 
 def adam(p, g, m, v, lr, step, b1=0.9, b2=0.999, eps=1e-8):

@@ -258,18 +258,41 @@ __global__ void k_conv_ref(const __nv_bfloat16* __restrict__ in, const __nv_bflo
     out[i] = __float2bfloat16(x);
 }
 
-// Packs f32 weights w[n][tap][c] (n < nv, c < cv, zero elsewhere) into the
-// bf16 K-major B-tile image of an (N rows) x (3*C) operand.  transpose = 1
-// packs w[c][tap][n] instead (the input-gradient operand).
+// Packs f32 weights into the bf16 K-major B-tile image of an (N rows) x (3*C)
+// operand.  transpose = 0: w is [nv][3][cv] and row n, column tap*C + c holds
+// w[n][tap][c]; transpose = 1: w is [cv][3][nv] and the same position holds
+// w[c][tap][n] (the input-gradient operand).  Zero beyond nv, cv.  project = 1
+// subtracts from every weight the mean over the output channels of the
+// forward layer (n for transpose = 0, c for transpose = 1): the layer's
+// outputs then sum to zero over those channels.
 __global__ void k_pack(const float* __restrict__ w, __nv_bfloat16* wpk, int N, int C, int nv, int cv,
-                       int transpose) {
+                       int transpose, int project) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N * 3 * C) return;
     const int n = i / (3 * C), k = i % (3 * C);
     const int tap = k / C, c = k % C;
+    const int o = transpose ? c : n, ii = transpose ? n : c;      // forward output / input channel
+    const int ov = transpose ? cv : nv, iv = transpose ? nv : cv;
     float x = 0.f;
-    if (n < nv && c < cv) x = transpose ? w[((size_t)c * 3 + tap) * nv + n] : w[((size_t)n * 3 + tap) * cv + c];
+    if (n < nv && c < cv) {
+        x = w[((size_t)o * 3 + tap) * iv + ii];
+        if (project) {
+            float s = 0.f;
+            for (int q = 0; q < ov; ++q) s += w[((size_t)q * 3 + tap) * iv + ii];
+            x -= s / (float)ov;
+        }
+    }
     wpk[kmaj_off(n, k, N)] = __float2bfloat16(x);
+}
+
+// bias[n] = b[n] (n < nv, minus the mean over nv when project), 0 up to N
+__global__ void k_bias(const float* __restrict__ b, float* bias, int N, int nv, int project) {
+    const int n = threadIdx.x;
+    if (n >= N) return;
+    float s = 0.f;
+    if (project)
+        for (int q = 0; q < nv; ++q) s += b[q];
+    bias[n] = n < nv ? b[n] - s / (float)nv : 0.f;
 }
 
 // Weight and bias gradients of y[t][n] = b[n] + sum w[n][tap][c] x[t+(tap-1)d][c]
@@ -326,25 +349,46 @@ __global__ void __launch_bounds__(NT) k_wgrad(const __nv_bfloat16* __restrict__ 
     }
 }
 
-// prediction = base + out (residual form) over the first `cv` of `C` channels;
-// loss partial sums over the interior [margin, T - margin) and the gradient
-// d loss / d out = 2 (pred - target) / count as bf16
+// prediction = base + out (residual form; base may be null) over the first
+// `cv` of `C` channels; loss partial sums over the interior [margin, T - margin)
+// and the gradient d loss / d out as bf16.  The loss per element is d^2 for
+// d = pred - target, or with delta > 0 the Huber loss (d^2 for |d| <= delta,
+// 2 delta |d| - delta^2 beyond), each over the element count and times the
+// channel's weight wch[c] when wch is not null.
+// project = 1 (C = 16) removes the mean over the cv channels from the
+// gradient of every sample: the gradient with respect to the raw output of a
+// layer whose outputs are projected onto zero channel sum.
 __global__ void k_loss(const __nv_bfloat16* __restrict__ out, const __nv_bfloat16* __restrict__ base,
                        const __nv_bfloat16* __restrict__ target, __nv_bfloat16* dout, float* loss, int B, int T,
-                       int C, int cv, int margin, float inv_count) {
+                       int C, int cv, int margin, float inv_count, int project, float delta,
+                       const float* __restrict__ wch) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    float l = 0.f;
-    if (i < (long long)B * T * C) {
-        const int c = (int)(i % C);
+    const bool in_range = i < (long long)B * T * C;
+    float l = 0.f, g = 0.f;
+    int c = 0;
+    if (in_range) {
+        c = (int)(i % C);
         const int t = (int)((i / C) % T);
-        float g = 0.f;
         if (c < cv && t >= margin && t < T - margin) {
-            const float d = __bfloat162float(base[i]) + __bfloat162float(out[i]) - __bfloat162float(target[i]);
-            l = d * d;
-            g = 2.f * d * inv_count;
+            const float d = (base ? __bfloat162float(base[i]) : 0.f) + __bfloat162float(out[i]) -
+                            __bfloat162float(target[i]);
+            const float wc = wch ? wch[c] : 1.f;
+            if (delta > 0.f && fabsf(d) > delta) {
+                l = wc * (2.f * delta * fabsf(d) - delta * delta);
+                g = 2.f * wc * copysignf(delta, d) * inv_count;
+            } else {
+                l = wc * d * d;
+                g = 2.f * wc * d * inv_count;
+            }
         }
-        dout[i] = __float2bfloat16(g);
     }
+    if (project) {
+        // the 16 channels of one sample are 16 consecutive lanes
+        float s = g;
+        for (int o = 8; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, 16);
+        if (c < cv) g -= s / (float)cv;
+    }
+    if (in_range) dout[i] = __float2bfloat16(g);
     // warp sum, one atomic per warp
     for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
     if ((threadIdx.x & 31) == 0 && l != 0.f) atomicAdd(loss, l * inv_count);
@@ -361,6 +405,162 @@ __global__ void k_adam(float* p, const float* g, float* m, float* v, int n, floa
     m[i] = mi;
     v[i] = vi;
     p[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+}
+
+// ---------------------------------------------------------------------------
+// surrogate input and output stages.  A batch holds S signals of N samples;
+// the engine's ensemble sums are imf_sum[s][m][t] (float64) with trial counts
+// count[s][m] for m < K; the network sees K IMF channels and the residual
+// channel (K + 1 <= C), all divided by the signal's RMS.
+// ---------------------------------------------------------------------------
+constexpr int GK = 10;                        // IMF channels of the network
+constexpr int NGRAM = (GK + 1) * (GK + 2) / 2;  // Gram entries over IMFs + residual
+constexpr int NSTAT = 2 + NGRAM;              // sum x^2, sum reconstruction error^2, Gram
+
+// scale[s] = sqrt(mean x[s]^2) (1 for a zero signal); one CTA per signal
+__global__ void __launch_bounds__(256) k_scale(const float* __restrict__ x, float* scale, int N) {
+    __shared__ double part[8];
+    const float* xs = x + (size_t)blockIdx.x * N;
+    double a = 0.0;
+    for (int t = threadIdx.x; t < N; t += 256) a += (double)xs[t] * (double)xs[t];
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < 8; ++w) s += part[w];
+        const double r = sqrt(s / N);
+        scale[blockIdx.x] = r > 0.0 ? (float)r : 1.f;
+    }
+}
+
+// per-mode means and the residual x - sum(means) (the order of the engine's
+// finalisation), divided by scale[s], as bf16 channels [s][t][C].  With
+// imf_sum2 / count2, the difference of the two decompositions (a training
+// target: large-ensemble minus small-ensemble channels), formed in float64.
+__global__ void k_prepare(const double* __restrict__ imf_sum, const int* __restrict__ count,
+                          const double* __restrict__ imf_sum2, const int* __restrict__ count2,
+                          const float* __restrict__ x, const float* __restrict__ scale, __nv_bfloat16* out, int S,
+                          int N, int K, int C) {
+    const long long total = (long long)S * N;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int s = (int)(i / N), t = (int)(i % N);
+        const double inv = 1.0 / (double)scale[s];
+        __align__(16) __nv_bfloat16 h[32];
+        for (int m = 0; m < C; ++m) h[m] = __float2bfloat16(0.f);
+        double acc = 0.0, acc2 = 0.0;
+        for (int m = 0; m < K; ++m) {
+            const size_t e = ((size_t)s * K + m) * N + t;
+            const int cnt = count[(size_t)s * K + m];
+            const double mean = imf_sum[e] / (double)(cnt > 0 ? cnt : 1);
+            acc += mean;
+            double v = mean;
+            if (imf_sum2) {
+                const int cnt2 = count2[(size_t)s * K + m];
+                const double mean2 = imf_sum2[e] / (double)(cnt2 > 0 ? cnt2 : 1);
+                acc2 += mean2;
+                v -= mean2;
+            }
+            h[m] = __float2bfloat16((float)(v * inv));
+        }
+        const double r = (double)x[i] - acc;
+        const double r2 = imf_sum2 ? (double)x[i] - acc2 : 0.0;
+        h[K] = __float2bfloat16((float)((r - r2) * inv));
+        uint4* o = reinterpret_cast<uint4*>(out + (size_t)i * C);
+        for (int q = 0; q < C / 8; ++q) o[q] = reinterpret_cast<const uint4*>(h)[q];
+    }
+}
+
+// served decomposition from the network's corrections of the first P modes:
+// imf[m] = mean_m + scale * net[m] (m < P), imf[m] = mean_m (P <= m < K),
+// resid = (x - sum mean) - scale * sum_{m<P} net[m] (the corrections move
+// content between the modes and the residual, the sum stays x); per-CTA
+// partial sums of x^2, of the reconstruction error (x - sum imf - resid)^2 and
+// of the Gram matrix of (imf_0..imf_{K-1}, resid).  grid (chunks, S), 128
+// threads.
+__global__ void __launch_bounds__(128) k_combine(const double* __restrict__ imf_sum, const int* __restrict__ count,
+                                                 const float* __restrict__ x, const float* __restrict__ scale,
+                                                 const __nv_bfloat16* __restrict__ net, double* imfs_out,
+                                                 double* resid_out, double* partial, int N, int C, int P) {
+    constexpr int K = GK;
+    __shared__ double red[4][NSTAT];
+    const int s = blockIdx.y, chunk = blockIdx.x, chunks = gridDim.x;
+    const int per = (N + chunks - 1) / chunks;
+    const int lo = chunk * per, hi = min(N, lo + per);
+    const double sc = (double)scale[s];
+    double cnt_d[K];
+#pragma unroll
+    for (int m = 0; m < K; ++m) {
+        const int cnt = count[(size_t)s * K + m];
+        cnt_d[m] = (double)(cnt > 0 ? cnt : 1);
+    }
+    double st[NSTAT];
+#pragma unroll
+    for (int j = 0; j < NSTAT; ++j) st[j] = 0.0;
+    for (int t = lo + (int)threadIdx.x; t < hi; t += 128) {
+        const size_t it = (size_t)s * N + t;
+        const __nv_bfloat16* o = net + it * C;
+        double c[K + 1];
+        double acc = 0.0, moved = 0.0, sum_c = 0.0;
+#pragma unroll
+        for (int m = 0; m < K; ++m) {
+            const double mean = imf_sum[((size_t)s * K + m) * N + t] / cnt_d[m];
+            acc += mean;
+            const double d = m < P ? sc * (double)__bfloat162float(o[m]) : 0.0;
+            moved += d;
+            c[m] = mean + d;
+            imfs_out[((size_t)s * K + m) * N + t] = c[m];
+            sum_c += c[m];
+        }
+        const double xv = (double)x[it];
+        c[K] = (xv - acc) - moved;
+        resid_out[it] = c[K];
+        const double e = xv - (sum_c + c[K]);
+        st[0] += xv * xv;
+        st[1] += e * e;
+        int q = 2;
+#pragma unroll
+        for (int a = 0; a <= K; ++a)
+#pragma unroll
+            for (int b = a; b <= K; ++b) st[q++] += c[a] * c[b];
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int j = 0; j < NSTAT; ++j) {
+        double v = st[j];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp][j] = v;
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < NSTAT; j += 128)
+        partial[((size_t)s * chunks + chunk) * NSTAT + j] = ((red[0][j] + red[1][j]) + red[2][j]) + red[3][j];
+}
+
+// per signal: the chunk partials added in chunk order; metrics[s] = {relative
+// reconstruction error, orthogonality index}; fallback[s] = 1 when the error
+// or the magnitude of the index exceeds its bound (or either is not finite).  The orthogonality index is Huang et
+// al. (1998): sum over pairs j != k of <c_j, c_k> over ||x||^2, the residual
+// counted as the last component.
+__global__ void k_gate(const double* __restrict__ partial, int S, int chunks, double recon_bound, double io_bound,
+                       double* metrics, int* fallback) {
+    constexpr int K = GK;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    double tot[NSTAT];
+    for (int j = 0; j < NSTAT; ++j) tot[j] = 0.0;
+    for (int ch = 0; ch < chunks; ++ch)
+        for (int j = 0; j < NSTAT; ++j) tot[j] += partial[((size_t)s * chunks + ch) * NSTAT + j];
+    double cross = 0.0;
+    int q = 2;
+    for (int a = 0; a <= K; ++a)
+        for (int b = a; b <= K; ++b, ++q)
+            if (b != a) cross += tot[q];
+    const double xx = tot[0] > 0.0 ? tot[0] : 1.0;
+    const double recon = sqrt(tot[1] / xx), io = 2.0 * cross / xx;
+    metrics[2 * s] = recon;
+    metrics[2 * s + 1] = io;
+    fallback[s] = !(recon <= recon_bound) || !(fabs(io) <= io_bound) ? 1 : 0;
 }
 
 }  // namespace sg
@@ -413,11 +613,11 @@ int32_t eemd_sg_conv(const void* in, const void* wpk, const float* bias, void* o
 }
 
 int32_t eemd_sg_pack(const float* w, void* wpk, int32_t n_rows, int32_t c, int32_t nv, int32_t cv,
-                     int32_t transpose, void* stream) {
+                     int32_t transpose, int32_t project, void* stream) {
     if (!w || !wpk || n_rows % 16 || c % 16 || nv > n_rows || cv > c) return EEMD_SG_E_BADARG;
     const int n = n_rows * 3 * c;
     k_pack<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(w, static_cast<__nv_bfloat16*>(wpk),
-                                                                           n_rows, c, nv, cv, transpose);
+                                                                           n_rows, c, nv, cv, transpose, project);
     return cudaGetLastError() == cudaSuccess ? EEMD_SG_OK : EEMD_SG_E_CUDA;
 }
 
@@ -432,14 +632,16 @@ int32_t eemd_sg_wgrad(const void* dy, const void* x, float* dw, float* db, int32
 }
 
 int32_t eemd_sg_loss(const void* out, const void* base, const void* target, void* dout, float* loss, int32_t B,
-                     int32_t T, int32_t c, int32_t cv, int32_t margin, void* stream) {
-    if (!out || !base || !target || !dout || !loss || 2 * margin >= T) return EEMD_SG_E_BADARG;
+                     int32_t T, int32_t c, int32_t cv, int32_t margin, int32_t project, float delta,
+                     const float* channel_weight, void* stream) {
+    if (!out || !target || !dout || !loss || 2 * margin >= T || cv < 1 || cv > c || (project && c != 16))
+        return EEMD_SG_E_BADARG;
     const long long n = (long long)B * T * c;
     const float inv = 1.f / (float)((long long)B * (T - 2 * margin) * cv);
     k_loss<<<(unsigned)((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         static_cast<const __nv_bfloat16*>(out), static_cast<const __nv_bfloat16*>(base),
         static_cast<const __nv_bfloat16*>(target), static_cast<__nv_bfloat16*>(dout), loss, B, T, c, cv, margin,
-        inv);
+        inv, project, delta, channel_weight);
     return cudaGetLastError() == cudaSuccess ? EEMD_SG_OK : EEMD_SG_E_CUDA;
 }
 
@@ -451,5 +653,48 @@ int32_t eemd_sg_adam(float* p, const float* g, float* m, float* v, int32_t n, fl
                                                                           bc2);
     return cudaGetLastError() == cudaSuccess ? EEMD_SG_OK : EEMD_SG_E_CUDA;
 }
+
+int32_t eemd_sg_bias(const float* b, float* bias, int32_t n_rows, int32_t nv, int32_t project, void* stream) {
+    if (!b || !bias || n_rows < 1 || n_rows > 1024 || nv < 1 || nv > n_rows) return EEMD_SG_E_BADARG;
+    k_bias<<<1, n_rows, 0, static_cast<cudaStream_t>(stream)>>>(b, bias, n_rows, nv, project);
+    return cudaGetLastError() == cudaSuccess ? EEMD_SG_OK : EEMD_SG_E_CUDA;
+}
+
+int32_t eemd_sg_scale(const float* x, float* scale, int32_t S, int32_t N, void* stream) {
+    if (!x || !scale || S < 1 || N < 1) return EEMD_SG_E_BADARG;
+    k_scale<<<S, 256, 0, static_cast<cudaStream_t>(stream)>>>(x, scale, N);
+    return cudaGetLastError() == cudaSuccess ? EEMD_SG_OK : EEMD_SG_E_CUDA;
+}
+
+int32_t eemd_sg_prepare(const double* imf_sum, const int32_t* mode_count, const double* imf_sum2,
+                        const int32_t* mode_count2, const float* x, const float* scale, void* out, int32_t S,
+                        int32_t N, int32_t K, int32_t C, void* stream) {
+    if (!imf_sum || !mode_count || !x || !scale || !out || S < 1 || N < 1 || K < 1 || C % 8 || C > 32 ||
+        K + 1 > C || (imf_sum2 && !mode_count2))
+        return EEMD_SG_E_BADARG;
+    const long long total = (long long)S * N;
+    const long long blocks = (total + 255) / 256;
+    k_prepare<<<(unsigned)(blocks < 148 * 16 ? blocks : 148 * 16), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        imf_sum, mode_count, imf_sum2, mode_count2, x, scale, static_cast<__nv_bfloat16*>(out), S, N, K, C);
+    return cudaGetLastError() == cudaSuccess ? EEMD_SG_OK : EEMD_SG_E_CUDA;
+}
+
+int32_t eemd_sg_combine(const double* imf_sum, const int32_t* mode_count, const float* x, const float* scale,
+                        const void* net_out, double* imfs_out, double* resid_out, double* partial, int32_t chunks,
+                        int32_t S, int32_t N, int32_t K, int32_t C, int32_t P, double recon_bound,
+                        double io_bound, double* metrics, int32_t* fallback, void* stream) {
+    if (!imf_sum || !mode_count || !x || !scale || !net_out || !imfs_out || !resid_out || !partial || !metrics ||
+        !fallback || S < 1 || N < 1 || K != GK || C % 8 || C > 32 || P < 0 || P > K || P > C || chunks < 1 ||
+        chunks > 65535)
+        return EEMD_SG_E_BADARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    k_combine<<<dim3(chunks, S), 128, 0, st>>>(imf_sum, mode_count, x, scale,
+                                                static_cast<const __nv_bfloat16*>(net_out), imfs_out, resid_out,
+                                                partial, N, C, P);
+    k_gate<<<(S + 127) / 128, 128, 0, st>>>(partial, S, chunks, recon_bound, io_bound, metrics, fallback);
+    return cudaGetLastError() == cudaSuccess ? EEMD_SG_OK : EEMD_SG_E_CUDA;
+}
+
+int32_t eemd_sg_stat_count(void) { return NSTAT; }
 
 }  // extern "C"
