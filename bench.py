@@ -585,16 +585,223 @@ def run_ours(args, wl: Workload):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# the learned surrogate (8-trial ensemble + network in place of 256 trials)
+# ---------------------------------------------------------------------------
+SURROGATE_WEIGHTS = ROOT / "eemd4cuda_b200" / "weights" / "surrogate_n65536.npy"
+SG_SIGNALS = 128
+
+
+def measured_peak_bf16():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["bf16_tflops"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return 1590.0, "fallback"
+
+
+def _surrogate_signal():
+    from eemd4cuda_b200 import surrogate as SU
+    return SU.make_signals([30000], 65536)
+
+
+def surrogate_cpu_workload() -> Workload:
+    """The plain 256-trial EEMD the surrogate stands in for, as a CPU sample:
+    tasks of one held-out 65536-sample signal, the first 2 of 10 IMFs (10
+    sifts each), scaled to 100 sifts per task."""
+    return Workload("surrogate65k",
+                    {"workload": "plain_256_trial_eemd_65536", "N": 65536, "trials": 256, "eps": 0.2,
+                     "max_imf": 10, "sifts_per_imf": 10, "storage": "float32", "solve": "float64"},
+                    E=256, eps=0.2, max_imf=10, max_sifts=10, tau=0.0, dtype="f32", seed=30000,
+                    cpu_tasks=16, cpu_max_imf=2, signals_fn=_surrogate_signal)
+
+
+def L_times():
+    from eemd4cuda_b200 import _lib as L
+    return L.KernelTimes()
+
+
+def run_surrogate(args):
+    """One step: the surrogate decomposition of SG_SIGNALS held-out signals of
+    65536 samples (8-trial ensemble, network, served modes and gate).  value
+    counts the 256 trials the step stands in for."""
+    import torch
+
+    rank, local_rank, world = rank_env()
+    if world > 1 and rank != 0:
+        return 0
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    from eemd4cuda_b200 import surrogate as SU
+
+    N, S, E_small, E_big = 65536, SG_SIGNALS, 8, 256
+    cb = CpuBaseline(surrogate_cpu_workload()) if world == 1 else None
+
+    net = SU.Net(seed=0)
+    if SURROGATE_WEIGHTS.exists():
+        net.load_state(np.load(SURROGATE_WEIGHTS))
+        weights = f"{SURROGATE_WEIGHTS.relative_to(ROOT)}"
+    else:
+        inp, tgt = SU.generate_pairs(range(10000, 10256), N, E_small, E_big)
+        SU.train(net, inp, tgt, steps=3000)
+        del inp, tgt
+        weights = "trained in this run (256 signals, 3000 steps)"
+    xs = SU.make_signals(range(30000, 30000 + S), N)
+    sur = SU.SurrogateEEMD(net, S, N, E_small, E_big, SU.engine_params())
+    sur.xd.copy_(torch.from_numpy(np.concatenate(xs)))
+    flush = torch.empty((2 * L2_BYTES,), dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        sur.run(S)
+    torch.cuda.synchronize()
+    net.check()
+
+    clk = ClockSampler(local_rank)
+    clk.start()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sur.run(S)
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+    clocks = clk.stop()
+    ms = total_ms / args.steps
+    value = S * N * E_big / (ms / 1e3) / 1e6
+
+    # split: the small ensemble, the network, the stages
+    flush.fill_(1)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    sur.imf_sum.zero_()
+    sur.mode_count.zero_()
+    kt = L_times()
+    ev[0].record(stream)
+    sur.ens.sums(sur.xd, S, 0, E_small, sur.imf_sum, sur.mode_count, times=kt)
+    ev[1].record(stream)
+    from eemd4cuda_b200 import _sg as SG
+    SG.scale(sur.xd, sur.scale, S, N)
+    SG.prepare(sur.imf_sum, sur.mode_count, sur.xd, sur.scale, sur.inp, S, N, sur.K, SU.CH)
+    ev[2].record(stream)
+    net.infer(sur.inp, sur.out, S, N, sur.chunk, sur.bufs)
+    ev[3].record(stream)
+    ev[3].synchronize()
+    ens_ms, stage_ms, net_ms = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2]), ev[2].elapsed_time(ev[3])
+    launches = sum(v["launches"] for v in kt.as_dict().values()) + sur.launches_per_run(S)
+    flops = SU.network_flops_per_sample() * S * N
+    n_conv = len(SU.DILATIONS) * ((S + sur.chunk - 1) // sur.chunk)
+    tflops = flops / (net_ms / 1e3) / 1e12
+    peak, peak_kind = measured_peak_bf16()
+
+    # the plain 256-trial EEMD of the same signals, and the errors against it
+    g = 16
+    ens_plain = SU.Ensembles(g, N, E_big)
+    K = sur.K
+    ps = torch.empty((g * K * N,), dtype=torch.float64, device=dev)
+    pc = torch.empty((g * K,), dtype=torch.int32, device=dev)
+    pm = torch.empty((g * K * N,), dtype=torch.float64, device=dev)
+    pr = torch.empty((g * N,), dtype=torch.float64, device=dev)
+    pn = torch.empty((g,), dtype=torch.int32, device=dev)
+    ens_plain.plain(sur.xd[:g * N], g, E_small, ps, pc, pm, pr, pn)  # warm-up
+    sur.run(S)
+    torch.cuda.synchronize()
+    imfs = sur.imfs.cpu().numpy()
+    met = sur.metrics.cpu().numpy()
+    fb = sur.fallback.cpu().numpy().astype(bool)
+    cnt = np.maximum(sur.mode_count.cpu().numpy().reshape(S, K), 1)
+    m8 = sur.imf_sum.cpu().numpy().reshape(S, K, N) / cnt[:, :, None]
+    plain_ms = 0.0
+    e8, es = [], []
+    for q0 in range(0, S, g):
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ens_plain.plain(sur.xd[q0 * N:(q0 + g) * N], g, E_big, ps, pc, pm, pr, pn)
+        e1.record(stream)
+        e1.synchronize()
+        plain_ms += e0.elapsed_time(e1)
+        big = pm.cpu().numpy().reshape(g, K, N)
+        for j in range(g):
+            i = q0 + j
+            e8.append([SU.rel_l2(m8[i][k], big[j][k]) for k in range(K)])
+            es.append([SU.rel_l2(imfs[i][k], big[j][k]) for k in range(K)])
+    e8, es = np.median(np.array(e8), axis=0), np.median(np.array(es), axis=0)
+
+    # end to end through the public call: host signals in, served modes out
+    # (fallback signals included)
+    served = sur.decompose(xs)
+    torch.cuda.synchronize()
+    e2e_ms = []
+    for _ in range(max(1, min(args.steps, 2))):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        served = sur.decompose(xs)
+        torch.cuda.synchronize()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e = statistics.median(e2e_ms)
+    nf = sum(st["fallback"] for _, _, st in served)
+
+    cpu = None
+    if cb is not None:
+        cb.step()
+        cpu = cb.describe(cb.value(cb.step(), 100.0))  # 10 IMFs x 10 sifts per task
+        cpu["sample"] += "; 256-trial EEMD units (the surrogate's output stands in for them)"
+        cb.close()
+
+    line = {
+        "metric": "surrogate EEMD Msamples*trials/s (256-trial equivalent)", "value": round(value, 3),
+        "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32+f64",
+        "data": "synthetic",
+        "config": {"workload": "surrogate_8_to_256_trials", "N": N, "signals": S, "trials_small": E_small,
+                   "trials_equivalent": E_big, "max_imf": 10, "sifts_per_imf": 10, "corrected_modes": SU.P_CORR,
+                   "network": "dilated conv 8 layers x 64 ch, k=3, d=1..128, bf16 / f32 accumulate",
+                   "weights": weights, "signals_seeds": "30000..30127 (held out)",
+                   "l2": "flushed between timed steps (256 MiB write)"},
+        "speedup_vs_plain_256": round(plain_ms / ms, 2), "plain_256_ms": round(plain_ms, 3),
+        "split_ms": {"ensemble_8": round(ens_ms, 3), "prepare": round(stage_ms, 3), "network": round(net_ms, 3)},
+        "median_rel_l2_per_imf": {"surrogate": [round(float(v), 4) for v in es],
+                                  "ensemble_8": [round(float(v), 4) for v in e8]},
+        "gate": {"recon_bound": SU.RECON_BOUND, "io_bound": SU.IO_BOUND, "io_form": "relative to the 8-trial modes",
+                 "fallbacks": int(fb.sum()), "fallbacks_absolute_io": int((np.abs(met[:, 1]) > SU.IO_BOUND).sum()),
+                 "max_recon": float(met[:, 0].max()), "median_abs_io": float(np.median(np.abs(met[:, 1]))),
+                 "median_abs_io_8": float(np.median(np.abs(met[:, 3]))),
+                 "median_abs_io_all": float(np.median(np.abs(met[:, 2])))},
+        "e2e": {"value": round(S * N * E_big / (e2e / 1e3) / 1e6, 3), "unit": UNIT, "ms_per_step": round(e2e, 3),
+                "h2d_bytes_per_step": S * N * 4, "d2h_bytes_per_step": S * (K + 1) * N * 8 + S * 3 * 8 + S * 4,
+                "fallbacks": nf},
+        "gpu_launches": launches * args.steps,
+        "roofline": {"bound": "tensor", "kernel": "k_conv_tc", "achieved": round(tflops, 2), "peak": peak,
+                     "peak_kind": peak_kind, "unit": "TFLOP/s", "frac": round(tflops * 1e12 / (peak * 1e12), 4),
+                     "traffic": None, "algorithmic_flops_per_launch": round(flops / n_conv),
+                     "avg_launch_ms": round(net_ms / n_conv, 5)},
+        "clocks": clocks,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="harmonic48k")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["surrogate"], default="harmonic48k")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload == "surrogate":
+        if args.impl == "reference":
+            return run_reference(args, surrogate_cpu_workload())
+        return run_surrogate(args)
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         return run_reference(args, wl)

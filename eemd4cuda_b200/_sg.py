@@ -48,14 +48,14 @@ def load() -> ctypes.CDLL:
                                     c_int32, c_int32, c_int32, c_int32, c_void_p]
     lib.eemd_sg_combine.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                     c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_int32, c_double,
-                                    c_double, c_void_p, c_void_p, c_void_p]
+                                    c_double, c_int32, c_void_p, c_void_p, c_void_p]
     lib.eemd_sg_stat_count.restype = c_int32
     lib.eemd_sg_wgrad.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32,
                                   c_int32, c_int32, c_int32, c_void_p]
     lib.eemd_sg_loss.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32,
                                  c_int32, c_int32, c_int32, c_float, c_void_p, c_void_p]
     lib.eemd_sg_adam.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_float, c_float, c_float,
-                                 c_float, c_int32, c_void_p]
+                                 c_float, c_int32, c_float, c_void_p, c_void_p]
     for f in EXPORTS[1:]:
         getattr(lib, f).restype = c_int32
     _lib = lib
@@ -105,10 +105,11 @@ def stat_count() -> int:
 
 
 def combine(imf_sum, mode_count, x, scl, net_out, imfs_out, resid_out, partial, chunks, S, N, K, C, P,
-            recon_bound, io_bound, metrics, fallback):
+            recon_bound, io_bound, metrics, fallback, io_relative=True):
     _check(load().eemd_sg_combine(_p(imf_sum), _p(mode_count), _p(x), _p(scl), _p(net_out), _p(imfs_out),
                                   _p(resid_out), _p(partial), chunks, S, N, K, C, P, float(recon_bound),
-                                  float(io_bound), _p(metrics), _p(fallback), _stream()), "eemd_sg_combine")
+                                  float(io_bound), int(io_relative), _p(metrics), _p(fallback), _stream()),
+           "eemd_sg_combine")
 
 
 def wgrad(dy, x, dw, db, B, T, n_rows, c, nv, cv, dil):
@@ -121,6 +122,6 @@ def loss(out, base, target, dout, acc, B, T, c, cv, margin, project=False, delta
                                int(project), float(delta), _p(weights), _stream()), "eemd_sg_loss")
 
 
-def adam(p, g, m, v, lr, step, b1=0.9, b2=0.999, eps=1e-8):
-    _check(load().eemd_sg_adam(_p(p), _p(g), _p(m), _p(v), p.numel(), lr, b1, b2, eps, step, _stream()),
-           "eemd_sg_adam")
+def adam(p, g, m, v, lr, step, b1=0.9, b2=0.999, eps=1e-8, max_norm=0.0, work=None):
+    _check(load().eemd_sg_adam(_p(p), _p(g), _p(m), _p(v), p.numel(), lr, b1, b2, eps, step, float(max_norm),
+                               _p(work), _stream()), "eemd_sg_adam")

@@ -395,16 +395,39 @@ __global__ void k_loss(const __nv_bfloat16* __restrict__ out, const __nv_bfloat1
 }
 
 // Adam (Kingma & Ba 2015) on f32 parameters
+// (with gnorm2, the gradient is scaled to norm at most max_norm; a step
+// whose gradient norm is not finite is skipped)
 __global__ void k_adam(float* p, const float* g, float* m, float* v, int n, float lr, float b1, float b2, float eps,
-                       float bc1, float bc2) {
+                       float bc1, float bc2, const float* gnorm2, float max_norm) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float gi = g[i];
+    float sc = 1.f;
+    if (gnorm2) {
+        const float nrm = sqrtf(*gnorm2);
+        if (!isfinite(nrm)) return;
+        if (nrm > max_norm) sc = max_norm / nrm;
+    }
+    const float gi = g[i] * sc;
     const float mi = b1 * m[i] + (1.f - b1) * gi;
     const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
     m[i] = mi;
     v[i] = vi;
     p[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+}
+
+// out[0] = sum of g[i]^2 (one CTA, fixed order)
+__global__ void __launch_bounds__(1024) k_sumsq(const float* __restrict__ g, int n, float* out) {
+    __shared__ float part[32];
+    float a = 0.f;
+    for (int i = threadIdx.x; i < n; i += 1024) a = fmaf(g[i], g[i], a);
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float s = 0.f;
+        for (int w = 0; w < 32; ++w) s += part[w];
+        out[0] = s;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -414,8 +437,10 @@ __global__ void k_adam(float* p, const float* g, float* m, float* v, int n, floa
 // channel (K + 1 <= C), all divided by the signal's RMS.
 // ---------------------------------------------------------------------------
 constexpr int GK = 10;                        // IMF channels of the network
+constexpr int PMAX = 6;                       // corrected modes at most
 constexpr int NGRAM = (GK + 1) * (GK + 2) / 2;  // Gram entries over IMFs + residual
-constexpr int NSTAT = 2 + NGRAM;              // sum x^2, sum reconstruction error^2, Gram
+constexpr int NREF = PMAX * (PMAX - 1) / 2;   // cross terms of the small-ensemble modes < PMAX
+constexpr int NSTAT = 2 + NGRAM + NREF;       // sum x^2, sum reconstruction error^2, Gram, reference cross terms
 
 // scale[s] = sqrt(mean x[s]^2) (1 for a zero signal); one CTA per signal
 __global__ void __launch_bounds__(256) k_scale(const float* __restrict__ x, float* scale, int N) {
@@ -501,11 +526,12 @@ __global__ void __launch_bounds__(128) k_combine(const double* __restrict__ imf_
     for (int t = lo + (int)threadIdx.x; t < hi; t += 128) {
         const size_t it = (size_t)s * N + t;
         const __nv_bfloat16* o = net + it * C;
-        double c[K + 1];
+        double c[K + 1], mr[PMAX];
         double acc = 0.0, moved = 0.0, sum_c = 0.0;
 #pragma unroll
         for (int m = 0; m < K; ++m) {
             const double mean = imf_sum[((size_t)s * K + m) * N + t] / cnt_d[m];
+            if (m < PMAX) mr[m] = mean;
             acc += mean;
             const double d = m < P ? sc * (double)__bfloat162float(o[m]) : 0.0;
             moved += d;
@@ -524,6 +550,10 @@ __global__ void __launch_bounds__(128) k_combine(const double* __restrict__ imf_
         for (int a = 0; a <= K; ++a)
 #pragma unroll
             for (int b = a; b <= K; ++b) st[q++] += c[a] * c[b];
+#pragma unroll
+        for (int a = 0; a < PMAX; ++a)
+#pragma unroll
+            for (int b = a + 1; b < PMAX; ++b) st[q++] += mr[a] * mr[b];
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
@@ -537,13 +567,17 @@ __global__ void __launch_bounds__(128) k_combine(const double* __restrict__ imf_
         partial[((size_t)s * chunks + chunk) * NSTAT + j] = ((red[0][j] + red[1][j]) + red[2][j]) + red[3][j];
 }
 
-// per signal: the chunk partials added in chunk order; metrics[s] = {relative
-// reconstruction error, orthogonality index}; fallback[s] = 1 when the error
-// or the magnitude of the index exceeds its bound (or either is not finite).  The orthogonality index is Huang et
-// al. (1998): sum over pairs j != k of <c_j, c_k> over ||x||^2, the residual
-// counted as the last component.
-__global__ void k_gate(const double* __restrict__ partial, int S, int chunks, double recon_bound, double io_bound,
-                       double* metrics, int* fallback) {
+// per signal: the chunk partials added in chunk order; metrics[s] =
+// {relative reconstruction error, orthogonality index of the P modes the
+// network corrects, orthogonality index of all IMFs and the residual,
+// orthogonality index of the same P modes of the small-ensemble means};
+// fallback[s] = 1 when the error exceeds recon_bound or the corrected modes'
+// index exceeds io_bound: in magnitude, or with io_relative by its magnitude
+// less that of the small-ensemble modes (or any of these is not finite).
+// Orthogonality index (Huang et al. 1998): sum over pairs j != k of
+// <c_j, c_k> over ||x||^2.
+__global__ void k_gate(const double* __restrict__ partial, int S, int chunks, int P, double recon_bound,
+                       double io_bound, int io_relative, double* metrics, int* fallback) {
     constexpr int K = GK;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S) return;
@@ -551,16 +585,26 @@ __global__ void k_gate(const double* __restrict__ partial, int S, int chunks, do
     for (int j = 0; j < NSTAT; ++j) tot[j] = 0.0;
     for (int ch = 0; ch < chunks; ++ch)
         for (int j = 0; j < NSTAT; ++j) tot[j] += partial[((size_t)s * chunks + ch) * NSTAT + j];
-    double cross = 0.0;
+    double cross = 0.0, cross_p = 0.0, cross_ref = 0.0;
     int q = 2;
     for (int a = 0; a <= K; ++a)
         for (int b = a; b <= K; ++b, ++q)
-            if (b != a) cross += tot[q];
+            if (b != a) {
+                cross += tot[q];
+                if (b < P) cross_p += tot[q];
+            }
+    for (int a = 0; a < PMAX; ++a)
+        for (int b = a + 1; b < PMAX; ++b, ++q)
+            if (b < P) cross_ref += tot[q];
     const double xx = tot[0] > 0.0 ? tot[0] : 1.0;
-    const double recon = sqrt(tot[1] / xx), io = 2.0 * cross / xx;
-    metrics[2 * s] = recon;
-    metrics[2 * s + 1] = io;
-    fallback[s] = !(recon <= recon_bound) || !(fabs(io) <= io_bound) ? 1 : 0;
+    const double recon = sqrt(tot[1] / xx), io_p = 2.0 * cross_p / xx, io = 2.0 * cross / xx,
+                 io_ref = 2.0 * cross_ref / xx;
+    metrics[4 * s] = recon;
+    metrics[4 * s + 1] = io_p;
+    metrics[4 * s + 2] = io;
+    metrics[4 * s + 3] = io_ref;
+    const double check = io_relative ? fabs(io_p) - fabs(io_ref) : fabs(io_p);
+    fallback[s] = !(recon <= recon_bound) || !(check <= io_bound) ? 1 : 0;
 }
 
 }  // namespace sg
@@ -646,11 +690,13 @@ int32_t eemd_sg_loss(const void* out, const void* base, const void* target, void
 }
 
 int32_t eemd_sg_adam(float* p, const float* g, float* m, float* v, int32_t n, float lr, float b1, float b2,
-                     float eps, int32_t step, void* stream) {
-    if (!p || !g || !m || !v || n < 0 || step < 1) return EEMD_SG_E_BADARG;
+                     float eps, int32_t step, float max_norm, float* work, void* stream) {
+    if (!p || !g || !m || !v || n < 0 || step < 1 || (max_norm > 0.f && !work)) return EEMD_SG_E_BADARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
     const float bc1 = 1.f - powf(b1, (float)step), bc2 = 1.f - powf(b2, (float)step);
-    k_adam<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(p, g, m, v, n, lr, b1, b2, eps, bc1,
-                                                                          bc2);
+    if (max_norm > 0.f) k_sumsq<<<1, 1024, 0, st>>>(g, n, work);
+    k_adam<<<(n + 255) / 256, 256, 0, st>>>(p, g, m, v, n, lr, b1, b2, eps, bc1, bc2,
+                                            max_norm > 0.f ? work : nullptr, max_norm);
     return cudaGetLastError() == cudaSuccess ? EEMD_SG_OK : EEMD_SG_E_CUDA;
 }
 
@@ -682,16 +728,18 @@ int32_t eemd_sg_prepare(const double* imf_sum, const int32_t* mode_count, const 
 int32_t eemd_sg_combine(const double* imf_sum, const int32_t* mode_count, const float* x, const float* scale,
                         const void* net_out, double* imfs_out, double* resid_out, double* partial, int32_t chunks,
                         int32_t S, int32_t N, int32_t K, int32_t C, int32_t P, double recon_bound,
-                        double io_bound, double* metrics, int32_t* fallback, void* stream) {
+                        double io_bound, int32_t io_relative, double* metrics, int32_t* fallback,
+                        void* stream) {
     if (!imf_sum || !mode_count || !x || !scale || !net_out || !imfs_out || !resid_out || !partial || !metrics ||
-        !fallback || S < 1 || N < 1 || K != GK || C % 8 || C > 32 || P < 0 || P > K || P > C || chunks < 1 ||
+        !fallback || S < 1 || N < 1 || K != GK || C % 8 || C > 32 || P < 0 || P > PMAX || P > C || chunks < 1 ||
         chunks > 65535)
         return EEMD_SG_E_BADARG;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     k_combine<<<dim3(chunks, S), 128, 0, st>>>(imf_sum, mode_count, x, scale,
                                                 static_cast<const __nv_bfloat16*>(net_out), imfs_out, resid_out,
                                                 partial, N, C, P);
-    k_gate<<<(S + 127) / 128, 128, 0, st>>>(partial, S, chunks, recon_bound, io_bound, metrics, fallback);
+    k_gate<<<(S + 127) / 128, 128, 0, st>>>(partial, S, chunks, P, recon_bound, io_bound, io_relative, metrics,
+                                            fallback);
     return cudaGetLastError() == cudaSuccess ? EEMD_SG_OK : EEMD_SG_E_CUDA;
 }
 

@@ -72,9 +72,12 @@ int32_t eemd_sg_loss(const void* out, const void* base, const void* target, void
                      int32_t T, int32_t c, int32_t cv, int32_t margin, int32_t project, float delta,
                      const float* channel_weight, void* stream);
 
-/* One Adam step (bias-corrected, step >= 1) on n f32 parameters. */
+/* One Adam step (bias-corrected, step >= 1) on n f32 parameters.  With
+ * max_norm > 0 the gradient is first scaled to a Euclidean norm of at most
+ * max_norm (work: one device float of scratch), and a step whose gradient
+ * norm is not finite leaves p, m and v unchanged. */
 int32_t eemd_sg_adam(float* p, const float* g, float* m, float* v, int32_t n, float lr, float b1, float b2,
-                     float eps, int32_t step, void* stream);
+                     float eps, int32_t step, float max_norm, float* work, void* stream);
 
 /* Surrogate input and output stages over a batch of S signals of N samples
  * x[s][t] (float32).  imf_sum [S][K][N] float64 and mode_count [S][K] int32
@@ -89,16 +92,20 @@ int32_t eemd_sg_adam(float* p, const float* g, float* m, float* v, int32_t n, fl
  *   float64 before the rounding (the training target: large-ensemble minus
  *   small-ensemble channels).
  * eemd_sg_combine: the served decomposition from the network output
- *   net_out[s][t][C], the corrections of the first P modes (P <= K):
+ *   net_out[s][t][C], the corrections of the first P modes (P <= 6):
  *   imfs_out[s][m][t] = mean_m + scale * net_out[.., m] for m < P and mean_m
  *   beyond, resid_out[s][t] = x - sum(mean) - scale * sum_{m<P} net_out[.., m]
  *   (float64; the IMFs and the residual still sum to x), then the gate:
- *   metrics[s] = {||x - sum(imfs) - resid|| / ||x||, orthogonality index
- *   (Huang et al. 1998: sum of <c_j, c_k> over pairs j != k of the IMFs and
- *   the residual, over ||x||^2)}, fallback[s] = 1 when the first exceeds
- *   recon_bound or the magnitude of the second io_bound (or either is not
- *   finite).  partial is device scratch of S * chunks * eemd_sg_stat_count()
- *   doubles; the chunk sums are added in a fixed order.  K must be 10. */
+ *   metrics[s][4] = {||x - sum(imfs) - resid|| / ||x||, orthogonality index
+ *   of the P corrected modes, orthogonality index of all K IMFs and the
+ *   residual, orthogonality index of the first P small-ensemble means}
+ *   (Huang et al. 1998: sum of <c_j, c_k> over pairs j != k of the
+ *   components, over ||x||^2); fallback[s] = 1 when the first exceeds
+ *   recon_bound or the second exceeds io_bound in magnitude (io_relative = 0)
+ *   or in magnitude less the magnitude of the fourth (io_relative = 1), or
+ *   any of these is not finite.  partial is device scratch of
+ *   S * chunks * eemd_sg_stat_count() doubles; the chunk sums are added in a
+ *   fixed order.  K must be 10. */
 int32_t eemd_sg_scale(const float* x, float* scale, int32_t S, int32_t N, void* stream);
 int32_t eemd_sg_prepare(const double* imf_sum, const int32_t* mode_count, const double* imf_sum2,
                         const int32_t* mode_count2, const float* x, const float* scale, void* out, int32_t S,
@@ -106,7 +113,8 @@ int32_t eemd_sg_prepare(const double* imf_sum, const int32_t* mode_count, const 
 int32_t eemd_sg_combine(const double* imf_sum, const int32_t* mode_count, const float* x, const float* scale,
                         const void* net_out, double* imfs_out, double* resid_out, double* partial, int32_t chunks,
                         int32_t S, int32_t N, int32_t K, int32_t C, int32_t P, double recon_bound,
-                        double io_bound, double* metrics, int32_t* fallback, void* stream);
+                        double io_bound, int32_t io_relative, double* metrics, int32_t* fallback,
+                        void* stream);
 int32_t eemd_sg_stat_count(void);
 
 #ifdef __cplusplus

@@ -85,7 +85,15 @@ def mse_residual(out, base, target, cv, margin, project=False, delta=0.0, weight
     return float(np.sum(el * mask) / count), g
 
 
-def adam(p, g, m, v, lr, step, b1=0.9, b2=0.999, eps=1e-8):
+def adam(p, g, m, v, lr, step, b1=0.9, b2=0.999, eps=1e-8, max_norm=0.0):
+    """Adam; max_norm > 0 first scales g to that Euclidean norm at most (a
+    non-finite norm skips the step)."""
+    if max_norm > 0:
+        nrm = float(np.sqrt(np.sum(np.asarray(g, np.float64) ** 2)))
+        if not np.isfinite(nrm):
+            return p, m, v
+        if nrm > max_norm:
+            g = g * (max_norm / nrm)
     m = b1 * m + (1 - b1) * g
     v = b2 * v + (1 - b2) * g * g
     p = p - lr * (m / (1 - b1 ** step)) / (np.sqrt(v / (1 - b2 ** step)) + eps)
@@ -127,7 +135,9 @@ def orthogonality_index(components, x):
 def combine(imf_sum, count, x, scale, net, P):
     """Served IMFs [S][K][N] and residual [S][N] from the network output
     net [S][N][C] (corrections of the first P modes, their sum taken from the
-    residual), with per-signal reconstruction error and orthogonality index."""
+    residual), with per-signal reconstruction error and orthogonality indices
+    of the P corrected modes, of all IMFs and the residual, and of the first P
+    small-ensemble means."""
     means, resid = means_and_residual(imf_sum, count, x)
     S, K, N = means.shape
     d = np.zeros((S, K, N))
@@ -140,5 +150,7 @@ def combine(imf_sum, count, x, scale, net, P):
     x = np.asarray(x, np.float64)
     recon = np.array([np.linalg.norm(x[s] - imfs[s].sum(axis=0) - res[s]) / np.linalg.norm(x[s])
                       for s in range(S)])
+    io_p = np.array([orthogonality_index(imfs[s][:P], x[s]) for s in range(S)])
     io = np.array([orthogonality_index(np.vstack([imfs[s], res[s][None]]), x[s]) for s in range(S)])
-    return imfs, res, recon, io
+    io_ref = np.array([orthogonality_index(means[s][:P], x[s]) for s in range(S)])
+    return imfs, res, recon, io_p, io, io_ref

@@ -106,3 +106,19 @@ def test_loss_and_adam():
     torch.cuda.synchronize()
     op, om, ov = SO.adam(p.astype(np.float64), gr, m, v, 1e-3, 1)
     assert np.allclose(pd.cpu().numpy(), op, rtol=1e-5, atol=1e-6)
+    # with the gradient clipped to norm 2 (its norm is about 31), twice
+    pd, gd, md, vd = (torch.from_numpy(a.copy()).cuda() for a in (p, gr, m, v))
+    work = torch.zeros((1,), dtype=torch.float32, device="cuda")
+    op, om, ov = p.astype(np.float64), m.astype(np.float64), v.astype(np.float64)
+    for step in (1, 2):
+        _sg.adam(pd, gd, md, vd, 1e-2, step, max_norm=2.0, work=work)
+        op, om, ov = SO.adam(op, gr.astype(np.float64), om, ov, 1e-2, step, max_norm=2.0)
+    torch.cuda.synchronize()
+    assert np.allclose(pd.cpu().numpy(), op, rtol=1e-5, atol=1e-6)
+    assert np.allclose(md.cpu().numpy(), om, rtol=1e-5, atol=1e-7)
+    # a non-finite gradient leaves everything unchanged
+    before = pd.clone()
+    gd[3] = float("nan")
+    _sg.adam(pd, gd, md, vd, 1e-2, 3, max_norm=2.0, work=work)
+    torch.cuda.synchronize()
+    assert torch.equal(pd, before)

@@ -115,13 +115,13 @@ def test_scale_prepare_combine_and_gate():
     res = torch.empty((S, N), dtype=torch.float64, device="cuda")
     chunks = 7
     part = torch.empty((S * chunks * _sg.stat_count(),), dtype=torch.float64, device="cuda")
-    met = torch.empty((S, 2), dtype=torch.float64, device="cuda")
+    met = torch.empty((S, 4), dtype=torch.float64, device="cuda")
     fb = torch.empty((S,), dtype=torch.int32, device="cuda")
     sc32 = sc.astype(np.float32).astype(np.float64)
-    oi, orr, orec, oio = SO.combine(imf_sum, count, x, sc32, netq, P)
+    oi, orr, orec, oio, oio_all, oio_ref = SO.combine(imf_sum, count, x, sc32, netq, P)
     io_bound = float(np.median(np.abs(oio[:4])))
     _sg.combine(sd, cd, xd, scale, dev(net, torch.bfloat16), imfs, res, part, chunks, S, N, K, C, P, 1e-3,
-                io_bound, met, fb)
+                io_bound, met, fb, io_relative=False)
     torch.cuda.synchronize()
     gi, gr, m = imfs.cpu().numpy(), res.cpu().numpy(), met.cpu().numpy()
     assert np.allclose(gi[:4], oi[:4], rtol=1e-12, atol=1e-12)
@@ -129,9 +129,20 @@ def test_scale_prepare_combine_and_gate():
     assert np.array_equal(gi[:, P:], oi[:, P:])
     assert np.all(m[:4, 0] < 1e-12)
     assert np.allclose(m[:4, 1], oio[:4], rtol=1e-9, atol=1e-12)
+    assert np.allclose(m[:4, 2], oio_all[:4], rtol=1e-9, atol=1e-12)
+    assert np.allclose(m[:, 3], oio_ref, rtol=1e-9, atol=1e-12)
     assert not np.isfinite(m[4, 0])
     flags = fb.cpu().numpy().tolist()
     assert flags[:4] == [int(abs(v) > io_bound) for v in oio[:4]]
+    assert flags[4] == 1
+    # the relative form: the bound applies to |io| - |io of the small-ensemble modes|
+    rel = np.abs(oio[:4]) - np.abs(oio_ref[:4])
+    rb = float(np.median(rel))
+    _sg.combine(sd, cd, xd, scale, dev(net, torch.bfloat16), imfs, res, part, chunks, S, N, K, C, P, 1e-3, rb,
+                met, fb, io_relative=True)
+    torch.cuda.synchronize()
+    flags = fb.cpu().numpy().tolist()
+    assert flags[:4] == [int(v > rb) for v in rel]
     assert flags[4] == 1
 
 
@@ -226,7 +237,7 @@ def test_training_gains_over_the_small_ensemble_and_gates_fall_back():
     # is then the plain EEMD
     N = 16384
     xs = SU.make_signals(range(30000, 30002), N)
-    sur = SU.SurrogateEEMD(net, 2, N, E_small, E_big, io_bound=0.0)
+    sur = SU.SurrogateEEMD(net, 2, N, E_small, E_big, io_bound=0.0, io_relative=False)
     served = sur.decompose(xs)
     plain = SU.plain_eemd(xs, N, E_big)
     for (m, r, st), (pm, pr) in zip(served, plain):

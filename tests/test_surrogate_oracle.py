@@ -102,14 +102,14 @@ def test_stages_identities():
     # channels times the scale sum back to x
     assert np.allclose((inp[:, :, :K + 1].sum(axis=-1)) * scale[:, None], x, atol=1e-12)
     # a zero network output serves the small-ensemble decomposition exactly
-    imfs, res, recon, io = SO.combine(imf_sum, count, x, scale, np.zeros((S, N, 16)), 6)
+    imfs, res, recon, _, _, _ = SO.combine(imf_sum, count, x, scale, np.zeros((S, N, 16)), 6)
     means, r = SO.means_and_residual(imf_sum, count, x)
     assert np.array_equal(imfs, means) and np.array_equal(res, r)
     assert np.all(recon < 1e-15)
     # any correction of the first P modes keeps the reconstruction and leaves
     # the later modes alone
     net = rng.standard_normal((S, N, 16))
-    imfs, res, recon, io = SO.combine(imf_sum, count, x, scale, net, 6)
+    imfs, res, recon, _, _, _ = SO.combine(imf_sum, count, x, scale, net, 6)
     assert np.all(recon < 1e-12)
     assert np.array_equal(imfs[:, 6:], means[:, 6:])
     # orthogonal components have index 0; two equal components have index 1/2
