@@ -309,7 +309,7 @@ def train(net: Net, inp, tgt, steps=2000, batch=32, crop=4096, lr=1e-3, seed=1, 
             mean = float(loss_acc.item()) / since  # the kernel adds every step's loss
             loss_acc.zero_()
             since = 0
-            history.append((step, mean))
+            history.append((step, mean, math.sqrt(float(net.work.item()))))  # with the last gradient norm
             if mean < best:
                 best, snap = mean, net.params.clone()
     torch.cuda.synchronize()
@@ -320,6 +320,44 @@ def train(net: Net, inp, tgt, steps=2000, batch=32, crop=4096, lr=1e-3, seed=1, 
         net.load_state(snap.cpu().numpy())
         restored = True
     return dict(history=history, seconds=time.time() - t0, weights=w.tolist(), restored=restored)
+
+
+def validation_loss(net: Net, inp, tgt, weights, delta=HUBER, chunk=4):
+    """The training loss over whole held-out signals (forward passes only)."""
+    torch = net.torch
+    S, N = inp.shape[0], inp.shape[1]
+    acc = torch.zeros((1,), dtype=torch.float32, device="cuda")
+    wd = torch.from_numpy(np.asarray(weights, np.float32)).cuda()
+    total = 0.0
+    for c0 in range(0, S, chunk):
+        cs = min(chunk, S - c0)
+        acts = net.forward(inp[c0:c0 + cs], cs, N)
+        dout = torch.empty((cs, N, CH), dtype=torch.bfloat16, device="cuda")
+        acc.zero_()
+        SG.loss(acts[-1], None, tgt[c0:c0 + cs], dout, acc, cs, N, CH, P_CORR, MARGIN, delta=delta, weights=wd)
+        total += float(acc.item()) * cs
+        del acts, dout
+    net.check()
+    return total / S
+
+
+def fit(inp, tgt, vinp, vtgt, candidates=3, steps=2000, batch=32, crop=4096, lr=1e-3, delta=HUBER):
+    """Trains `candidates` networks from different initialisations and crop
+    orders and keeps the one with the lowest validation loss (some runs stay
+    on a plateau where the first modes' averaged noise is not yet removed)."""
+    w = channel_weights(tgt)
+    best, report = None, []
+    for c in range(candidates):
+        net = Net(seed=c)
+        tr = train(net, inp, tgt, steps=steps, batch=batch, crop=crop, lr=lr, seed=1 + c, delta=delta, weights=w)
+        vl = validation_loss(net, vinp, vtgt, w, delta)
+        report.append(dict(candidate=c, validation_loss=vl, seconds=round(tr["seconds"], 1),
+                           restored_best=tr["restored"], loss_history=[(h[0], h[1]) for h in tr["history"][::10]]))
+        if best is None or vl < best[1]:
+            best = (net, vl, c)
+        else:
+            del net
+    return best[0], dict(chosen=best[2], candidates=report, channel_weights=[round(float(v), 3) for v in w])
 
 
 # ---------------------------------------------------------------------------
@@ -593,28 +631,33 @@ def main(argv=None):
     ap.add_argument("--E-big", type=int, default=256)
     ap.add_argument("--floor-signals", type=int, default=8)
     ap.add_argument("--delta", type=float, default=HUBER)
+    ap.add_argument("--candidates", type=int, default=3)
+    ap.add_argument("--val-signals", type=int, default=32)
     ap.add_argument("--save", default="", help="write the trained parameters (.npy)")
     ap.add_argument("--load", default="", help="skip training: read parameters (.npy)")
     ap.add_argument("--time-network", type=int, default=0, metavar="S",
                     help="only time the network's forward pass over S signals of N samples")
     args = ap.parse_args(argv)
     t0 = time.time()
-    net = Net(seed=0)
     if args.time_network:
-        return time_network(net, args.time_network, args.N, args.load)
-    out = dict(N=args.N, E_small=args.E_small, E_big=args.E_big, params=net.n_params)
+        return time_network(Net(seed=0), args.time_network, args.N, args.load)
+    out = dict(N=args.N, E_small=args.E_small, E_big=args.E_big)
     if args.load:
+        net = Net(seed=0)
         net.load_state(np.load(args.load))
     else:
         inp, tgt = generate_pairs(range(10000, 10000 + args.train_signals), args.N, args.E_small, args.E_big)
+        vinp, vtgt = generate_pairs(range(20000, 20000 + args.val_signals), args.N, args.E_small, args.E_big)
         out["data_seconds"] = round(time.time() - t0, 1)
-        tr = train(net, inp, tgt, steps=args.steps, batch=args.batch, crop=args.crop, lr=args.lr, delta=args.delta)
-        del inp, tgt
-        out.update(train_signals=args.train_signals, steps=args.steps, batch=args.batch, crop=args.crop,
-                   train_seconds=round(tr["seconds"], 1), loss_history=tr["history"][::5],
-                   channel_weights=[round(v, 3) for v in tr["weights"]], restored_best=tr["restored"])
+        t1 = time.time()
+        net, rep = fit(inp, tgt, vinp, vtgt, candidates=args.candidates, steps=args.steps, batch=args.batch,
+                       crop=args.crop, lr=args.lr, delta=args.delta)
+        del inp, tgt, vinp, vtgt
+        out.update(train_signals=args.train_signals, val_signals=args.val_signals, steps=args.steps,
+                   batch=args.batch, crop=args.crop, lr=args.lr, train_seconds=round(time.time() - t1, 1), fit=rep)
         if args.save:
             np.save(args.save, net.state())
+    out["params"] = net.n_params
     ev = evaluate(net, range(30000, 30000 + args.eval_signals), args.N, args.E_small, args.E_big,
                   floor_signals=args.floor_signals)
     out.update(summarize(ev))
