@@ -123,7 +123,9 @@ __global__ void __launch_bounds__(NT) k_conv_tc(const __nv_bfloat16* __restrict_
     __nv_bfloat16* sB = reinterpret_cast<__nv_bfloat16*>(smem + A_BYTES);
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tmem_slot;
+    __shared__ float sbias[COUT];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int i = tid; i < COUT; i += NT) sbias[i] = bias ? bias[i] : 0.f;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
@@ -217,7 +219,7 @@ __global__ void __launch_bounds__(NT) k_conv_tc(const __nv_bfloat16* __restrict_
                 const __nv_bfloat16* mh = reinterpret_cast<const __nv_bfloat16*>(&mv);
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
-                    float x = v[c0 + i] + (bias ? bias[c0 + i] : 0.f);
+                    float x = v[c0 + i] + sbias[c0 + i];
                     if (relu) x = fmaxf(x, 0.f);
                     if (mk && !(__bfloat162float(mh[i]) > 0.f)) x = 0.f;
                     h[i] = __float2bfloat16(x);
@@ -622,8 +624,22 @@ int launch_tc(const void* in, const void* wpk, const float* bias, void* out, int
     if (cudaFuncSetAttribute(k_conv_tc<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return EEMD_SG_E_CUDA;
+    // persistent CTAs: as many as fit on the device at once (shared memory bounds them)
+    static int resident = 0;
+    if (resident == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv_tc<CIN, COUT>, NT, smem) != cudaSuccess)
+            return EEMD_SG_E_CUDA;
+        // tensor memory: 512 columns per SM, TCOLS per CTA (an allocation that
+        // does not fit would wait for another CTA's release)
+        const int tcols = COUT < 32 ? 32 : COUT;
+        if (per_sm > 512 / tcols) per_sm = 512 / tcols;
+        resident = sms * (per_sm > 0 ? per_sm : 1);
+    }
     const int tiles = B * ((T + TM - 1) / TM);
-    const int grid = tiles < 2 * 148 ? tiles : 2 * 148;
+    const int grid = tiles < resident ? tiles : resident;
     k_conv_tc<CIN, COUT><<<grid, NT, smem, st>>>(static_cast<const __nv_bfloat16*>(in),
                                                   static_cast<const __nv_bfloat16*>(wpk), bias,
                                                   static_cast<__nv_bfloat16*>(out), B, T, dil, dir, relu,
