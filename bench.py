@@ -9,7 +9,7 @@ spline solve.  Metric: Msamples*trials/s = sum(N)*E / step time (whole job:
 summed over ranks).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload harmonic48k|plain8k|amfm4m|uneven512]
+                    [--workload harmonic48k|plain8k|amfm4m|uneven512|surrogate|ceemdan48k]
 
 The other workloads measure the remaining configurations of the path:
 plain8k (single-trial plain EMD, float64, mirror ends, N=8192), amfm4m (N=2^22
@@ -791,16 +791,120 @@ def run_surrogate(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# CEEMDAN (emd_ref.py:220-259 semantics) on the engine
+# ---------------------------------------------------------------------------
+CEEMDAN_WL = Workload(
+    "ceemdan48k",
+    {"workload": "harmonic_clicks_48k_ceemdan", "N": 48000, "trials": 100, "eps": 0.2, "tau": 0.25,
+     "max_sifts": 50, "storage": "float64", "solve": "float64 (seam windows)", "noise": "default_rng(0) W [E,N]",
+     "signals": 1},
+    E=100, eps=0.2, max_imf=1, max_sifts=50, tau=0.25, dtype="f64", seed=1, cpu_tasks=16,
+    signals_fn=_harmonic)
+
+
+def run_ceemdan(args):
+    """One step: the whole CEEMDAN of the 48 kHz harmonic signal (stage 0
+    noise EMDs plus every stage).  value counts N samples per (stage, trial),
+    stage 0 included."""
+    import torch
+
+    rank, local_rank, world = rank_env()
+    if world > 1 and rank != 0:
+        return 0
+    torch.cuda.set_device(local_rank)
+    from eemd4cuda_b200 import _lib as L
+    from eemd4cuda_b200 import emd_par as M
+    from eemd4cuda_b200.ceemdan import ceemdan
+
+    wl = CEEMDAN_WL
+    cb = CpuBaseline(wl) if world == 1 else None
+    x = wl.signals()[0]
+    N, E = len(x), wl.E
+    kw = dict(E=E, eps=wl.eps, seed=0, tau=wl.tau, max_sifts=wl.max_sifts)
+    for _ in range(args.warmup):
+        c, r, st = ceemdan(x, **kw)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    clk = ClockSampler(local_rank)
+    clk.start()
+    total = 0.0
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        c, r, st = ceemdan(x, **kw)
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    clocks = clk.stop()
+    ms = total / args.steps
+    stages = st["n_imfs"] + 1
+    value = N * E * stages / (ms / 1e3) / 1e6
+
+    # roofline of k_emd on one stage-1 launch (first IMF of x + beta W[e])
+    dev = torch.device("cuda", local_rank)
+    p1 = M.make_params(dtype=np.float64, noise_mode=L.EEMD_NOISE_SCALED, eps=float(wl.eps * np.std(x)),
+                       tau=wl.tau, max_sifts=wl.max_sifts, max_imf=1, min_extrema=4)
+    ws = torch.empty((L.workspace_size(p1, [N], E, False),), dtype=torch.uint8, device=dev)
+    Wd = torch.from_numpy(np.random.default_rng(0).standard_normal((E, N))).to(dev)
+    xd = torch.from_numpy(x).to(dev)
+    imf_sum = torch.zeros((N,), dtype=torch.float64, device=dev)
+    cnt = torch.zeros((1,), dtype=torch.int32, device=dev)
+    klog = torch.full((E, 1, wl.max_sifts, 2), -1, dtype=torch.int32, device=dev)
+    nmode = torch.zeros((E,), dtype=torch.int32, device=dev)
+    times = L.KernelTimes()
+    L.run(p1, xd, [N], 0, E, ws, noise=Wd, imf_sum=imf_sum, mode_count=cnt)
+    L.run(p1, xd, [N], 0, E, ws, noise=Wd, imf_sum=imf_sum, mode_count=cnt, times=times, knot_log=klog,
+          nmode=nmode)
+    torch.cuda.synchronize()
+    kt = times.as_dict()
+    ev = kt["emd"]
+    emd_bytes = emd_algorithmic_bytes(klog.cpu().numpy(), nmode.cpu().numpy(), [N], E, 8)
+    gbs = emd_bytes / (ev["ms"] / 1e3) / 1e9 if ev["ms"] > 0 else 0.0
+    peak, peak_kind = measured_peak_hbm()
+    launches_stage = sum(v["launches"] for v in kt.values())
+
+    cpu = None
+    if cb is not None:
+        cb.step()
+        cpu = cb.describe(cb.value(cb.step()))
+        cpu["sample"] += "; stage-1 tasks (first IMF of x + eps*std(x)*w), the unit of this line"
+        cb.close()
+    line = {
+        "metric": "CEEMDAN Msamples*trials/s (per stage)", "value": round(value, 3), "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(wl.config, stages=stages, parallelism="replicas1",
+                       note="host numpy computes beta = eps*std(r) and the stop tests between stages, as the "
+                            "reference does; value and e2e are the same call (host signal in, host modes out)"),
+        "e2e": {"value": round(value, 3), "unit": UNIT, "ms_per_step": round(ms, 3),
+                "h2d_bytes_per_step": (E * N + N) * 8, "d2h_bytes_per_step": (2 * stages * N + E) * 8},
+        "gpu_launches": (launches_stage * stages + 1) * args.steps,
+        "roofline": {"bound": "hbm", "kernel": "k_emd", "stage": 1, "achieved": round(gbs, 2), "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(gbs / peak, 4), "traffic": None,
+                     "algorithmic_bytes_per_launch": round(emd_bytes), "avg_launch_ms": round(ev["ms"], 5)},
+        "noise_modes": sorted(set(st["noise_modes"])), "clocks": clocks,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["surrogate"], default="harmonic48k")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["surrogate", "ceemdan48k"], default="harmonic48k")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload == "ceemdan48k":
+        if args.impl == "reference":
+            return run_reference(args, CEEMDAN_WL)
+        return run_ceemdan(args)
     if args.workload == "surrogate":
         if args.impl == "reference":
             return run_reference(args, surrogate_cpu_workload())

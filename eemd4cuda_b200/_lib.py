@@ -33,6 +33,7 @@ EEMD_NOISE_NONE = 0
 EEMD_NOISE_PHILOX = 1
 EEMD_NOISE_INJECTED = 2
 EEMD_NOISE_PREPERTURBED = 3
+EEMD_NOISE_SCALED = 4
 ABI_VERSION = 1
 
 # every symbol include/eemd_b200.h declares

@@ -656,6 +656,9 @@ __device__ __forceinline__ double trial_input(const Ctx& C, const TaskDesc& d, i
     const double xv = ldv<T>(C.x, d.x_off + t);
     switch (C.noise_mode) {
         case EEMD_NOISE_INJECTED: return rnd<T>(xv + ldv<T>(C.noise, d.noise_off + t));
+        case EEMD_NOISE_SCALED:
+            // the product, then the sum, each rounded (the reference forms beta * w, then x + that)
+            return rnd<T>(__dadd_rn(xv, __dmul_rn(C.noise_scale, ldv<T>(C.noise, d.noise_off + t))));
         case EEMD_NOISE_PHILOX:
             return rnd<T>(xv + C.sigma[d.signal] * philox_normal(C.seed, d.signal, d.trial, t));
         default: return xv;  // NONE, PREPERTURBED
@@ -1699,7 +1702,7 @@ int check_params(const eemd_params* p) {
     if (p->max_sifts < 1 || p->max_imf < 1 || p->max_imf > 4096) return EEMD_E_BADARG;
     if (p->end_mode != EEMD_END_NATURAL && p->end_mode != EEMD_END_MIRROR) return EEMD_E_BADARG;
     if (p->rules != EEMD_RULES_REF && p->rules != EEMD_RULES_NUMBA) return EEMD_E_BADARG;
-    if (p->noise_mode < EEMD_NOISE_NONE || p->noise_mode > EEMD_NOISE_PREPERTURBED) return EEMD_E_BADARG;
+    if (p->noise_mode < EEMD_NOISE_NONE || p->noise_mode > EEMD_NOISE_SCALED) return EEMD_E_BADARG;
     // warp tile: 32 lanes x 8 float32 samples or x 4 float64 samples
     const int wt = (p->dtype == EEMD_F64) ? Geo<double>::WT : Geo<float>::WT;
     if (p->tile != 0 && p->tile != wt) return EEMD_E_BADARG;
@@ -1975,7 +1978,8 @@ int32_t eemd_run_traced(const eemd_params* p, const void* x, const int64_t* leng
     int rc = make_layout(p, lengths, n_signals, trial_count, trial_begin, imfs != nullptr, L);
     if (rc) return rc;
     if (!x || !ws) return EEMD_E_BADARG;
-    if (p->noise_mode == EEMD_NOISE_INJECTED && !noise) return EEMD_E_BADARG;
+    if ((p->noise_mode == EEMD_NOISE_INJECTED || p->noise_mode == EEMD_NOISE_SCALED) && !noise)
+        return EEMD_E_BADARG;
     if (ws_bytes < L.total) return EEMD_E_NOMEM;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     char* base = static_cast<char*>(ws);
@@ -2020,6 +2024,7 @@ int32_t eemd_run_traced(const eemd_params* p, const void* x, const int64_t* leng
     C.S = L.S;
     C.scr_rows = L.scr_rows;
     C.tau = p->tau;
+    C.noise_scale = p->eps;
     C.seed = p->seed;
     C.watchdog = p->watchdog != 0 ? p->watchdog : (1LL << 24);
 

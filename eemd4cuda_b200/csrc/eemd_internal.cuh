@@ -118,6 +118,7 @@ struct Ctx {
     int32_t max_sifts, max_imf, min_extrema, end_mode, rules, noise_mode;
     int32_t B, S, scr_rows;
     double tau;
+    double noise_scale;           // EEMD_NOISE_SCALED: the factor on noise[task][n]
     uint64_t seed;
     long long watchdog;
 };

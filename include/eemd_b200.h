@@ -69,6 +69,8 @@ extern "C" {
 #define EEMD_NOISE_PHILOX       1  /* x + eps*std(x)*N(0,1), Philox4x32-10 keyed by (seed, signal, trial) */
 #define EEMD_NOISE_INJECTED     2  /* x + noise[task][n] (noise already scaled) */
 #define EEMD_NOISE_PREPERTURBED 3  /* x holds one perturbed signal per task: x[task][n] */
+#define EEMD_NOISE_SCALED       4  /* x + eps * noise[task][n] (eps absolute; product and sum each
+                                      rounded): the CEEMDAN stage input, emd_ref.py:247-248 */
 
 typedef struct eemd_params {
     int32_t  dtype;           /* EEMD_F64 or EEMD_F32 */

@@ -22,6 +22,7 @@ Followed reference lines (misureaudio/EEMD4CUDA):
   emd_gpu_v5_dsbt.py:51-74 + audit_eemd/test_block_thomas.py:86-114
                      seam-window Thomas (owned-only) -> dsbt_solve()
   audit_eemd/test_block_thomas.py:121-133 tile scan  -> scan_tiles()
+  emd_ref.py:158-162, 166-168, 220-259 CEEMDAN        -> ceemdan()
 """
 from __future__ import annotations
 
@@ -295,6 +296,47 @@ def eemd(x, X, **kw):
     res = [emd_1d(X[e], **kw) for e in range(X.shape[0])]
     avg, resid, _ = ensemble_mean(x, [r[0] for r in res])
     return avg, resid, res
+
+
+def ceemdan(x, E=100, eps=0.2, seed=0, tau=0.25, max_sifts=50, end="natural"):
+    """CEEMDAN as the reference computes it (emd_ref.py:220-259).
+
+    W = default_rng(seed).standard_normal((E, N)) (emd_ref.py:166-168).
+    Stage 0: the full EMD of every W[e]; only its mode count is used (the
+    stop test below; the normalised noise IMFs are not added anywhere).
+    Stage k: while max|r| >= 1e-12 and std(r) >= 1e-10, beta = eps*std(r),
+    c_k = (sum over e, in order, of the first IMF of r + beta*W[e]) / E (first
+    IMF: emd_1d with max_imf=1, min_extrema=4, emd_ref.py:158-162), r -= c_k;
+    stop after stage k when k >= the mode count of every noise EMD.
+    Returns (c [n_imfs, N], r, stats with E, n_imfs, noise_modes, stage_sifts)."""
+    x = np.asarray(x, dtype=float)
+    N = len(x)
+    W = np.random.default_rng(seed).standard_normal((E, N))
+    noise_modes = [emd_1d(W[e] + np.zeros(N), tau=tau, max_sifts=max_sifts, min_extrema=4, end=end)[2]["n_modes"]
+                   for e in range(E)]
+    c_imfs = []
+    stage_sifts = []
+    resid = x.copy()
+    while True:
+        if np.max(np.abs(resid)) < 1e-12 or np.std(resid) < 1e-10:
+            break
+        stage = len(c_imfs)
+        beta = eps * np.std(resid)
+        c = np.zeros(N)
+        sifts = []
+        for e in range(E):
+            imfs, _, st = emd_1d(resid + beta * W[e], tau=tau, max_sifts=max_sifts, max_imf=1, min_extrema=4,
+                                 end=end)
+            c += imfs[0]
+            sifts.append(st["per_mode_sifts"][0])
+        c /= E
+        c_imfs.append(c)
+        stage_sifts.append(sifts)
+        resid = resid - c
+        if all(stage >= noise_modes[e] for e in range(E)):
+            break
+    return np.array(c_imfs), resid, dict(E=E, n_imfs=len(c_imfs), noise_modes=noise_modes,
+                                         stage_sifts=stage_sifts)
 
 
 # ---------------------------------------------------------------------------
