@@ -9,7 +9,7 @@ spline solve.  Metric: Msamples*trials/s = sum(N)*E / step time (whole job:
 summed over ranks).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload harmonic48k|plain8k|amfm4m|uneven512|surrogate|ceemdan48k]
+                    [--workload harmonic48k|plain8k|amfm4m|uneven512|surrogate|ceemdan48k|spectra48k]
 
 The other workloads measure the remaining configurations of the path:
 plain8k (single-trial plain EMD, float64, mirror ends, N=8192), amfm4m (N=2^22
@@ -891,16 +891,129 @@ def run_ceemdan(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# the IMF spectra stage (spectra.py:18-58 semantics) on the device
+# ---------------------------------------------------------------------------
+def run_spectra(args):
+    """One step: the Tier-2 spectra of the bench workload's decomposition --
+    STFT (nperseg 4096, 50 % overlap) of x and of its 8 ensemble-mean IMFs and
+    the Hilbert frequency / amplitude of every IMF -- on device-resident rows.
+    value = rows x N / step time."""
+    import torch
+
+    rank, local_rank, world = rank_env()
+    if world > 1 and rank != 0:
+        return 0
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    from eemd4cuda_b200 import emd_par as M
+    from eemd4cuda_b200 import spectra
+    from oracle import spectra_oracle as SPO
+
+    wl = WORKLOADS["harmonic48k"]
+    x = wl.signals()[0]
+    r = M.decompose(x.astype(np.float32), E=wl.E, eps=wl.eps, tau=wl.tau, max_sifts=wl.max_sifts,
+                    max_imf=wl.max_imf, seed=wl.seed, dtype=np.float32)
+    sr, N, nper = 48000, len(x), 4096
+    imfs = torch.from_numpy(np.ascontiguousarray(r.imfs)).to(dev)
+    xd = torch.from_numpy(np.ascontiguousarray(x, dtype=np.float64)).to(dev).reshape(1, -1)
+    rows = 1 + r.n_modes
+
+    def step():
+        spectra.stft_device(xd, sr, nper)
+        spectra.stft_device(imfs, sr, nper)
+        return spectra.hilbert_if_device(imfs, sr)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    flush = torch.empty((2 * L2_BYTES,), dtype=torch.uint8, device=dev)
+    clk = ClockSampler(local_rank)
+    clk.start()
+    total = 0.0
+    for _ in range(args.steps):
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    clocks = clk.stop()
+    ms = total / args.steps
+    value = rows * N / (ms / 1e3) / 1e6
+    # Hilbert alone on the IMFs: algorithmic bytes = read the row, write frequency and amplitude
+    flush.fill_(1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    spectra.hilbert_if_device(imfs, sr)
+    e1.record(stream)
+    e1.synchronize()
+    h_ms = e0.elapsed_time(e1)
+    h_bytes = r.n_modes * N * (8 + 16)
+    gbs = h_bytes / (h_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    # end to end through the host API (host rows in, host spectra out)
+    hx, himfs = np.ascontiguousarray(x, dtype=np.float64), np.ascontiguousarray(r.imfs)
+    e2e_ms = []
+    for _ in range(max(1, args.steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        spectra.stft_block(hx, sr, nper)
+        spectra.stft_block(himfs, sr, nper)
+        spectra.hilbert_if(himfs, sr)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e = statistics.median(e2e_ms)
+    F, T = nper // 2 + 1, (N + nper - nper // 2) // (nper // 2)
+    # CPU: the oracle's numpy restatement of the reference's scipy calls, one core
+    t0 = time.perf_counter()
+    SPO.stft(hx, sr, nper)
+    for k in range(r.n_modes):
+        SPO.stft(himfs[k], sr, nper)
+        SPO.hilbert_if(himfs[k], sr)
+    cpu_s = time.perf_counter() - t0
+    line = {
+        "metric": "IMF spectra Msamples/s", "value": round(value, 3), "unit": "Msamples/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "spectra_of_harmonic48k_decomposition", "N": N, "rows": rows,
+                   "imfs": r.n_modes, "nperseg": nper, "noverlap": nper // 2, "sr": sr,
+                   "l2": "flushed between timed steps (256 MiB write)"},
+        "e2e": {"value": round(rows * N / (e2e / 1e3) / 1e6, 3), "unit": "Msamples/s", "ms_per_step": round(e2e, 3),
+                "h2d_bytes_per_step": rows * N * 8 + r.n_modes * N * 8,
+                "d2h_bytes_per_step": rows * F * T * 16 + 2 * r.n_modes * N * 8},
+        "gpu_launches": 6 * args.steps,  # k_frames + k_stft_out per STFT call, k_analytic + k_if_amp (cuFFT not counted)
+        "roofline": {"bound": "hbm", "kernel": "hilbert stage (cuFFT D2Z, k_analytic, Z2Z, k_if_amp)",
+                     "achieved": round(gbs, 2), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": round(gbs / peak, 4), "traffic": None, "algorithmic_bytes": h_bytes,
+                     "ms": round(h_ms, 4)},
+        "cpu_baseline": {"value": round(rows * N / cpu_s / 1e6, 4), "unit": "Msamples/s", "cores": 1,
+                         "kind": "port", "sample": "the whole step once with the oracle's numpy restatement "
+                                                    "(numpy FFT, one thread)"},
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["surrogate", "ceemdan48k"], default="harmonic48k")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["surrogate", "ceemdan48k", "spectra48k"],
+                    default="harmonic48k")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload == "spectra48k":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "spectra48k analyses the engine's IMFs of the "
+                              "bench workload (a GPU result); its line carries the numpy restatement's CPU time"}))
+            return 0
+        return run_spectra(args)
     if args.workload == "ceemdan48k":
         if args.impl == "reference":
             return run_reference(args, CEEMDAN_WL)

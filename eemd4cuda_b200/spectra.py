@@ -1,0 +1,95 @@
+"""The IMF spectra stage on the device, with the reference's interface
+(audio_eemd/spectra.py:18-58): stft_block, hilbert_if, if_stats.
+
+stft_block and hilbert_if take one signal (1-D) or a batch of rows (2-D,
+[M, N]) as host arrays and return host arrays, like the reference; the
+*_device variants take and return float64 torch tensors resident on the GPU,
+so the IMFs of eemd_finalize can be analysed without leaving the device.
+All arithmetic runs in libeemd_spectra.so (cuFFT for the transforms, this
+package's kernels between them); if_stats is the reference's host reduction.
+"""
+from __future__ import annotations
+
+import warnings
+
+import numpy as np
+
+from . import _sp
+
+__all__ = ["stft_block", "hilbert_if", "if_stats", "stft_device", "hilbert_if_device"]
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("the spectra stage needs a CUDA device")
+    return torch
+
+
+def hilbert_if_device(x, sr):
+    """x: float64 CUDA tensor [M, N] (or [N]) -> (inst_freq, inst_amp) of the same shape."""
+    torch = _torch()
+    x2 = x.reshape(1, -1) if x.dim() == 1 else x
+    x2 = x2.contiguous()
+    M, N = int(x2.shape[0]), int(x2.shape[1])
+    if N < 2:
+        raise ValueError("hilbert_if needs at least 2 samples")
+    freq = torch.empty_like(x2)
+    amp = torch.empty_like(x2)
+    ws = torch.empty((_sp.hilbert_workspace(M, N),), dtype=torch.uint8, device=x2.device)
+    _sp.hilbert_if(x2, M, N, sr, freq, amp, ws)
+    return freq.reshape(x.shape), amp.reshape(x.shape)
+
+
+def hilbert_if(imf, sr):
+    """Instantaneous frequency [Hz] and amplitude of one IMF (or of each row):
+    z = imf + i H(imf), d/dt arg(z) / 2 pi, |z| (spectra.py:32-45)."""
+    torch = _torch()
+    a = np.ascontiguousarray(imf, dtype=np.float64)
+    f, A = hilbert_if_device(torch.from_numpy(a).cuda(), sr)
+    return f.cpu().numpy(), A.cpu().numpy()
+
+
+def _segments(N, nperseg, noverlap):
+    # scipy's rule: a segment longer than the input is cut to it (with a warning)
+    if nperseg > N:
+        warnings.warn(f"nperseg = {nperseg} is greater than input length = {N}, using nperseg = {N}")
+        nperseg = N
+    if noverlap is None:
+        noverlap = nperseg // 2
+    if noverlap >= nperseg:
+        raise ValueError("noverlap must be less than nperseg.")
+    return int(nperseg), int(noverlap)
+
+
+def stft_device(x, sr, nperseg=4096, noverlap=None):
+    """x: float64 CUDA tensor [M, N] (or [N]) -> (f, t, Z complex128 [M, F, T] (or [F, T]))."""
+    torch = _torch()
+    x2 = (x.reshape(1, -1) if x.dim() == 1 else x).contiguous()
+    M, N = int(x2.shape[0]), int(x2.shape[1])
+    nperseg, noverlap = _segments(N, nperseg, noverlap)
+    F, T = _sp.stft_shape(N, nperseg, noverlap)
+    Z = torch.empty((M, F, T), dtype=torch.complex128, device=x2.device)
+    ws = torch.empty((_sp.stft_workspace(M, N, nperseg, noverlap),), dtype=torch.uint8, device=x2.device)
+    _sp.stft(x2, M, N, nperseg, noverlap, Z, ws)
+    f = np.fft.rfftfreq(nperseg, 1.0 / sr)
+    t = np.arange(T) * (nperseg - noverlap) / float(sr)
+    return f, t, (Z[0] if x.dim() == 1 else Z)
+
+
+def stft_block(x, sr, nperseg=4096, noverlap=None):
+    """STFT of a signal (or of each row): Hann window, 50 % overlap by
+    default, zero-extended ends, one-sided (spectra.py:18-29).  Returns (f, t, Zxx)."""
+    torch = _torch()
+    a = np.ascontiguousarray(x, dtype=np.float64)
+    f, t, Z = stft_device(torch.from_numpy(a).cuda(), sr, nperseg, noverlap)
+    return f, t, Z.cpu().numpy()
+
+
+def if_stats(w: np.ndarray) -> dict:
+    """Median / IQR of an IF series, positive part only (spectra.py:48-58)."""
+    wp = w[w > 0]
+    if wp.size == 0:
+        return {"median": None, "iqr": None, "n_pos_frac": 0.0}
+    lo, hi = np.percentile(wp, [25, 75])
+    return {"median": float(np.median(wp)), "iqr": float(hi - lo), "n_pos_frac": float(wp.size / w.size)}

@@ -1,0 +1,77 @@
+"""The spectra stage on the GPU (libeemd_spectra.so) against fixtures made by
+the reference's own audio_eemd/spectra.py and against the CPU oracle."""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from oracle import spectra_oracle as SP
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+from eemd4cuda_b200 import spectra  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def golden():
+    d = np.load(GOLDEN / "spectra_cases.npz")
+    return {k: d[k] for k in d.files}
+
+
+def steady(amp, frac=1e-3):
+    """samples whose analytic-signal magnitude (and its neighbours') is not
+    near zero: elsewhere the phase, hence the frequency, is ill-conditioned"""
+    ok = amp > frac * amp.max()
+    return ok & np.roll(ok, 1) & np.roll(ok, -1)
+
+
+@pytest.mark.parametrize("name", ["a", "b", "c"])
+def test_spectra_match_reference(golden, name):
+    N, sr, nper, nov = golden[f"{name}_params"].tolist()
+    nov = None if nov < 0 else nov
+    X = golden[f"{name}_x"]
+    # the batched call: all rows at once
+    f, t, Z = spectra.stft_block(X, sr, nperseg=nper, noverlap=nov)
+    w, A = spectra.hilbert_if(X, sr)
+    assert np.allclose(f, golden[f"{name}_f"], rtol=0, atol=1e-9)
+    assert np.allclose(t, golden[f"{name}_t"], rtol=0, atol=1e-12)
+    for r in range(X.shape[0]):
+        Zr = golden[f"{name}_{r}_Z"]
+        assert Z[r].shape == Zr.shape
+        assert np.max(np.abs(Z[r] - Zr)) <= 1e-11 * np.max(np.abs(Zr))
+        Ar, wr = golden[f"{name}_{r}_amp"], golden[f"{name}_{r}_if"]
+        assert np.max(np.abs(A[r] - Ar)) <= 1e-11 * np.max(Ar)
+        m = steady(Ar)
+        assert np.max(np.abs(w[r] - wr)[m]) <= 1e-6 * sr
+        st = spectra.if_stats(w[r])
+        ref = golden[f"{name}_{r}_ifstats"]
+        assert abs(st["n_pos_frac"] - ref[2]) <= 2.0 / N
+        assert abs(st["median"] - ref[0]) <= 1e-6 * sr
+    # one row at a time gives the same as the batch
+    f1, t1, Z1 = spectra.stft_block(X[1], sr, nperseg=nper, noverlap=nov)
+    w1, A1 = spectra.hilbert_if(X[1], sr)
+    assert np.max(np.abs(Z1 - Z[1])) <= 1e-13 * np.max(np.abs(Z1))
+    assert np.max(np.abs(A1 - A[1])) <= 1e-13 * np.max(A1)
+
+
+def test_spectra_of_imfs_48k_against_the_oracle():
+    """Ten IMF-sized rows of 48 000 samples, device-resident in and out."""
+    rng = np.random.default_rng(5)
+    sr, N = 48000, 48000
+    t = np.arange(N) / sr
+    rows = [np.sin(2 * np.pi * (f0 * t + 30 * t * t)) * (1 + 0.2 * np.sin(2 * np.pi * 2 * t))
+            for f0 in rng.uniform(30, 9000, 10)]
+    X = np.vstack(rows)
+    Xd = torch.from_numpy(X).cuda()
+    w, A = spectra.hilbert_if_device(Xd, sr)
+    f, tt, Z = spectra.stft_device(Xd, sr, nperseg=4096)
+    assert w.is_cuda and Z.is_cuda
+    w, A, Z = w.cpu().numpy(), A.cpu().numpy(), Z.cpu().numpy()
+    for r in range(10):
+        ow, oA = SP.hilbert_if(X[r], sr)
+        assert np.max(np.abs(A[r] - oA)) <= 1e-10 * np.max(oA)
+        m = steady(oA)
+        # the oracle differentiates a cumulative phase of up to ~1e5 rad; allow its rounding
+        assert np.max(np.abs(w[r] - ow)[m]) <= 1e-6 * sr
+        _, _, oZ = SP.stft(X[r], sr, 4096)
+        assert np.max(np.abs(Z[r] - oZ)) <= 1e-11 * np.max(np.abs(oZ))

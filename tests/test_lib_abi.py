@@ -107,3 +107,26 @@ def test_run_rejects_small_workspace_without_touching_the_device():
     rc = lib.eemd_run(ctypes.byref(p), ctypes.c_void_p(16), la, 1, 0, 1, None, None, None, None,
                       None, None, None, None, None, None, ctypes.c_void_p(16), need, None)
     assert rc == L.EEMD_E_BADARG
+
+
+@pytest.mark.parametrize("header,module", [("eemd_surrogate.h", "_sg"), ("eemd_spectra.h", "_sp")])
+def test_other_libraries_export_their_headers(header, module):
+    import importlib
+    mod = importlib.import_module(f"eemd4cuda_b200.{module}")
+    text = re.sub(r"/\*.*?\*/", "", (HEADER.parent / header).read_text(), flags=re.S)
+    declared = sorted(set(re.findall(r"\b(eemd_[a-z_]+)\s*\(", text)))
+    assert declared == sorted(mod.EXPORTS)
+    lib = ctypes.CDLL(str(mod.lib_path()))
+    for name in declared:
+        assert hasattr(lib, name), name
+
+
+def test_stft_shape_matches_the_reference_frame_count():
+    from eemd4cuda_b200 import _sp
+    # scipy.signal.stft(boundary='zeros', padded=False): N + 2*(nperseg//2) samples, hop nperseg - noverlap
+    for N, nper, nov in [(48000, 4096, 2048), (3000, 256, 128), (4097, 512, 384), (2048, 2048, 1024)]:
+        F, T = _sp.stft_shape(N, nper, nov)
+        assert F == nper // 2 + 1
+        assert T == (N + 2 * (nper // 2) - nov) // (nper - nov)
+    with pytest.raises(_sp.SpectraError):
+        _sp.stft_shape(100, 64, 64)
