@@ -237,6 +237,181 @@ __global__ void __launch_bounds__(NT) k_conv_tc(const __nv_bfloat16* __restrict_
     }
 }
 
+// ---------------------------------------------------------------------------
+// Double-buffered variant: two input-tile buffers and two accumulators in
+// tensor memory.  Per tile k of this CTA: wait until MMA(k-1) is done (its
+// accumulator is complete and its input buffer free), start the copies of
+// tile k+1 into that buffer, wait for tile k's copies, issue MMA(k), then run
+// the epilogue of tile k-1 while MMA(k) and the copies of tile k+1 proceed.
+// ---------------------------------------------------------------------------
+template <int CIN>
+__device__ __forceinline__ void stage_tile(__nv_bfloat16* sA, const __nv_bfloat16* in, int tile, int tiles_per_b,
+                                           int T, int dil, int dir, int tid) {
+    const int b = tile / tiles_per_b, t0 = (tile % tiles_per_b) * TM;
+    const __nv_bfloat16* inb = in + (size_t)b * T * CIN;
+    for (int i = tid; i < 3 * TM * (CIN / 8); i += NT) {
+        const int chunk = i % (CIN / 8);
+        const int r = (i / (CIN / 8)) % TM;
+        const int tap = i / ((CIN / 8) * TM);
+        const int ts = t0 + r + dir * (tap - 1) * dil;
+        const bool ok = (ts >= 0 && ts < T);
+        cp16(sA + kmaj_off(r, tap * CIN + chunk * 8, TM),
+             ok ? (const void*)(inb + (size_t)ts * CIN + chunk * 8) : (const void*)inb, ok ? 16 : 0);
+    }
+}
+
+// bounded wait for an mbarrier phase; false when it gave up
+__device__ __forceinline__ bool wait_parity(uint64_t* bar, uint32_t phase, long long limit) {
+    long long spins = 0;
+    uint32_t done = 0;
+    while (!done) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(phase)
+            : "memory");
+        if (!done && ++spins > limit) return false;
+    }
+    return true;
+}
+
+template <int COUT>
+__device__ __forceinline__ void epilogue(uint32_t taddr, const float* sbias, __nv_bfloat16* out,
+                                         const __nv_bfloat16* __restrict__ mask, int tile, int tiles_per_b, int T,
+                                         int relu, int warp, int lane) {
+    float v[COUT];
+    tmem_ld<COUT>(taddr + ((uint32_t)(32 * warp) << 16), v);
+    const int b = tile / tiles_per_b, t = (tile % tiles_per_b) * TM + 32 * warp + lane;
+    if (t >= T) return;
+    __nv_bfloat16* o = out + ((size_t)b * T + t) * COUT;
+    const __nv_bfloat16* mk = mask ? mask + ((size_t)b * T + t) * COUT : nullptr;
+#pragma unroll
+    for (int c0 = 0; c0 < COUT; c0 += 8) {
+        __align__(16) __nv_bfloat16 h[8];
+        uint4 mv = make_uint4(0, 0, 0, 0);
+        if (mk) mv = *reinterpret_cast<const uint4*>(mk + c0);
+        const __nv_bfloat16* mh = reinterpret_cast<const __nv_bfloat16*>(&mv);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            float x = v[c0 + i] + sbias[c0 + i];
+            if (relu) x = fmaxf(x, 0.f);
+            if (mk && !(__bfloat162float(mh[i]) > 0.f)) x = 0.f;
+            h[i] = __float2bfloat16(x);
+        }
+        *reinterpret_cast<uint4*>(o + c0) = *reinterpret_cast<const uint4*>(h);
+    }
+}
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(NT) k_conv_tc2(const __nv_bfloat16* __restrict__ in,
+                                                 const __nv_bfloat16* __restrict__ wpk,
+                                                 const float* __restrict__ bias, __nv_bfloat16* out, int B, int T,
+                                                 int dil, int dir, int relu, const __nv_bfloat16* __restrict__ mask,
+                                                 int* err, long long spin_limit) {
+    constexpr int K = 3 * CIN;
+    constexpr int KSTEPS = K / 16;
+    constexpr int A_BYTES = K * TM * 2;
+    constexpr int B_BYTES = K * COUT * 2;
+    constexpr int ACOLS = COUT < 32 ? 32 : COUT;  // columns of one accumulator
+    constexpr int TCOLS = 2 * ACOLS;
+    static_assert(CIN % 16 == 0 && COUT % 16 == 0 && TCOLS <= 512, "shape");
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __nv_bfloat16* sA0 = reinterpret_cast<__nv_bfloat16*>(smem);
+    __nv_bfloat16* sB = reinterpret_cast<__nv_bfloat16*>(smem + 2 * A_BYTES);
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t tmem_slot;
+    __shared__ float sbias[COUT];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int i = tid; i < COUT; i += NT) sbias[i] = bias ? bias[i] : 0.f;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                         smem_u32(&tmem_slot)),
+                     "r"(TCOLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mbar[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    const int tiles_per_b = (T + TM - 1) / TM;
+    const int n_tiles = B * tiles_per_b;
+    const int nk = blockIdx.x < n_tiles ? (n_tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    // weights and the first tile: one copy group
+    for (int i = tid; i < B_BYTES / 16; i += NT) cp16(reinterpret_cast<char*>(sB) + 16 * i, wpk + 8 * i, 16);
+    if (nk > 0) stage_tile<CIN>(sA0, in, blockIdx.x, tiles_per_b, T, dil, dir, tid);
+    cp_commit();
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    const uint32_t a_base = smem_u32(sA0), b_base = smem_u32(sB);
+    constexpr uint32_t IDESC = instr_desc(TM, COUT);
+    uint32_t phase[2] = {0u, 0u};
+    bool failed = false;
+    for (int k = 0; k < nk; ++k) {
+        const int buf = k & 1;
+        if (k >= 1) {
+            // MMA(k-1): its accumulator complete, its input buffer free
+            if (!wait_parity(&mbar[buf ^ 1], phase[buf ^ 1], spin_limit)) failed = true;
+            phase[buf ^ 1] ^= 1u;
+        }
+        if (__syncthreads_or(failed ? 1 : 0)) {
+            if (tid == 0) raise(err, EEMD_SG_E_TIMEOUT);
+            break;
+        }
+        if (k + 1 < nk)
+            stage_tile<CIN>(reinterpret_cast<__nv_bfloat16*>(smem + (buf ^ 1) * A_BYTES), in,
+                            blockIdx.x + (k + 1) * gridDim.x, tiles_per_b, T, dil, dir, tid);
+        cp_commit();
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // tile k's copies (and the weights) landed
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t a_buf = a_base + buf * A_BYTES;
+#pragma unroll
+            for (int s2 = 0; s2 < KSTEPS; ++s2) {
+                const uint64_t da = smem_desc(a_buf + s2 * 2 * (TM * 16), TM * 16, 128);
+                const uint64_t db = smem_desc(b_base + s2 * 2 * (COUT * 16), COUT * 16, 128);
+                const uint32_t acc = s2 > 0 ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem + buf * ACOLS),
+                    "l"(da), "l"(db), "r"(IDESC), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             smem_u32(&mbar[buf]))
+                         : "memory");
+        }
+        if (k >= 1) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            epilogue<COUT>(tmem + (buf ^ 1) * ACOLS, sbias, out, mask, blockIdx.x + (k - 1) * gridDim.x,
+                           tiles_per_b, T, relu, warp, lane);
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    }
+    if (nk > 0 && !failed) {
+        const int last = (nk - 1) & 1;
+        const bool ok = wait_parity(&mbar[last], phase[last], spin_limit);
+        if (__syncthreads_or(ok ? 0 : 1)) {
+            if (tid == 0) raise(err, EEMD_SG_E_TIMEOUT);
+        } else {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            epilogue<COUT>(tmem + last * ACOLS, sbias, out, mask, blockIdx.x + (nk - 1) * gridDim.x, tiles_per_b, T,
+                           relu, warp, lane);
+        }
+    }
+    cp_wait_all();
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
+    }
+}
+
 // CUDA-core convolution with the same arguments (reference for the tensor-core path)
 __global__ void k_conv_ref(const __nv_bfloat16* __restrict__ in, const __nv_bfloat16* __restrict__ wpk,
                            const float* __restrict__ bias, __nv_bfloat16* out, int B, int T, int cin, int cout,
@@ -617,6 +792,40 @@ __global__ void k_gate(const double* __restrict__ partial, int S, int chunks, in
 using namespace sg;
 
 namespace {
+// the double-buffered kernel: CTAs per SM from shared memory (the carveout
+// at its maximum), tensor-memory columns and threads
+template <int CIN, int COUT>
+int launch_tc2(const void* in, const void* wpk, const float* bias, void* out, int B, int T, int dil, int dir,
+               int relu, const void* mask, int* err, long long spin, cudaStream_t st) {
+    const size_t smem = (size_t)2 * 3 * CIN * TM * 2 + (size_t)3 * CIN * COUT * 2;
+    if (cudaFuncSetAttribute(k_conv_tc2<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_conv_tc2<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100) !=
+            cudaSuccess)
+        return EEMD_SG_E_CUDA;
+    static int resident = 0;
+    if (resident == 0) {
+        int dev = 0, sms = 0, smem_sm = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess)
+            return EEMD_SG_E_CUDA;
+        const int per_block = (int)smem + 1024 + 1024;  // dynamic + static + the per-block reservation
+        int per_sm = smem_sm / per_block;
+        const int tcols = 2 * (COUT < 32 ? 32 : COUT);
+        if (per_sm > 512 / tcols) per_sm = 512 / tcols;
+        if (per_sm > 2048 / NT) per_sm = 2048 / NT;
+        resident = sms * (per_sm > 0 ? per_sm : 1);
+    }
+    const int tiles = B * ((T + TM - 1) / TM);
+    const int grid = tiles < resident ? tiles : resident;
+    k_conv_tc2<CIN, COUT><<<grid, NT, smem, st>>>(static_cast<const __nv_bfloat16*>(in),
+                                                   static_cast<const __nv_bfloat16*>(wpk), bias,
+                                                   static_cast<__nv_bfloat16*>(out), B, T, dil, dir, relu,
+                                                   static_cast<const __nv_bfloat16*>(mask), err, spin);
+    return cudaGetLastError() == cudaSuccess ? EEMD_SG_OK : EEMD_SG_E_CUDA;
+}
+
 template <int CIN, int COUT>
 int launch_tc(const void* in, const void* wpk, const float* bias, void* out, int B, int T, int dil, int dir,
               int relu, const void* mask, int* err, long long spin, cudaStream_t st) {
@@ -666,6 +875,15 @@ int32_t eemd_sg_conv(const void* in, const void* wpk, const float* bias, void* o
         return cudaGetLastError() == cudaSuccess ? EEMD_SG_OK : EEMD_SG_E_CUDA;
     }
     const long long spin = spin_limit > 0 ? spin_limit : (1LL << 24);
+    if (tensor_cores == 2) {
+        if (cin == 64 && cout == 64)
+            return launch_tc2<64, 64>(in, wpk, bias, out, B, T, dil, dir, relu, mask, err, spin, st);
+        if (cin == 16 && cout == 64)
+            return launch_tc2<16, 64>(in, wpk, bias, out, B, T, dil, dir, relu, mask, err, spin, st);
+        if (cin == 64 && cout == 16)
+            return launch_tc2<64, 16>(in, wpk, bias, out, B, T, dil, dir, relu, mask, err, spin, st);
+        return EEMD_SG_E_BADARG;
+    }
     if (cin == 64 && cout == 64) return launch_tc<64, 64>(in, wpk, bias, out, B, T, dil, dir, relu, mask, err, spin, st);
     if (cin == 16 && cout == 64) return launch_tc<16, 64>(in, wpk, bias, out, B, T, dil, dir, relu, mask, err, spin, st);
     if (cin == 64 && cout == 16) return launch_tc<64, 16>(in, wpk, bias, out, B, T, dil, dir, relu, mask, err, spin, st);
