@@ -6,7 +6,10 @@
 // float32 accumulation).  Activations are channels-last, [batch][time][C]
 // with C = 16 (10 IMF channels, zero padded) or 64.
 //
-// Every convolution is an implicit GEMM on the 5th-generation tensor cores:
+// Every convolution is an implicit GEMM on the 5th-generation tensor cores
+// (three forms: k_conv_tc, single-buffered with cp.async staging; k_conv_tc2,
+// double-buffered; k_conv_tma, double-buffered with bulk-tensor loads -- the
+// one the network uses):
 //     D[t][n] = sum_{tap, c} X[t + dir*(tap-1)*dil][c] * W[n][tap*Cin + c]
 // with M = 128 time samples per tile, N = the output channels and
 // K = 3*Cin.  The CTA stages the three shifted copies of its input tile
@@ -22,6 +25,7 @@
 // The weight gradient, the loss, Adam and the packing kernels run on CUDA
 // cores.  A plain CUDA-core convolution with the same arguments is kept for
 // checking the tensor-core path on the GPU.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
@@ -412,6 +416,157 @@ __global__ void __launch_bounds__(NT) k_conv_tc2(const __nv_bfloat16* __restrict
     }
 }
 
+// ---------------------------------------------------------------------------
+// TMA-fed variant.  The input is a 3-D tensor map [B][T][CIN] (bf16, box
+// {8 channels, 128 samples, 1}); one tile's A operand is 3*CIN/8 boxes, each
+// exactly one K-chunk column of the K-major no-swizzle layout (128 rows x
+// 16 bytes), issued by one thread with cp.async.bulk.tensor and counted on a
+// transaction mbarrier.  Rows outside [0, T) of the signal are zero-filled by
+// the tensor map's bounds (the channel coordinate is a multiple of 8, so every
+// box starts on a 16-byte boundary).  Pipeline as k_conv_tc2: two input
+// buffers, two tensor-memory accumulators, the epilogue of tile k-1 overlaps
+// MMA k and the loads of tile k+1.  No multicast.
+// ---------------------------------------------------------------------------
+template <int CIN>
+__device__ __forceinline__ void tma_tile(const CUtensorMap* tmap, uint32_t dst, uint64_t* full, int tile,
+                                         int tiles_per_b, int dil, int dir) {
+    constexpr uint32_t BYTES = 3u * CIN * TM * 2u;
+    const int b = tile / tiles_per_b, t0 = (tile % tiles_per_b) * TM;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(full)), "r"(BYTES)
+                 : "memory");
+#pragma unroll
+    for (int tap = 0; tap < 3; ++tap) {
+        const int ts = t0 + dir * (tap - 1) * dil;
+#pragma unroll
+        for (int kc = 0; kc < CIN / 8; ++kc) {
+            const uint32_t d = dst + (uint32_t)((tap * (CIN / 8) + kc) * TM * 16);
+            asm volatile(
+                "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+                "[%5];\n" ::"r"(d),
+                "l"(reinterpret_cast<uint64_t>(tmap)), "r"(kc * 8), "r"(ts), "r"(b), "r"(smem_u32(full))
+                : "memory");
+        }
+    }
+}
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(NT) k_conv_tma(const __grid_constant__ CUtensorMap tmap,
+                                                 const __nv_bfloat16* __restrict__ wpk,
+                                                 const float* __restrict__ bias, __nv_bfloat16* out, int B, int T,
+                                                 int dil, int dir, int relu, const __nv_bfloat16* __restrict__ mask,
+                                                 int* err, long long spin_limit) {
+    constexpr int K = 3 * CIN;
+    constexpr int KSTEPS = K / 16;
+    constexpr int A_BYTES = K * TM * 2;
+    constexpr int B_BYTES = K * COUT * 2;
+    constexpr int ACOLS = COUT < 32 ? 32 : COUT;
+    constexpr int TCOLS = 2 * ACOLS;
+    static_assert(CIN % 16 == 0 && COUT % 16 == 0 && TCOLS <= 512, "shape");
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t full[2];
+    __shared__ __align__(8) uint64_t mmad[2];
+    __shared__ uint32_t tmem_slot;
+    __shared__ float sbias[COUT];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int i = tid; i < COUT; i += NT) sbias[i] = bias ? bias[i] : 0.f;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                         smem_u32(&tmem_slot)),
+                     "r"(TCOLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        for (int i = 0; i < 2; ++i) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&full[i])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mmad[i])));
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    const int tiles_per_b = (T + TM - 1) / TM;
+    const int n_tiles = B * tiles_per_b;
+    const uint32_t a_base = smem_u32(smem), b_base = a_base + 2 * A_BYTES;
+    // the bulk-tensor copies need 128-byte aligned destinations: refuse to run otherwise
+    const bool aligned = (a_base & 127u) == 0;
+    if (!aligned && tid == 0) raise(err, EEMD_SG_E_BADARG);
+    const int nk = (aligned && blockIdx.x < n_tiles) ? (n_tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    // the packed weights once (ordinary copies, then made visible to the async proxy)
+    for (int i = tid; i < B_BYTES / 16; i += NT) cp16(smem + 2 * A_BYTES + 16 * i, wpk + 8 * i, 16);
+    cp_commit();
+    cp_wait_all();
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    constexpr uint32_t IDESC = instr_desc(TM, COUT);
+    if (tid == 0 && nk > 0) tma_tile<CIN>(&tmap, a_base, &full[0], blockIdx.x, tiles_per_b, dil, dir);
+    uint32_t fph[2] = {0u, 0u}, mph[2] = {0u, 0u};
+    bool failed = false;
+    for (int k = 0; k < nk; ++k) {
+        const int buf = k & 1;
+        if (k >= 1) {
+            if (!wait_parity(&mmad[buf ^ 1], mph[buf ^ 1], spin_limit)) failed = true;
+            mph[buf ^ 1] ^= 1u;
+        }
+        if (__syncthreads_or(failed ? 1 : 0)) {
+            if (tid == 0) raise(err, EEMD_SG_E_TIMEOUT);
+            break;
+        }
+        if (tid == 0) {
+            if (k + 1 < nk)
+                tma_tile<CIN>(&tmap, a_base + (buf ^ 1) * A_BYTES, &full[buf ^ 1],
+                              blockIdx.x + (k + 1) * gridDim.x, tiles_per_b, dil, dir);
+            if (!wait_parity(&full[buf], fph[buf], spin_limit)) {
+                failed = true;
+            } else {
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                const uint32_t a_buf = a_base + buf * A_BYTES;
+#pragma unroll
+                for (int s2 = 0; s2 < KSTEPS; ++s2) {
+                    const uint64_t da = smem_desc(a_buf + s2 * 2 * (TM * 16), TM * 16, 128);
+                    const uint64_t db = smem_desc(b_base + s2 * 2 * (COUT * 16), COUT * 16, 128);
+                    const uint32_t acc = s2 > 0 ? 1u : 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem + buf * ACOLS),
+                        "l"(da), "l"(db), "r"(IDESC), "r"(acc));
+                }
+                asm volatile(
+                    "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                        smem_u32(&mmad[buf]))
+                    : "memory");
+            }
+            fph[buf] ^= 1u;
+        }
+        __syncwarp();
+        if (k >= 1) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            epilogue<COUT>(tmem + (buf ^ 1) * ACOLS, sbias, out, mask, blockIdx.x + (k - 1) * gridDim.x,
+                           tiles_per_b, T, relu, warp, lane);
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    }
+    if (__syncthreads_or(failed ? 1 : 0)) {
+        if (tid == 0) raise(err, EEMD_SG_E_TIMEOUT);
+    } else if (nk > 0) {
+        const int last = (nk - 1) & 1;
+        const bool ok = wait_parity(&mmad[last], mph[last], spin_limit);
+        if (__syncthreads_or(ok ? 0 : 1)) {
+            if (tid == 0) raise(err, EEMD_SG_E_TIMEOUT);
+        } else {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            epilogue<COUT>(tmem + last * ACOLS, sbias, out, mask, blockIdx.x + (nk - 1) * gridDim.x, tiles_per_b, T,
+                           relu, warp, lane);
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
+    }
+}
+
 // CUDA-core convolution with the same arguments (reference for the tensor-core path)
 __global__ void k_conv_ref(const __nv_bfloat16* __restrict__ in, const __nv_bfloat16* __restrict__ wpk,
                            const float* __restrict__ bias, __nv_bfloat16* out, int B, int T, int cin, int cout,
@@ -792,6 +947,65 @@ __global__ void k_gate(const double* __restrict__ partial, int S, int chunks, in
 using namespace sg;
 
 namespace {
+// 3-D tensor map of the input [B][T][CIN] bf16 with the box {8, 128, 1}
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int input_map(CUtensorMap* m, const void* in, int B, int T, int CIN) {
+    static EncodeTiled encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return EEMD_SG_E_CUDA;
+        encode = reinterpret_cast<EncodeTiled>(fn);
+    }
+    if ((reinterpret_cast<uintptr_t>(in) & 15) != 0) return EEMD_SG_E_BADARG;  // a tensor map needs 16-byte alignment
+    const cuuint64_t dims[3] = {(cuuint64_t)CIN, (cuuint64_t)T, (cuuint64_t)B};
+    const cuuint64_t strides[2] = {(cuuint64_t)CIN * 2, (cuuint64_t)T * CIN * 2};
+    const cuuint32_t box[3] = {8, (cuuint32_t)TM, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(in), dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? EEMD_SG_OK : EEMD_SG_E_CUDA;
+}
+
+template <int CIN, int COUT>
+int launch_tma(const void* in, const void* wpk, const float* bias, void* out, int B, int T, int dil, int dir,
+               int relu, const void* mask, int* err, long long spin, cudaStream_t st) {
+    const size_t smem = (size_t)2 * 3 * CIN * TM * 2 + (size_t)3 * CIN * COUT * 2;
+    if (cudaFuncSetAttribute(k_conv_tma<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_conv_tma<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100) !=
+            cudaSuccess)
+        return EEMD_SG_E_CUDA;
+    CUtensorMap m;
+    const int rc = input_map(&m, in, B, T, CIN);
+    if (rc) return rc;
+    static int resident = 0;
+    if (resident == 0) {
+        int dev = 0, sms = 0, smem_sm = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess)
+            return EEMD_SG_E_CUDA;
+        int per_sm = smem_sm / ((int)smem + 2048);
+        const int tcols = 2 * (COUT < 32 ? 32 : COUT);
+        if (per_sm > 512 / tcols) per_sm = 512 / tcols;
+        if (per_sm > 2048 / NT) per_sm = 2048 / NT;
+        resident = sms * (per_sm > 0 ? per_sm : 1);
+    }
+    const int tiles = B * ((T + TM - 1) / TM);
+    const int grid = tiles < resident ? tiles : resident;
+    k_conv_tma<CIN, COUT><<<grid, NT, smem, st>>>(m, static_cast<const __nv_bfloat16*>(wpk), bias,
+                                                   static_cast<__nv_bfloat16*>(out), B, T, dil, dir, relu,
+                                                   static_cast<const __nv_bfloat16*>(mask), err, spin);
+    return cudaGetLastError() == cudaSuccess ? EEMD_SG_OK : EEMD_SG_E_CUDA;
+}
+
 // the double-buffered kernel: CTAs per SM from shared memory (the carveout
 // at its maximum), tensor-memory columns and threads
 template <int CIN, int COUT>
@@ -875,6 +1089,15 @@ int32_t eemd_sg_conv(const void* in, const void* wpk, const float* bias, void* o
         return cudaGetLastError() == cudaSuccess ? EEMD_SG_OK : EEMD_SG_E_CUDA;
     }
     const long long spin = spin_limit > 0 ? spin_limit : (1LL << 24);
+    if (tensor_cores == 3) {
+        if (cin == 64 && cout == 64)
+            return launch_tma<64, 64>(in, wpk, bias, out, B, T, dil, dir, relu, mask, err, spin, st);
+        if (cin == 16 && cout == 64)
+            return launch_tma<16, 64>(in, wpk, bias, out, B, T, dil, dir, relu, mask, err, spin, st);
+        if (cin == 64 && cout == 16)
+            return launch_tma<64, 16>(in, wpk, bias, out, B, T, dil, dir, relu, mask, err, spin, st);
+        return EEMD_SG_E_BADARG;
+    }
     if (tensor_cores == 2) {
         if (cin == 64 && cout == 64)
             return launch_tc2<64, 64>(in, wpk, bias, out, B, T, dil, dir, relu, mask, err, spin, st);

@@ -37,8 +37,10 @@ int32_t eemd_sg_version(void);
  * non-null mask ([b][t][cout] bf16) zeroes entries whose mask is not > 0
  * (the ReLU derivative).  tensor_cores = 1 runs the tcgen05 implicit GEMM,
  * 2 its double-buffered form (the next tile's copies and the previous tile's
- * epilogue overlap the MMA; same results bit for bit), 0 a CUDA-core
- * reference kernel with identical semantics.  *err (device,
+ * epilogue overlap the MMA), 3 the double-buffered form fed by bulk-tensor
+ * (TMA) copies of a 3-D tensor map over x (x must be 16-byte aligned); all
+ * three give the same results bit for bit.  0 runs a CUDA-core reference
+ * kernel with identical semantics.  *err (device,
  * may be null) receives EEMD_SG_E_TIMEOUT if a tensor-core wait gives up
  * after spin_limit polls (0: default). */
 int32_t eemd_sg_conv(const void* x, const void* w_packed, const float* bias, void* y, int32_t B, int32_t T,

@@ -126,10 +126,11 @@ def test_loss_and_adam():
 
 @pytest.mark.parametrize("cin,cout", [(16, 64), (64, 64), (64, 16)])
 @pytest.mark.parametrize("dil", [1, 13, 128])
-def test_double_buffered_kernel_equals_single_buffered(cin, cout, dil):
+def test_double_buffered_kernels_equal_single_buffered(cin, cout, dil):
     """tensor_cores=2 (two input buffers and accumulators, epilogue of tile
-    k-1 overlapping MMA k) against tensor_cores=1, forward and masked input
-    gradient, with more tiles than CTAs and a ragged last tile."""
+    k-1 overlapping MMA k) and 3 (the same fed by bulk-tensor copies) against
+    tensor_cores=1, forward and masked input gradient, with more tiles than
+    CTAs, a ragged last tile and halo rows outside the signal."""
     rng = np.random.default_rng(100 + cin + cout + dil)
     B, T = 8, 10000
     x = rng.standard_normal((B, T, cin)).astype(np.float32)
@@ -139,23 +140,23 @@ def test_double_buffered_kernel_equals_single_buffered(cin, cout, dil):
     wp = packed(w, cout, cin)
     err = torch.zeros((1,), dtype=torch.int32, device="cuda")
     ys = []
-    for mode in (1, 2):
+    for mode in (1, 2, 3):
         y = torch.full((B, T, cout), 7.0, dtype=torch.bfloat16, device="cuda")
         _sg.conv(xd, wp, bd, y, B, T, cin, cout, dil, relu=True, tensor_cores=mode, err=err)
         ys.append(y)
     torch.cuda.synchronize()
     assert int(err.item()) == 0
-    assert torch.equal(ys[0], ys[1])
+    assert torch.equal(ys[0], ys[1]) and torch.equal(ys[0], ys[2])
     # masked input gradient
     dy = rng.standard_normal((B, T, cout)).astype(np.float32)
     mask = (rng.random((B, T, cin)) > 0.3).astype(np.float32)
     wpt = packed(w, cin, cout, transpose=True)
     gs = []
-    for mode in (1, 2):
+    for mode in (1, 2, 3):
         g = torch.full((B, T, cin), 7.0, dtype=torch.bfloat16, device="cuda")
         _sg.conv(bf16(dy).cuda(), wpt, None, g, B, T, cout, cin, dil, direction=-1, mask=bf16(mask).cuda(),
                  tensor_cores=mode, err=err)
         gs.append(g)
     torch.cuda.synchronize()
     assert int(err.item()) == 0
-    assert torch.equal(gs[0], gs[1])
+    assert torch.equal(gs[0], gs[1]) and torch.equal(gs[0], gs[2])
