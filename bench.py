@@ -695,6 +695,9 @@ def run_surrogate(args):
     ens_ms, stage_ms, net_ms = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2]), ev[2].elapsed_time(ev[3])
     launches = sum(v["launches"] for v in kt.as_dict().values()) + sur.launches_per_run(S)
     flops = SU.network_flops_per_sample() * S * N
+    # bytes of the pass: every layer reads its input and writes its output once (bf16, padded channels)
+    net_bytes = sum((lay["cin_p"] + lay["cout_p"]) * 2 for lay in net.layers) * S * N
+    hbm_peak, hbm_kind = measured_peak_hbm()
     n_conv = len(SU.DILATIONS) * ((S + sur.chunk - 1) // sur.chunk)
     tflops = flops / (net_ms / 1e3) / 1e12
     peak, peak_kind = measured_peak_bf16()
@@ -779,10 +782,15 @@ def run_surrogate(args):
                 "h2d_bytes_per_step": S * N * 4, "d2h_bytes_per_step": S * (K + 1) * N * 8 + S * 3 * 8 + S * 4,
                 "fallbacks": nf},
         "gpu_launches": launches * args.steps,
-        "roofline": {"bound": "tensor", "kernel": "k_conv_tc", "achieved": round(tflops, 2), "peak": peak,
+        "roofline": {"bound": "tensor", "kernel": "k_conv_tma", "achieved": round(tflops, 2), "peak": peak,
                      "peak_kind": peak_kind, "unit": "TFLOP/s", "frac": round(tflops * 1e12 / (peak * 1e12), 4),
                      "traffic": None, "algorithmic_flops_per_launch": round(flops / n_conv),
                      "avg_launch_ms": round(net_ms / n_conv, 5)},
+        # one 64-channel layer does 96 FLOP per byte, below the ridge: the layer's own bound is HBM
+        "roofline_hbm": {"bound": "hbm", "kernel": "k_conv_tma", "achieved": round(net_bytes / (net_ms / 1e3) / 1e9, 2),
+                         "peak": hbm_peak, "peak_kind": hbm_kind, "unit": "GB/s",
+                         "frac": round(net_bytes / (net_ms / 1e3) / 1e9 / hbm_peak, 4),
+                         "algorithmic_bytes_per_pass": net_bytes},
         "clocks": clocks,
     }
     if cpu is not None:
