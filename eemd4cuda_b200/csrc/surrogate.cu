@@ -423,10 +423,19 @@ __global__ void __launch_bounds__(NT) k_conv_tc2(const __nv_bfloat16* __restrict
 // 16 bytes), issued by one thread with cp.async.bulk.tensor and counted on a
 // transaction mbarrier.  Rows outside [0, T) of the signal are zero-filled by
 // the tensor map's bounds (the channel coordinate is a multiple of 8, so every
-// box starts on a 16-byte boundary).  Pipeline as k_conv_tc2: two input
-// buffers, two tensor-memory accumulators, the epilogue of tile k-1 overlaps
-// MMA k and the loads of tile k+1.  No multicast.
+// box starts on a 16-byte boundary).  Pipeline: TMA_STAGES input buffers
+// (tiles k+1 .. k+TMA_STAGES-1 in flight while tile k is multiplied), two
+// tensor-memory accumulators, the epilogue of tile k-1 overlapping MMA k.
+// No multicast.
 // ---------------------------------------------------------------------------
+// input-tile buffers of k_conv_tma (tiles in flight while one is multiplied);
+// 3 measured no faster than 2 (1.364 vs 1.349 ms for the 8-layer pass over
+// 16 x 65536 samples): the copies are not what each tile waits for
+#ifndef EEMD_SG_TMA_STAGES
+#define EEMD_SG_TMA_STAGES 2
+#endif
+constexpr int TMA_STAGES = EEMD_SG_TMA_STAGES;
+
 template <int CIN>
 __device__ __forceinline__ void tma_tile(const CUtensorMap* tmap, uint32_t dst, uint64_t* full, int tile,
                                          int tiles_per_b, int dil, int dir) {
@@ -459,11 +468,12 @@ __global__ void __launch_bounds__(NT) k_conv_tma(const __grid_constant__ CUtenso
     constexpr int KSTEPS = K / 16;
     constexpr int A_BYTES = K * TM * 2;
     constexpr int B_BYTES = K * COUT * 2;
+    constexpr int NBUF = TMA_STAGES;              // input tiles in flight + the one being multiplied
     constexpr int ACOLS = COUT < 32 ? 32 : COUT;
     constexpr int TCOLS = 2 * ACOLS;
     static_assert(CIN % 16 == 0 && COUT % 16 == 0 && TCOLS <= 512, "shape");
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) uint64_t full[2];
+    __shared__ __align__(8) uint64_t full[NBUF];
     __shared__ __align__(8) uint64_t mmad[2];
     __shared__ uint32_t tmem_slot;
     __shared__ float sbias[COUT];
@@ -476,21 +486,19 @@ __global__ void __launch_bounds__(NT) k_conv_tma(const __grid_constant__ CUtenso
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
     }
     if (tid == 0) {
-        for (int i = 0; i < 2; ++i) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&full[i])));
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mmad[i])));
-        }
+        for (int i = 0; i < NBUF; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&full[i])));
+        for (int i = 0; i < 2; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mmad[i])));
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     const int tiles_per_b = (T + TM - 1) / TM;
     const int n_tiles = B * tiles_per_b;
-    const uint32_t a_base = smem_u32(smem), b_base = a_base + 2 * A_BYTES;
+    const uint32_t a_base = smem_u32(smem), b_base = a_base + NBUF * A_BYTES;
     // the bulk-tensor copies need 128-byte aligned destinations: refuse to run otherwise
     const bool aligned = (a_base & 127u) == 0;
     if (!aligned && tid == 0) raise(err, EEMD_SG_E_BADARG);
     const int nk = (aligned && blockIdx.x < n_tiles) ? (n_tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
     // the packed weights once (ordinary copies, then made visible to the async proxy)
-    for (int i = tid; i < B_BYTES / 16; i += NT) cp16(smem + 2 * A_BYTES + 16 * i, wpk + 8 * i, 16);
+    for (int i = tid; i < B_BYTES / 16; i += NT) cp16(smem + NBUF * A_BYTES + 16 * i, wpk + 8 * i, 16);
     cp_commit();
     cp_wait_all();
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -499,28 +507,43 @@ __global__ void __launch_bounds__(NT) k_conv_tma(const __grid_constant__ CUtenso
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const uint32_t tmem = tmem_slot;
     constexpr uint32_t IDESC = instr_desc(TM, COUT);
-    if (tid == 0 && nk > 0) tma_tile<CIN>(&tmap, a_base, &full[0], blockIdx.x, tiles_per_b, dil, dir);
-    uint32_t fph[2] = {0u, 0u}, mph[2] = {0u, 0u};
+    // tiles 0 .. NBUF-2 in flight before the loop
+    if (tid == 0)
+        for (int j = 0; j < NBUF - 1 && j < nk; ++j)
+            tma_tile<CIN>(&tmap, a_base + j * A_BYTES, &full[j], blockIdx.x + j * gridDim.x, tiles_per_b, dil, dir);
+    uint32_t fph[NBUF], mph[2] = {0u, 0u};
+#pragma unroll
+    for (int i = 0; i < NBUF; ++i) fph[i] = 0u;
     bool failed = false;
+    int ib = 0;  // input buffer of tile k (k mod NBUF)
     for (int k = 0; k < nk; ++k) {
-        const int buf = k & 1;
+        const int acc_b = k & 1;
         if (k >= 1) {
-            if (!wait_parity(&mmad[buf ^ 1], mph[buf ^ 1], spin_limit)) failed = true;
-            mph[buf ^ 1] ^= 1u;
+            // MMA(k-1): its accumulator complete, its input buffer free
+            if (!wait_parity(&mmad[acc_b ^ 1], mph[acc_b ^ 1], spin_limit)) failed = true;
+            mph[acc_b ^ 1] ^= 1u;
         }
         if (__syncthreads_or(failed ? 1 : 0)) {
             if (tid == 0) raise(err, EEMD_SG_E_TIMEOUT);
             break;
         }
         if (tid == 0) {
-            if (k + 1 < nk)
-                tma_tile<CIN>(&tmap, a_base + (buf ^ 1) * A_BYTES, &full[buf ^ 1],
-                              blockIdx.x + (k + 1) * gridDim.x, tiles_per_b, dil, dir);
-            if (!wait_parity(&full[buf], fph[buf], spin_limit)) {
+            // tile k+NBUF-1 into the buffer MMA(k-1) used (the last free one)
+            const int kn = k + NBUF - 1;
+            if (kn < nk) {
+                const int nb = ib == 0 ? NBUF - 1 : ib - 1;
+                tma_tile<CIN>(&tmap, a_base + nb * A_BYTES, &full[nb], blockIdx.x + kn * gridDim.x, tiles_per_b,
+                              dil, dir);
+            }
+            uint32_t ph = 0;
+#pragma unroll
+            for (int i = 0; i < NBUF; ++i)
+                if (i == ib) ph = fph[i];
+            if (!wait_parity(&full[ib], ph, spin_limit)) {
                 failed = true;
             } else {
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-                const uint32_t a_buf = a_base + buf * A_BYTES;
+                const uint32_t a_buf = a_base + ib * A_BYTES;
 #pragma unroll
                 for (int s2 = 0; s2 < KSTEPS; ++s2) {
                     const uint64_t da = smem_desc(a_buf + s2 * 2 * (TM * 16), TM * 16, 128);
@@ -528,23 +551,26 @@ __global__ void __launch_bounds__(NT) k_conv_tma(const __grid_constant__ CUtenso
                     const uint32_t acc = s2 > 0 ? 1u : 0u;
                     asm volatile(
                         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem + buf * ACOLS),
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem + acc_b * ACOLS),
                         "l"(da), "l"(db), "r"(IDESC), "r"(acc));
                 }
                 asm volatile(
                     "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                        smem_u32(&mmad[buf]))
+                        smem_u32(&mmad[acc_b]))
                     : "memory");
             }
-            fph[buf] ^= 1u;
+#pragma unroll
+            for (int i = 0; i < NBUF; ++i)
+                if (i == ib) fph[i] ^= 1u;
         }
         __syncwarp();
         if (k >= 1) {
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            epilogue<COUT>(tmem + (buf ^ 1) * ACOLS, sbias, out, mask, blockIdx.x + (k - 1) * gridDim.x,
+            epilogue<COUT>(tmem + (acc_b ^ 1) * ACOLS, sbias, out, mask, blockIdx.x + (k - 1) * gridDim.x,
                            tiles_per_b, T, relu, warp, lane);
         }
         asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+        ib = ib + 1 == NBUF ? 0 : ib + 1;
     }
     if (__syncthreads_or(failed ? 1 : 0)) {
         if (tid == 0) raise(err, EEMD_SG_E_TIMEOUT);
@@ -976,7 +1002,7 @@ int input_map(CUtensorMap* m, const void* in, int B, int T, int CIN) {
 template <int CIN, int COUT>
 int launch_tma(const void* in, const void* wpk, const float* bias, void* out, int B, int T, int dil, int dir,
                int relu, const void* mask, int* err, long long spin, cudaStream_t st) {
-    const size_t smem = (size_t)2 * 3 * CIN * TM * 2 + (size_t)3 * CIN * COUT * 2;
+    const size_t smem = (size_t)TMA_STAGES * 3 * CIN * TM * 2 + (size_t)3 * CIN * COUT * 2;
     if (cudaFuncSetAttribute(k_conv_tma<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
             cudaSuccess ||
         cudaFuncSetAttribute(k_conv_tma<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100) !=
