@@ -280,6 +280,53 @@ __device__ __forceinline__ bool wait_parity(uint64_t* bar, uint32_t phase, long 
     return true;
 }
 
+// columns [c0, c0 + NC) of this warp's 32 accumulator lanes (NC a multiple of 8)
+template <int NC>
+__device__ __forceinline__ void tmem_ld_cols(uint32_t taddr, float (&v)[NC]) {
+    static_assert(NC % 8 == 0, "columns");
+#pragma unroll
+    for (int q = 0; q < NC / 8; ++q) {
+        uint32_t r[8];
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                       "=r"(r[7])
+                     : "r"(taddr + 8u * q));
+#pragma unroll
+        for (int i = 0; i < 8; ++i) v[8 * q + i] = __uint_as_float(r[i]);
+    }
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+// epilogue of a column slice: warp `warp` reads lane quadrant warp % 4 and
+// columns [(warp / 4) * NC, +NC) of the accumulator at taddr
+template <int COUT, int NC>
+__device__ __forceinline__ void epilogue_cols(uint32_t taddr, const float* sbias, __nv_bfloat16* out,
+                                              const __nv_bfloat16* __restrict__ mask, int tile, int tiles_per_b,
+                                              int T, int relu, int warp, int lane) {
+    const int quad = warp & 3, c_base = (warp >> 2) * NC;
+    float v[NC];
+    tmem_ld_cols<NC>(taddr + ((uint32_t)(32 * quad) << 16) + (uint32_t)c_base, v);
+    const int b = tile / tiles_per_b, t = (tile % tiles_per_b) * TM + 32 * quad + lane;
+    if (t >= T) return;
+    __nv_bfloat16* o = out + ((size_t)b * T + t) * COUT + c_base;
+    const __nv_bfloat16* mk = mask ? mask + ((size_t)b * T + t) * COUT + c_base : nullptr;
+#pragma unroll
+    for (int c0 = 0; c0 < NC; c0 += 8) {
+        __align__(16) __nv_bfloat16 h[8];
+        uint4 mv = make_uint4(0, 0, 0, 0);
+        if (mk) mv = *reinterpret_cast<const uint4*>(mk + c0);
+        const __nv_bfloat16* mh = reinterpret_cast<const __nv_bfloat16*>(&mv);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            float x = v[c0 + i] + sbias[c_base + c0 + i];
+            if (relu) x = fmaxf(x, 0.f);
+            if (mk && !(__bfloat162float(mh[i]) > 0.f)) x = 0.f;
+            h[i] = __float2bfloat16(x);
+        }
+        *reinterpret_cast<uint4*>(o + c0) = *reinterpret_cast<const uint4*>(h);
+    }
+}
+
 template <int COUT>
 __device__ __forceinline__ void epilogue(uint32_t taddr, const float* sbias, __nv_bfloat16* out,
                                          const __nv_bfloat16* __restrict__ mask, int tile, int tiles_per_b, int T,
@@ -435,6 +482,12 @@ __global__ void __launch_bounds__(NT) k_conv_tc2(const __nv_bfloat16* __restrict
 #define EEMD_SG_TMA_STAGES 2
 #endif
 constexpr int TMA_STAGES = EEMD_SG_TMA_STAGES;
+// warps of k_conv_tma: 4 (one per accumulator lane quadrant) or 8 (two per
+// quadrant, each reading half the columns in the epilogue)
+#ifndef EEMD_SG_TMA_EPI_WARPS
+#define EEMD_SG_TMA_EPI_WARPS 8
+#endif
+constexpr int TMA_EPI_WARPS = EEMD_SG_TMA_EPI_WARPS;
 
 template <int CIN>
 __device__ __forceinline__ void tma_tile(const CUtensorMap* tmap, uint32_t dst, uint64_t* full, int tile,
@@ -458,8 +511,8 @@ __device__ __forceinline__ void tma_tile(const CUtensorMap* tmap, uint32_t dst, 
     }
 }
 
-template <int CIN, int COUT>
-__global__ void __launch_bounds__(NT) k_conv_tma(const __grid_constant__ CUtensorMap tmap,
+template <int CIN, int COUT, int EW>
+__global__ void __launch_bounds__(32 * EW) k_conv_tma(const __grid_constant__ CUtensorMap tmap,
                                                  const __nv_bfloat16* __restrict__ wpk,
                                                  const float* __restrict__ bias, __nv_bfloat16* out, int B, int T,
                                                  int dil, int dir, int relu, const __nv_bfloat16* __restrict__ mask,
@@ -471,14 +524,15 @@ __global__ void __launch_bounds__(NT) k_conv_tma(const __grid_constant__ CUtenso
     constexpr int NBUF = TMA_STAGES;              // input tiles in flight + the one being multiplied
     constexpr int ACOLS = COUT < 32 ? 32 : COUT;
     constexpr int TCOLS = 2 * ACOLS;
-    static_assert(CIN % 16 == 0 && COUT % 16 == 0 && TCOLS <= 512, "shape");
+    constexpr int THR = 32 * EW;                  // EW = 4: one warp per lane quadrant; 8: two, each half the columns
+    static_assert(CIN % 16 == 0 && COUT % 16 == 0 && TCOLS <= 512 && (EW == 4 || EW == 8), "shape");
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t full[NBUF];
     __shared__ __align__(8) uint64_t mmad[2];
     __shared__ uint32_t tmem_slot;
     __shared__ float sbias[COUT];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    for (int i = tid; i < COUT; i += NT) sbias[i] = bias ? bias[i] : 0.f;
+    for (int i = tid; i < COUT; i += THR) sbias[i] = bias ? bias[i] : 0.f;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                          smem_u32(&tmem_slot)),
@@ -498,7 +552,7 @@ __global__ void __launch_bounds__(NT) k_conv_tma(const __grid_constant__ CUtenso
     if (!aligned && tid == 0) raise(err, EEMD_SG_E_BADARG);
     const int nk = (aligned && blockIdx.x < n_tiles) ? (n_tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
     // the packed weights once (ordinary copies, then made visible to the async proxy)
-    for (int i = tid; i < B_BYTES / 16; i += NT) cp16(smem + NBUF * A_BYTES + 16 * i, wpk + 8 * i, 16);
+    for (int i = tid; i < B_BYTES / 16; i += THR) cp16(smem + NBUF * A_BYTES + 16 * i, wpk + 8 * i, 16);
     cp_commit();
     cp_wait_all();
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -566,7 +620,7 @@ __global__ void __launch_bounds__(NT) k_conv_tma(const __grid_constant__ CUtenso
         __syncwarp();
         if (k >= 1) {
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            epilogue<COUT>(tmem + (acc_b ^ 1) * ACOLS, sbias, out, mask, blockIdx.x + (k - 1) * gridDim.x,
+            epilogue_cols<COUT, COUT * 4 / EW>(tmem + (acc_b ^ 1) * ACOLS, sbias, out, mask, blockIdx.x + (k - 1) * gridDim.x,
                            tiles_per_b, T, relu, warp, lane);
         }
         asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -581,7 +635,7 @@ __global__ void __launch_bounds__(NT) k_conv_tma(const __grid_constant__ CUtenso
             if (tid == 0) raise(err, EEMD_SG_E_TIMEOUT);
         } else {
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            epilogue<COUT>(tmem + last * ACOLS, sbias, out, mask, blockIdx.x + (nk - 1) * gridDim.x, tiles_per_b, T,
+            epilogue_cols<COUT, COUT * 4 / EW>(tmem + last * ACOLS, sbias, out, mask, blockIdx.x + (nk - 1) * gridDim.x, tiles_per_b, T,
                            relu, warp, lane);
         }
     }
@@ -1003,9 +1057,10 @@ template <int CIN, int COUT>
 int launch_tma(const void* in, const void* wpk, const float* bias, void* out, int B, int T, int dil, int dir,
                int relu, const void* mask, int* err, long long spin, cudaStream_t st) {
     const size_t smem = (size_t)TMA_STAGES * 3 * CIN * TM * 2 + (size_t)3 * CIN * COUT * 2;
-    if (cudaFuncSetAttribute(k_conv_tma<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+    constexpr int EW = TMA_EPI_WARPS;
+    if (cudaFuncSetAttribute(k_conv_tma<CIN, COUT, EW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
             cudaSuccess ||
-        cudaFuncSetAttribute(k_conv_tma<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100) !=
+        cudaFuncSetAttribute(k_conv_tma<CIN, COUT, EW>, cudaFuncAttributePreferredSharedMemoryCarveout, 100) !=
             cudaSuccess)
         return EEMD_SG_E_CUDA;
     CUtensorMap m;
@@ -1021,12 +1076,12 @@ int launch_tma(const void* in, const void* wpk, const float* bias, void* out, in
         int per_sm = smem_sm / ((int)smem + 2048);
         const int tcols = 2 * (COUT < 32 ? 32 : COUT);
         if (per_sm > 512 / tcols) per_sm = 512 / tcols;
-        if (per_sm > 2048 / NT) per_sm = 2048 / NT;
+        if (per_sm > 2048 / (32 * EW)) per_sm = 2048 / (32 * EW);
         resident = sms * (per_sm > 0 ? per_sm : 1);
     }
     const int tiles = B * ((T + TM - 1) / TM);
     const int grid = tiles < resident ? tiles : resident;
-    k_conv_tma<CIN, COUT><<<grid, NT, smem, st>>>(m, static_cast<const __nv_bfloat16*>(wpk), bias,
+    k_conv_tma<CIN, COUT, EW><<<grid, 32 * EW, smem, st>>>(m, static_cast<const __nv_bfloat16*>(wpk), bias,
                                                    static_cast<__nv_bfloat16*>(out), B, T, dil, dir, relu,
                                                    static_cast<const __nv_bfloat16*>(mask), err, spin);
     return cudaGetLastError() == cudaSuccess ? EEMD_SG_OK : EEMD_SG_E_CUDA;
