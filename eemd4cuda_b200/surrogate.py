@@ -452,6 +452,19 @@ class SurrogateEEMD:
                    self.partial, self.cps, S, N, K, CH, P_CORR, self.recon_bound, self.io_bound, self.metrics,
                    self.fallback, io_relative=self.io_relative)
 
+    def _host_buffers(self):
+        """Pinned host staging for decompose (allocated at its first call):
+        the signals in, the served modes, residuals and gate results out."""
+        if getattr(self, "_hbuf", None) is None:
+            torch = self.torch
+            pin = dict(pin_memory=True)
+            self._hbuf = dict(x=torch.empty((self.S * self.N,), dtype=torch.float32, **pin),
+                              imfs=torch.empty((self.S, self.K, self.N), dtype=torch.float64, **pin),
+                              resid=torch.empty((self.S, self.N), dtype=torch.float64, **pin),
+                              met=torch.empty((self.S, 4), dtype=torch.float64, **pin),
+                              fb=torch.empty((self.S,), dtype=torch.int32, **pin))
+        return self._hbuf
+
     def launches_per_run(self, S) -> int:
         """Kernels of libeemd_surrogate.so per run (the engine's are counted by the engine)."""
         return 2 + len(DILATIONS) * ((S + self.chunk - 1) // self.chunk) + 2
@@ -464,13 +477,20 @@ class SurrogateEEMD:
         S = len(xs)
         if S > self.S or any(len(x) != self.N for x in xs):
             raise ValueError(f"at most {self.S} signals of {self.N} samples")
-        self.xd[:S * self.N].copy_(torch.from_numpy(np.concatenate([np.asarray(x, np.float32) for x in xs])))
+        hb = self._host_buffers()
+        n = S * self.N
+        hb["x"][:n].numpy()[:] = np.concatenate([np.asarray(x, np.float32) for x in xs])
+        self.xd[:n].copy_(hb["x"][:n], non_blocking=True)
         self.run(S)
+        for name, d in (("imfs", self.imfs), ("resid", self.resid), ("met", self.metrics), ("fb", self.fallback)):
+            hb[name][:S].copy_(d[:S], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
         self.net.check()
-        imfs = self.imfs[:S].cpu().numpy()
-        resid = self.resid[:S].cpu().numpy()
-        met = self.metrics[:S].cpu().numpy()
-        fb = self.fallback[:S].cpu().numpy().astype(bool)
+        # fresh arrays: the pinned buffers are reused by the next call
+        imfs = hb["imfs"][:S].numpy().copy()
+        resid = hb["resid"][:S].numpy().copy()
+        met = hb["met"][:S].numpy().copy()
+        fb = hb["fb"][:S].numpy().astype(bool)
         flagged = [i for i in range(S) if fb[i]]
         plain = {}
         if flagged:
