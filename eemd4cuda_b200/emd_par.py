@@ -28,6 +28,7 @@ Keyword-only extensions:
 from __future__ import annotations
 
 import math
+import threading
 import time
 from dataclasses import dataclass, field
 
@@ -172,6 +173,21 @@ def _auto_batch(torch, p, N, E, bytes_per_el):
     return min(E, b)
 
 
+_STAGE = {}
+_STAGE_LOCK = threading.Lock()
+
+
+def _staging(torch, slots, N):
+    """Pinned host buffers for the outputs of one shape (the latest shape only is kept)."""
+    key = (slots, N)
+    if key not in _STAGE:
+        _STAGE.clear()
+        _STAGE[key] = (torch.empty((slots, N), dtype=torch.float64, pin_memory=True),
+                       torch.empty((N,), dtype=torch.float64, pin_memory=True),
+                       torch.empty((1,), dtype=torch.int32, pin_memory=True))
+    return _STAGE[key]
+
+
 def _run_ensemble(x, *, E, eps, tau, max_sifts, max_imf, min_extrema, end, seed, batch,
                   noise, rules, exact, dtype, config):
     """EEMD of one signal: batches of trials into device sums, then mean/residual."""
@@ -213,21 +229,28 @@ def _run_ensemble(x, *, E, eps, tau, max_sifts, max_imf, min_extrema, end, seed,
         nz = None
         if host_noise is not None:
             nz = torch.from_numpy(np.ascontiguousarray(host_noise[b0:b1], dtype=dt)).to(dev)
-        nsift = torch.empty((Eb,), dtype=torch.int32, device=dev)
-        nmode = torch.empty((Eb,), dtype=torch.int32, device=dev)
-        flags = torch.empty((Eb,), dtype=torch.int32, device=dev)
+        # the per-trial sift counts, mode counts and flags: one array, one copy back
+        cnt = torch.empty((3, Eb), dtype=torch.int32, device=dev)
         L.run(p, xd, [N], b0, Eb, ws, noise=nz, imf_sum=imf_sum, mode_count=mode_count,
-              nsift=nsift, nmode=nmode, flags=flags)
-        per_trial_sifts.extend(nsift.cpu().tolist())
-        per_trial_modes.extend(nmode.cpu().tolist())
-        flags_all.extend(flags.cpu().tolist())
+              nsift=cnt[0], nmode=cnt[1], flags=cnt[2])
+        ch = cnt.cpu()
+        per_trial_sifts.extend(ch[0].tolist())
+        per_trial_modes.extend(ch[1].tolist())
+        flags_all.extend(ch[2].tolist())
     imf_mean = torch.empty((slots, N), dtype=torch.float64, device=dev)
     resid = torch.empty((N,), dtype=torch.float64, device=dev)
     n_modes_d = torch.empty((1,), dtype=torch.int32, device=dev)
     L.finalize(p, xd, [N], imf_sum, mode_count, imf_mean, resid, n_modes_d)
-    n_modes = int(n_modes_d.item())
-    imfs = imf_mean[:n_modes].cpu().numpy()
-    residual = resid.cpu().numpy()
+    # all outputs through pinned staging with one synchronisation
+    with _STAGE_LOCK:  # callers on several threads share the buffers
+        h_mean, h_resid, h_n = _staging(torch, slots, N)
+        h_mean.copy_(imf_mean, non_blocking=True)
+        h_resid.copy_(resid, non_blocking=True)
+        h_n.copy_(n_modes_d, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        n_modes = int(h_n[0])
+        imfs = h_mean[:n_modes].numpy().copy()
+        residual = h_resid.numpy().copy()
     dt_s = time.time() - t0
     reached = any(f & 1 for f in flags_all)
     stats = dict(method="gpu", backend="b200", E=E, n_modes=n_modes, batch=batch,
