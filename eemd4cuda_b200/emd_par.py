@@ -36,7 +36,7 @@ import numpy as np
 
 from . import _lib as L
 
-__all__ = ["decompose", "EMDResult", "make_reference_sweep", "gpu_eemd_full", "EngineConfig"]
+__all__ = ["decompose", "decompose_many", "EMDResult", "make_reference_sweep", "gpu_eemd_full", "EngineConfig"]
 
 
 # =====================================================================
@@ -333,6 +333,77 @@ def decompose(x, method="auto", E=64, eps=0.2, tau=0.25, max_sifts=50, max_imf=-
                                            seed=seed, batch=batch, noise=noise, rules=rules,
                                            exact=exact, dtype=dtype, config=config)
     return EMDResult(imfs=imfs, residual=resid, n_modes=imfs.shape[0], stats=stats)
+
+
+def decompose_many(xs, E=64, eps=0.2, tau=0.25, max_sifts=50, max_imf=-1, min_extrema=4,
+                   end="natural", seed=0, batch=None, *, rules="ref", exact=False, dtype=np.float64,
+                   config: EngineConfig | None = None) -> list:
+    """EEMD (E > 1) or EMD (E = 1) of many 1-D signals of any lengths: every
+    (signal, trial) task of a trial batch in one persistent launch, the tasks
+    queued longest first.  Returns one EMDResult per signal, as decompose
+    would.  The Philox noise is keyed by (seed, signal index in xs, trial), so
+    signal i's ensemble equals decompose(xs[i], seed=seed) only for i = 0;
+    with E = 1 every result equals decompose(xs[i], E=1) (IMFs bit for bit;
+    the residual is x minus the IMFs' sum here)."""
+    torch = _torch()
+    xs = [np.asarray(x, dtype=float) for x in xs]
+    if not xs:
+        return []
+    for x in xs:
+        if x.ndim != 1:
+            raise ValueError("every signal must be 1-D")
+        if len(x) < 8:
+            raise ValueError("signal too short for EMD (need >= 8 samples)")
+    E = int(E)
+    if E < 1:
+        raise ValueError("E must be >= 1")
+    lengths = [len(x) for x in xs]
+    S, NS = len(xs), sum(lengths)
+    slots = imf_slots(max(lengths), max_imf)
+    dt = np.dtype(dtype)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    mode = L.EEMD_NOISE_NONE if E == 1 else L.EEMD_NOISE_PHILOX
+    p = make_params(dtype=dt, noise_mode=mode, eps=eps, seed=seed, tau=tau, max_sifts=max_sifts,
+                    max_imf=slots, min_extrema=min_extrema, end=end, rules=rules, exact=exact,
+                    config=config)
+    if batch is None:
+        free, _ = torch.cuda.mem_get_info()
+        per_trial = L.workspace_size(p, lengths, 1, False)
+        batch = max(1, int(free * 0.7 // max(per_trial, 1)))
+    batch = max(1, min(int(batch), E))
+    xd = torch.from_numpy(np.concatenate([x.astype(dt) for x in xs])).to(dev)
+    imf_sum = torch.zeros((slots * NS,), dtype=torch.float64, device=dev)
+    mode_count = torch.zeros((S * slots,), dtype=torch.int32, device=dev)
+    ws = torch.empty((L.workspace_size(p, lengths, batch, False),), dtype=torch.uint8, device=dev)
+    sifts = np.zeros((S, E), dtype=np.int64)
+    modes = np.zeros((S, E), dtype=np.int64)
+    flags = np.zeros((S, E), dtype=np.int64)
+    t0 = time.time()
+    for b0 in range(0, E, batch):
+        Eb = min(batch, E - b0)
+        cnt = torch.empty((3, S * Eb), dtype=torch.int32, device=dev)
+        L.run(p, xd, lengths, b0, Eb, ws, imf_sum=imf_sum, mode_count=mode_count, nsift=cnt[0], nmode=cnt[1],
+              flags=cnt[2])
+        ch = cnt.cpu().numpy().reshape(3, S, Eb)  # tasks are signal-major: task = s * Eb + e
+        sifts[:, b0:b0 + Eb], modes[:, b0:b0 + Eb], flags[:, b0:b0 + Eb] = ch[0], ch[1], ch[2]
+    imf_mean = torch.empty((slots * NS,), dtype=torch.float64, device=dev)
+    resid = torch.empty((NS,), dtype=torch.float64, device=dev)
+    n_modes = torch.empty((S,), dtype=torch.int32, device=dev)
+    L.finalize(p, xd, lengths, imf_sum, mode_count, imf_mean, resid, n_modes)
+    mh, rh, nh = imf_mean.cpu().numpy(), resid.cpu().numpy(), n_modes.cpu().numpy()
+    wall = time.time() - t0
+    out, off = [], 0
+    for s, x in enumerate(xs):
+        n = lengths[s]
+        m = int(nh[s])
+        imfs = mh[slots * off:slots * (off + n)].reshape(slots, n)[:m].copy()
+        stats = dict(method="gpu", backend="b200", E=E, n_modes=m, batch=batch, signal=s, signals=S,
+                     per_trial_total_sifts=sifts[s].copy(), per_trial_n_modes=modes[s].copy(),
+                     max_imf_reached=bool((flags[s] & 1).any() and max_imf == -1), gpu_time_s=wall,
+                     noise="philox" if E > 1 else "none", x=x)
+        out.append(EMDResult(imfs=imfs, residual=rh[off:off + n].copy(), n_modes=m, stats=stats))
+        off += n
+    return out
 
 
 def gpu_eemd_full(x, E=64, tau=0.25, max_sifts=50, max_imf=12, seed=0, K=None, nthreads=128,
