@@ -345,7 +345,6 @@ def decompose_many(xs, E=64, eps=0.2, tau=0.25, max_sifts=50, max_imf=-1, min_ex
     signal i's ensemble equals decompose(xs[i], seed=seed) only for i = 0;
     with E = 1 every result equals decompose(xs[i], E=1) (IMFs bit for bit;
     the residual is x minus the IMFs' sum here)."""
-    torch = _torch()
     xs = [np.asarray(x, dtype=float) for x in xs]
     if not xs:
         return []
@@ -357,6 +356,7 @@ def decompose_many(xs, E=64, eps=0.2, tau=0.25, max_sifts=50, max_imf=-1, min_ex
     E = int(E)
     if E < 1:
         raise ValueError("E must be >= 1")
+    torch = _torch()
     lengths = [len(x) for x in xs]
     S, NS = len(xs), sum(lengths)
     slots = imf_slots(max(lengths), max_imf)

@@ -78,3 +78,14 @@ def test_make_params_validation():
         M.make_params(dtype=np.float32, exact=True)
     p = M.make_params(dtype=np.float32, end="mirror", rules="numba", max_sifts=10, max_imf=8)
     assert p.dtype == 1 and p.end_mode == 1 and p.rules == 1 and p.max_sifts == 10
+
+
+def test_decompose_many_validates_before_the_device():
+    from eemd4cuda_b200 import emd_par as M
+    assert M.decompose_many([]) == []
+    with pytest.raises(ValueError):
+        M.decompose_many([np.ones(100), np.ones(5)])
+    with pytest.raises(ValueError):
+        M.decompose_many([np.ones((2, 50))])
+    with pytest.raises(ValueError):
+        M.decompose_many([np.ones(100)], E=0)
