@@ -826,7 +826,8 @@ def run_surrogate(args):
 CEEMDAN_WL = Workload(
     "ceemdan48k",
     {"workload": "harmonic_clicks_48k_ceemdan", "N": 48000, "trials": 100, "eps": 0.2, "tau": 0.25,
-     "max_sifts": 50, "storage": "float64", "solve": "float64 (seam windows)", "noise": "default_rng(0) W [E,N]",
+     "max_sifts": 50, "storage": "float64", "solve": "float64 (seam windows)",
+     "noise": "W [E,N] drawn on the device (eemd_philox_normals, seed 0)",
      "signals": 1},
     E=100, eps=0.2, max_imf=1, max_sifts=50, tau=0.25, dtype="f64", seed=1, cpu_tasks=16,
     signals_fn=_harmonic)
@@ -850,7 +851,7 @@ def run_ceemdan(args):
     cb = CpuBaseline(wl) if world == 1 else None
     x = wl.signals()[0]
     N, E = len(x), wl.E
-    kw = dict(E=E, eps=wl.eps, seed=0, tau=wl.tau, max_sifts=wl.max_sifts)
+    kw = dict(E=E, eps=wl.eps, seed=0, tau=wl.tau, max_sifts=wl.max_sifts, noise="philox")
     for _ in range(args.warmup):
         c, r, st = ceemdan(x, **kw)
     torch.cuda.synchronize()
@@ -869,6 +870,13 @@ def run_ceemdan(args):
     ms = total / args.steps
     stages = st["n_imfs"] + 1
     value = N * E * stages / (ms / 1e3) / 1e6
+    # the same call with the reference's numpy noise draw (host PCG64, the parity mode)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    _, _, st_ref = ceemdan(x, **dict(kw, noise="reference"))
+    e1.record(stream)
+    e1.synchronize()
+    ref_noise_ms = e0.elapsed_time(e1)
 
     # roofline of k_emd on one stage-1 launch (first IMF of x + beta W[e])
     dev = torch.device("cuda", local_rank)
@@ -913,6 +921,8 @@ def run_ceemdan(args):
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": round(gbs / peak, 4), "traffic": None,
                      "algorithmic_bytes_per_launch": round(emd_bytes), "avg_launch_ms": round(ev["ms"], 5)},
         "noise_modes": sorted(set(st["noise_modes"])), "clocks": clocks,
+        "reference_noise": {"ms_per_step": round(ref_noise_ms, 3), "stages": st_ref["n_imfs"] + 1,
+                            "note": "W from numpy default_rng(seed) on the host, as the reference draws it"},
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu

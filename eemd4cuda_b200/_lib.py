@@ -39,7 +39,7 @@ ABI_VERSION = 1
 # every symbol include/eemd_b200.h declares
 EXPORTS = ("eemd_default_params", "eemd_version", "eemd_strerror",
            "eemd_workspace_size", "eemd_run", "eemd_run_traced", "eemd_run_static",
-           "eemd_finalize")
+           "eemd_finalize", "eemd_philox_normals")
 
 KERNEL_KINDS = ("sigma", "emd", "reduce", "outputs", "k4", "k5", "k6", "k7")
 
@@ -133,6 +133,8 @@ def load() -> ctypes.CDLL:
     lib.eemd_finalize.argtypes = [POINTER(EemdParams), c_void_p, POINTER(c_int64), c_int32,
                                   c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
     lib.eemd_finalize.restype = c_int32
+    lib.eemd_philox_normals.argtypes = [ctypes.c_uint64, c_int32, c_int32, c_int32, c_int64, c_void_p, c_void_p]
+    lib.eemd_philox_normals.restype = c_int32
     v = lib.eemd_version()
     if v != ABI_VERSION:
         raise RuntimeError(f"{path}: ABI version {v}, expected {ABI_VERSION}")
@@ -220,6 +222,17 @@ def run_static(p: EemdParams, x, lengths, trial_begin: int, trial_count: int, *,
                                 _ptr(imf_sum), _ptr(mode_count), _ptr(nsift), _ptr(nmode),
                                 _ptr(mode_sifts), _ptr(knot_log), _ptr(flags), c_void_p(st))
     check(rc, "eemd_run_static")
+
+
+def philox_normals(seed: int, signal: int, trial_begin: int, trial_count: int, n: int, out,
+                   stream=None) -> None:
+    """eemd_philox_normals into a float64 device tensor out [trial_count * n]."""
+    import torch
+
+    st = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    rc = load().eemd_philox_normals(int(seed) & 0xFFFFFFFFFFFFFFFF, int(signal), int(trial_begin),
+                                    int(trial_count), int(n), _ptr(out), c_void_p(st))
+    check(rc, "eemd_philox_normals")
 
 
 def finalize(p: EemdParams, x, lengths, imf_sum, mode_count, imf_mean, residual, n_modes,

@@ -142,6 +142,15 @@ __device__ __forceinline__ double philox_normal(uint64_t seed, int signal, int t
     return (t & 1) ? rad * s : rad * c;
 }
 
+// out[e][t] = the standard normal the Philox noise mode adds to trial
+// trial_begin + e of signal `signal` at sample t (before the eps*std(x) scale)
+__global__ void k_philox_fill(uint64_t seed, int signal, int trial_begin, int trials, int64_t n, double* out) {
+    const int64_t total = (int64_t)trials * n;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = philox_normal(seed, signal, trial_begin + (int)(i / n), i % n);
+}
+
 // ---------------------------------------------------------------------------
 // block reductions (fixed order => deterministic)
 // ---------------------------------------------------------------------------
@@ -1955,6 +1964,16 @@ const char* eemd_strerror(int32_t status) {
                    "(EEMD_STATIC_SCRATCH_BYTES); use eemd_run with a workspace";
         default: return "unknown status";
     }
+}
+
+int32_t eemd_philox_normals(uint64_t seed, int32_t signal, int32_t trial_begin, int32_t trial_count, int64_t n,
+                            double* out, void* stream) {
+    if (!out || signal < 0 || trial_begin < 0 || trial_count < 1 || n < 1) return EEMD_E_BADARG;
+    const int64_t total = (int64_t)trial_count * n;
+    const int64_t blocks = (total + 255) / 256;
+    k_philox_fill<<<(unsigned)(blocks < 148 * 32 ? blocks : 148 * 32), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        seed, signal, trial_begin, trial_count, n, out);
+    return cudaGetLastError() == cudaSuccess ? EEMD_OK : EEMD_E_CUDA;
 }
 
 int32_t eemd_workspace_size(const eemd_params* p, const int64_t* lengths, int32_t n_signals,

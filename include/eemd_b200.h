@@ -105,6 +105,14 @@ int32_t eemd_version(void);
 /* Human-readable text for a status code. */
 const char* eemd_strerror(int32_t status);
 
+/* out[e][t] (device, float64 [trial_count][n]) = the standard normal that
+ * EEMD_NOISE_PHILOX adds, scaled by eps*std(x), to trial trial_begin + e of
+ * signal `signal` at sample t.  The device counterpart of a host noise draw
+ * such as emd_ref.py:166-168 _gen_noise (a different stream: Philox4x32-10
+ * with Box-Muller, not numpy's PCG64 ziggurat). */
+int32_t eemd_philox_normals(uint64_t seed, int32_t signal, int32_t trial_begin, int32_t trial_count, int64_t n,
+                            double* out, void* stream);
+
 /* Device bytes of workspace one eemd_run() needs for n_signals signals of the
  * given lengths (host array) with trial_count trials each.  imfs_external != 0
  * means the caller passes its own per-trial IMF buffer to eemd_run(). */

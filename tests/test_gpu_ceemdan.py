@@ -59,3 +59,26 @@ def test_ceemdan_48k_staircase_properties():
     # the staircase ends after stage max(noise modes) unless the residual vanished first
     assert st["n_imfs"] <= max(st["noise_modes"]) + 1
     assert all(len(s) == 32 for s in st["stage_sifts"])
+
+
+def test_philox_noise_ceemdan():
+    """noise='philox': W drawn on the device; the staircase is complete and
+    deterministic, and W is standard normal."""
+    from eemd4cuda_b200 import _lib as L
+    from eemd4cuda_b200 import signals
+    W = torch.empty((16, 20000), dtype=torch.float64, device="cuda")
+    L.philox_normals(5, 0, 0, 16, 20000, W)
+    w = W.cpu().numpy()
+    assert abs(w.mean()) < 0.01 and abs(w.std() - 1.0) < 0.01
+    W2 = torch.empty_like(W)
+    L.philox_normals(5, 0, 0, 16, 20000, W2)
+    assert torch.equal(W, W2)
+    L.philox_normals(5, 0, 3, 2, 20000, W2[:2])
+    assert torch.equal(W2[:2], W[3:5])  # keyed by the absolute trial
+    x = signals.harmonic_clicks(8000, seed=2, fs=8000.0)
+    a = ceemdan(x, E=16, seed=5, noise="philox")
+    b = ceemdan(x, E=16, seed=5, noise="philox")
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    c, r, st = a
+    assert np.max(np.abs(x - c.sum(axis=0) - r)) <= 1e-12 * np.abs(x).max()
+    assert st["n_imfs"] <= max(st["noise_modes"]) + 1
