@@ -71,33 +71,40 @@ def ceemdan(x, E=100, eps=0.2, parallel=True, n_workers=None, seed=0, *, tau=0.2
     if max(noise_modes) >= slots:
         raise RuntimeError(f"a noise EMD reached the {slots}-mode cap")
 
+    # per-stage results stay on the device until the staircase ends: the
+    # residual is the only copy back per stage (numpy forms beta and the stop
+    # tests from it)
+    max_st = max(noise_modes) + 1
     imf_sum = torch.empty((N,), dtype=torch.float64, device=dev)
-    count = torch.empty((1,), dtype=torch.int32, device=dev)
-    c_d = torch.empty((N,), dtype=torch.float64, device=dev)
+    cnt_buf = torch.zeros((max_st,), dtype=torch.int32, device=dev)
+    c_buf = torch.empty((max_st, N), dtype=torch.float64, device=dev)
+    sift_buf = torch.empty((max_st, E), dtype=torch.int32, device=dev)
     nm = torch.empty((1,), dtype=torch.int32, device=dev)
     r_d = torch.from_numpy(x.copy()).to(dev)
     r_next = torch.empty_like(r_d)
-    stage_sifts = torch.zeros((E,), dtype=torch.int32, device=dev)
     resid = x.copy()
-    c_imfs, sifts = [], []
+    n_st = 0
     while True:
         if np.max(np.abs(resid)) < 1e-12 or np.std(resid) < 1e-10:
             break
-        stage = len(c_imfs)
+        stage = n_st
         p1.eps = float(eps * np.std(resid))  # beta of this stage
         imf_sum.zero_()
-        count.zero_()
-        L.run(p1, r_d, [N], 0, E, ws, noise=Wd, imf_sum=imf_sum, mode_count=count, nsift=stage_sifts)
-        L.finalize(p1, r_d, [N], imf_sum, count, c_d, r_next, nm)
-        if int(count.item()) != E:
-            raise ValueError(f"CEEMDAN stage {stage}: {E - int(count.item())} of {E} trials have no first IMF "
-                             "(fewer than 4 extrema)")
-        c_imfs.append(c_d.cpu().numpy())
-        sifts.append(stage_sifts.cpu().numpy().tolist())
+        cnt = cnt_buf[stage:stage + 1]
+        L.run(p1, r_d, [N], 0, E, ws, noise=Wd, imf_sum=imf_sum, mode_count=cnt, nsift=sift_buf[stage])
+        L.finalize(p1, r_d, [N], imf_sum, cnt, c_buf[stage], r_next, nm)
         resid = r_next.cpu().numpy()
+        n_st += 1
         r_d, r_next = r_next, r_d
         if all(stage >= m for m in noise_modes):
             break
+    counts = cnt_buf[:n_st].cpu().numpy()
+    for stage, k in enumerate(counts):
+        if int(k) != E:
+            raise ValueError(f"CEEMDAN stage {stage}: {E - int(k)} of {E} trials have no first IMF "
+                             "(fewer than 4 extrema)")
+    c_imfs = list(c_buf[:n_st].cpu().numpy())
+    sifts = sift_buf[:n_st].cpu().numpy().tolist()
     c = np.array(c_imfs) if c_imfs else np.zeros((0, N))
     return c, resid, dict(E=E, n_imfs=len(c_imfs), noise_modes=noise_modes, stage_sifts=sifts, method="gpu",
                           backend="b200", exact=bool(exact), noise=noise)
