@@ -160,6 +160,19 @@ def resolve_segment(a: AudioFile, limits=None, unit="s", max_file_sec=DEFAULT_MA
     return select_segment(a, limits, unit), limits, unit, defaulted
 
 
+def segment_bounds(n: int, n_seg: int) -> list:
+    """[start, stop) of consecutive segments of n_seg samples covering n
+    samples; a last segment under 8 samples (too short for EMD) joins its
+    predecessor."""
+    if n < 1:
+        raise ValueError("empty signal")
+    bounds = [(s, min(s + n_seg, n)) for s in range(0, n, n_seg)]
+    if bounds[-1][1] - bounds[-1][0] < 8 and len(bounds) > 1:
+        bounds[-2] = (bounds[-2][0], bounds[-1][1])
+        bounds.pop()
+    return bounds
+
+
 def decompose_segments(x, sr, segment_s=DEFAULT_SEGMENT_SEC, *, E=64, eps=0.2, tau=0.25, max_sifts=50,
                        max_imf=8, seed=0, dtype=np.float32, outdir=None, return_modes=True):
     """EEMD of x cut into consecutive segments of segment_s seconds (the last
@@ -175,13 +188,7 @@ def decompose_segments(x, sr, segment_s=DEFAULT_SEGMENT_SEC, *, E=64, eps=0.2, t
     from . import results
 
     x = np.asarray(x, dtype=np.float64)
-    n_seg = max(1, int(round(segment_s * sr)))
-    bounds = [(s, min(s + n_seg, len(x))) for s in range(0, len(x), n_seg)]
-    if not bounds:
-        raise ValueError("empty signal")
-    if bounds[-1][1] - bounds[-1][0] < 8 and len(bounds) > 1:
-        bounds[-2] = (bounds[-2][0], bounds[-1][1])  # a sliver joins the previous segment
-        bounds.pop()
+    bounds = segment_bounds(len(x), max(1, int(round(segment_s * sr))))
     dev = torch.device("cuda", torch.cuda.current_device())
     dt = np.dtype(dtype)
     tdt = torch.float32 if dt == np.float32 else torch.float64

@@ -67,3 +67,11 @@ def test_segments_and_errors(tmp_path):
     (tmp_path / "bad.wav").write_bytes(b"not audio")
     with pytest.raises(audio.AudioError):
         audio.load_audio(tmp_path / "bad.wav")
+
+
+def test_segment_bounds():
+    assert audio.segment_bounds(20500, 8000) == [(0, 8000), (8000, 16000), (16000, 20500)]
+    assert audio.segment_bounds(16005, 8000) == [(0, 8000), (8000, 16005)]  # a 5-sample sliver joins
+    assert audio.segment_bounds(100, 8000) == [(0, 100)]
+    with pytest.raises(ValueError):
+        audio.segment_bounds(0, 8000)
