@@ -37,7 +37,10 @@ namespace eemd {
 constexpr int THREADS = 32 * EEMD_CTA_WARPS;  // threads per CTA of k_emd
 constexpr int CTAS_PER_SM = 16 / EEMD_CTA_WARPS;  // 16 warps of 128 registers fill an SM
 constexpr int MAXC = 8;           // largest cluster
-constexpr int FAST_B = 8;         // owned rows per window, fast solve (register resident)
+#ifndef EEMD_FAST_B
+#define EEMD_FAST_B 8
+#endif
+constexpr int FAST_B = EEMD_FAST_B;  // owned rows per window, fast solve (register resident)
 #ifndef EEMD_WSCAP
 #define EEMD_WSCAP 352
 #endif
