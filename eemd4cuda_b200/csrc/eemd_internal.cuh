@@ -37,10 +37,15 @@ namespace eemd {
 constexpr int THREADS = 32 * EEMD_CTA_WARPS;  // threads per CTA of k_emd
 constexpr int CTAS_PER_SM = 16 / EEMD_CTA_WARPS;  // 16 warps of 128 registers fill an SM
 constexpr int MAXC = 8;           // largest cluster
+// owned rows per window of the fast solve (its forward state is register
+// resident): 3 measured fastest (config 2 6.66 ms, 2^22 x 64 trials 143.9 ms,
+// 1024 tasks of 65536 samples 83.5 ms; 8: 7.17 / 147.2 / 92.4; 2, 4, 5, 6,
+// 12 and 16 in between or slower) -- fewer registers outweigh the extra halo
+// rows per owned knot
 #ifndef EEMD_FAST_B
-#define EEMD_FAST_B 8
+#define EEMD_FAST_B 3
 #endif
-constexpr int FAST_B = EEMD_FAST_B;  // owned rows per window, fast solve (register resident)
+constexpr int FAST_B = EEMD_FAST_B;
 #ifndef EEMD_WSCAP
 #define EEMD_WSCAP 352
 #endif
