@@ -217,7 +217,9 @@ def _run_ensemble(x, *, E, eps, tau, max_sifts, max_imf, min_extrema, end, seed,
     xd = torch.from_numpy(np.ascontiguousarray(x, dtype=dt)).to(dev)
     imf_sum = torch.zeros((slots, N), dtype=torch.float64, device=dev)
     mode_count = torch.zeros((slots,), dtype=torch.int32, device=dev)
-    per_trial_sifts, per_trial_modes, flags_all = [], [], []
+    # the per-trial sift counts, mode counts and flags of every batch in one
+    # device array, copied back with the outputs (no wait between launches)
+    cnt = torch.empty((3, E), dtype=torch.int32, device=dev)
     ws = None
     t0 = time.time()
     for b0 in range(0, E, batch):
@@ -229,14 +231,8 @@ def _run_ensemble(x, *, E, eps, tau, max_sifts, max_imf, min_extrema, end, seed,
         nz = None
         if host_noise is not None:
             nz = torch.from_numpy(np.ascontiguousarray(host_noise[b0:b1], dtype=dt)).to(dev)
-        # the per-trial sift counts, mode counts and flags: one array, one copy back
-        cnt = torch.empty((3, Eb), dtype=torch.int32, device=dev)
         L.run(p, xd, [N], b0, Eb, ws, noise=nz, imf_sum=imf_sum, mode_count=mode_count,
-              nsift=cnt[0], nmode=cnt[1], flags=cnt[2])
-        ch = cnt.cpu()
-        per_trial_sifts.extend(ch[0].tolist())
-        per_trial_modes.extend(ch[1].tolist())
-        flags_all.extend(ch[2].tolist())
+              nsift=cnt[0, b0:b1], nmode=cnt[1, b0:b1], flags=cnt[2, b0:b1])
     imf_mean = torch.empty((slots, N), dtype=torch.float64, device=dev)
     resid = torch.empty((N,), dtype=torch.float64, device=dev)
     n_modes_d = torch.empty((1,), dtype=torch.int32, device=dev)
@@ -247,10 +243,11 @@ def _run_ensemble(x, *, E, eps, tau, max_sifts, max_imf, min_extrema, end, seed,
         h_mean.copy_(imf_mean, non_blocking=True)
         h_resid.copy_(resid, non_blocking=True)
         h_n.copy_(n_modes_d, non_blocking=True)
-        torch.cuda.current_stream().synchronize()
+        ch = cnt.cpu()  # synchronises the stream: every copy above has landed
         n_modes = int(h_n[0])
         imfs = h_mean[:n_modes].numpy().copy()
         residual = h_resid.numpy().copy()
+    per_trial_sifts, per_trial_modes, flags_all = ch[0].tolist(), ch[1].tolist(), ch[2].tolist()
     dt_s = time.time() - t0
     reached = any(f & 1 for f in flags_all)
     stats = dict(method="gpu", backend="b200", E=E, n_modes=n_modes, batch=batch,
