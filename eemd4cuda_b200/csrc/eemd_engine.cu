@@ -247,6 +247,16 @@ struct Geo {
 
 __host__ __device__ inline int stage_pad(int k) { return k + (k >> 4); }
 
+// Staging slot of knot k.  The lanes of a solve pass read knots one window
+// width apart: exact windows (16 knots) pad one slot every 16 so that the
+// lanes spread over the banks; fast windows of an odd width already hit 32
+// distinct banks unpadded (stride 3 is a permutation of the 32 banks, and of
+// the 16 bank pairs of a half-warp's doubles), and padding would collide them.
+template <bool EXACT>
+__host__ __device__ inline int stage_slot(int k) {
+    return (EXACT || FAST_B % 2 == 0) ? stage_pad(k) : k;
+}
+
 __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 
 // per-warp solve staging: slopes (double), knot times (int), knot values (storage type)
@@ -307,7 +317,7 @@ __device__ __forceinline__ void real_knot(const Ctx& C, const Slot& sl, const Ta
 // Stage the mirror-space knots rlo .. rlo+kcount-1 (lane-strided); each lane
 // finds the segment of its first real knot by binary search and then walks
 // forward, since its later knots follow in the same or later segments.
-template <typename T>
+template <typename T, bool EXACT>
 __device__ __forceinline__ void stage_range(const Ctx& C, const Slot& sl, const TaskSm& S, int env, int rlo,
                                             int kcount, int* skt, T* sky, int lane) {
     const int* pr = S.pref[S.kpar][env];
@@ -316,8 +326,8 @@ __device__ __forceinline__ void stage_range(const Ctx& C, const Slot& sl, const 
     int r = -1;
     for (int k = lane; k < kcount; k += 32) {
         int i2 = rlo + k;
-        int* kt_s = &skt[stage_pad(k)];
-        T* ky_s = &sky[stage_pad(k)];
+        int* kt_s = &skt[stage_slot<EXACT>(k)];
+        T* ky_s = &sky[stage_slot<EXACT>(k)];
         if (mir) {
             if (i2 == 0) {
                 *kt_s = S.tfirst[env];
@@ -390,8 +400,8 @@ __device__ __forceinline__ Row row_of(int ta, int tb, int tc, double sa, double 
     return w;
 }
 
-#define SKT(k) skt[stage_pad(k)]
-#define SSL(k) ssl[stage_pad(k)]
+#define SKT(k) skt[stage_slot<kExact>(k)]
+#define SSL(k) ssl[stage_slot<kExact>(k)]
 
 // Interval records of one envelope in mirror space: RS storage-type elements
 // per record: [0] t_k (integer bit pattern), [1] y_k, [2] fast: c1 / exact:
@@ -408,6 +418,7 @@ struct Rec {
 template <typename T>
 __device__ void window_exact(const Ctx& C, const int* skt, const T* sky, const double* ssl, int base,
                              int n, int w, const Rec<T>& R, int p2) {
+    constexpr bool kExact = true;
     const int B = C.B, S = C.S;
     const int o0 = w * B;
     const int o1 = min(n, o0 + B) - 1;
@@ -433,7 +444,7 @@ __device__ void window_exact(const Ctx& C, const int* skt, const T* sky, const d
     }
     auto put = [&](int k, double Mk) {
         R.at(k, 0) = tbits<T>(SKT(k - base));
-        R.at(k, 1) = sky[stage_pad(k - base)];
+        R.at(k, 1) = sky[stage_slot<kExact>(k - base)];
         R.at(k, 2) = (T)Mk;
     };
     double xv = dp;
@@ -454,6 +465,7 @@ __device__ void window_exact(const Ctx& C, const int* skt, const T* sky, const d
 template <typename T>
 __device__ void window_fast(const Ctx& C, const int* skt, const T* sky, const double* ssl, int base, int n,
                             int w, const Rec<T>& R, int p2) {
+    constexpr bool kExact = false;
     const int S = C.S;
     const int o0 = w * FAST_B;
     const int cnt = min(FAST_B, n - o0);
@@ -519,7 +531,7 @@ __device__ void window_fast(const Ctx& C, const int* skt, const T* sky, const do
         const int t0 = SKT(k - base), t1 = SKT(k + 1 - base);
         const double h = (double)(t1 - t0);
         R.at(k, 0) = tbits<T>(t0);
-        R.at(k, 1) = sky[stage_pad(k - base)];
+        R.at(k, 1) = sky[stage_slot<kExact>(k - base)];
         R.at(k, 2) = (T)fma(-h * (1.0 / 6.0), fma(2.0, Ma, Mb), SSL(k - base));
         R.at(k, 3) = (T)(0.5 * Ma);
         R.at(k, 4) = (T)((Mb - Ma) * fast_rcp(h) * (1.0 / 6.0));
@@ -624,16 +636,16 @@ __device__ void solve_task(const Ctx& C, const Slot& sl, TaskSm& S, unsigned cha
         const int rlo = max(0, w0 * Bw - C.S);
         const int rhi = min(n - 1, min(n, wend * Bw) - 1 + C.S);
         const int kcount = rhi + 3 - rlo;  // knots rlo .. rhi+2
-        stage_range<T>(C, sl, S, env, rlo, kcount, skt, sky, lane);
+        stage_range<T, EXACT>(C, sl, S, env, rlo, kcount, skt, sky, lane);
         cp_async_commit();
         cp_async_wait<0>();
         __syncwarp();
         SUB(0);
         for (int k = lane; k + 1 < kcount; k += 32) {
-            const int ta = skt[stage_pad(k)], tb = skt[stage_pad(k + 1)];
-            const double ya = (double)sky[stage_pad(k)], yb = (double)sky[stage_pad(k + 1)];
+            const int ta = skt[stage_slot<EXACT>(k)], tb = skt[stage_slot<EXACT>(k + 1)];
+            const double ya = (double)sky[stage_slot<EXACT>(k)], yb = (double)sky[stage_slot<EXACT>(k + 1)];
             // emd_ref.py:47: (y_{q+1}-y_q)/H_q (the same IEEE division in exact mode)
-            ssl[stage_pad(k)] = EXACT ? (yb - ya) / (double)(tb - ta) : (yb - ya) * fast_rcp((double)(tb - ta));
+            ssl[stage_slot<EXACT>(k)] = EXACT ? (yb - ya) / (double)(tb - ta) : (yb - ya) * fast_rcp((double)(tb - ta));
         }
         __syncwarp();
         SUB(1);
