@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(1024) k_sigma(const SignalDesc* sdesc, const v
 // per-CTA task context (shared memory)
 // ---------------------------------------------------------------------------
 constexpr int NWARP = THREADS / 32;
-constexpr int MAXSEG = 8 * NWARP;  // knot segments per task: one per warp of up to 8 CTAs
+constexpr int MAXSEG = MAXC * NWARP;  // knot segments per task: one per warp of up to MAXC CTAs
 
 struct Xchg {              // one CTA's published segment results (DSMEM-visible)
     double num, den;       // SD partial sums of the segment
@@ -1705,9 +1705,40 @@ struct Layout {
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// Clusters of c CTAs of the k_emd instance for (dtype, exact) that the
+// current device can hold at once (0 if the query fails, e.g. no device).
+int active_clusters(int dtype, bool exact, int c) {
+    const void* fn = (dtype == EEMD_F32) ? (const void*)k_emd<float, false>
+                                         : (exact ? (const void*)k_emd<double, true> : (const void*)k_emd<double, false>);
+    const size_t smem = smem_bytes(dtype == EEMD_F32 ? 4 : 8);
+    int n = 0;
+    bool ok = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess;
+    if (ok && c > 8) ok = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess;
+    if (ok) {
+        cudaLaunchConfig_t cfg;
+        memset(&cfg, 0, sizeof(cfg));
+        cfg.gridDim = dim3((unsigned)c, 1, 1);
+        cfg.blockDim = dim3(THREADS, 1, 1);
+        cfg.dynamicSmemBytes = smem;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = (unsigned)c;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        ok = cudaOccupancyMaxActiveClusters(&n, fn, &cfg) == cudaSuccess;
+    }
+    if (!ok) {
+        (void)cudaGetLastError();  // a failed query leaves no sticky state for the launch checks
+        n = 0;
+    }
+    return n;
+}
+
 // The cluster spreads one task over several SMs when there are fewer tasks
 // than CTA slots.
-int autotune_csize(int64_t n_tasks, int64_t nmin) {
+int autotune_csize(int64_t n_tasks, int64_t nmin, int dtype, bool exact) {
     // leave a fifth of the CTA slots free: clusters must fit inside a GPC,
     // and the last clusters to be placed would otherwise wait for a second
     // wave.  Signals of a million samples or more take every slot: each CTA
@@ -1720,6 +1751,18 @@ int autotune_csize(int64_t n_tasks, int64_t nmin) {
     // the last round's idle tail (1024 tasks of 65536 samples: 94.6 ms at 2
     // against 97.0 at 1)
     if (c == 1 && nmin >= (1 << 16)) c = 2;
+    // signals of a million samples or more with slots to spare at 8 CTAs per
+    // task (64 tasks use 512 of 592): a larger, non-portable cluster when the
+    // device holds every task's cluster at once (a task waiting for a second
+    // wave would double the launch)
+    if (c == 8 && nmin >= (1 << 20)) {
+        for (int c2 = (int)std::min<int64_t>(MAXC, slots / std::max<int64_t>(n_tasks, 1)); c2 > 8; --c2) {
+            if (active_clusters(dtype, exact, c2) >= n_tasks) {
+                c = c2;
+                break;
+            }
+        }
+    }
     while (c > 1 && nmin / c < 2048) --c;
     return c;
 }
@@ -1737,7 +1780,7 @@ int check_params(const eemd_params* p) {
     if (p->tile != 0 && p->tile != wt) return EEMD_E_BADARG;
     if (p->knots_per_block < 0 || p->knots_per_block > 4096 || p->halo < 0 || p->halo > 256)
         return EEMD_E_BADARG;
-    if (p->cluster_size < 0 || p->cluster_size > 8) return EEMD_E_BADARG;
+    if (p->cluster_size < 0 || p->cluster_size > MAXC) return EEMD_E_BADARG;
     return EEMD_OK;
 }
 
@@ -1754,7 +1797,7 @@ int make_layout(const eemd_params* p, const int64_t* lengths, int n_signals, int
         nmax = std::max(nmax, lengths[s]);
         nmin = std::min(nmin, lengths[s]);
     }
-    L.csize = p->cluster_size ? p->cluster_size : autotune_csize(n_tasks, nmin);
+    L.csize = p->cluster_size ? p->cluster_size : autotune_csize(n_tasks, nmin, p->dtype, p->exact != 0);
     // decay halo of the seam windows: the truncation error falls like
     // (2 - sqrt 3)^S; 16 rows put it far below float32 rounding
     L.S = p->halo ? p->halo : (p->exact ? 32 : (p->dtype == EEMD_F32 ? 16 : 24));
@@ -1883,6 +1926,9 @@ int launch_emd(const Ctx& C, const Layout& L, cudaStream_t st, Tracer& tr) {
     const size_t smem = smem_bytes((int)sizeof(T));
     if (cudaFuncSetAttribute(k_emd<T, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
+        return EEMD_E_CUDA;
+    if (L.csize > 8 &&
+        cudaFuncSetAttribute(k_emd<T, EXACT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
         return EEMD_E_CUDA;
     cudaLaunchConfig_t cfg;
     memset(&cfg, 0, sizeof(cfg));

@@ -36,7 +36,9 @@ namespace eemd {
 #endif
 constexpr int THREADS = 32 * EEMD_CTA_WARPS;  // threads per CTA of k_emd
 constexpr int CTAS_PER_SM = 16 / EEMD_CTA_WARPS;  // 16 warps of 128 registers fill an SM
-constexpr int MAXC = 8;           // largest cluster
+// largest cluster: portable clusters reach 8 CTAs; 9 to 16 are non-portable
+// and are taken only when the device reports that all of them fit at once
+constexpr int MAXC = 16;
 // owned rows per window of the fast solve (its forward state is register
 // resident): 3 measured fastest (config 2 6.66 ms, 2^22 x 64 trials 143.9 ms,
 // 1024 tasks of 65536 samples 83.5 ms; 8: 7.17 / 147.2 / 92.4; 2, 4, 5, 6,

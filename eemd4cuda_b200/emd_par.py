@@ -79,7 +79,7 @@ class EngineConfig:
     tile: samples per warp tile; only 32 x 8 (float32) or 32 x 4 (float64).
     knots_per_block, halo: exact-mode solve window and decay halo.
     watchdog: spin limit of the device waits (negative: test mode).
-    cluster_size: CTAs sharing one signal (1..8)."""
+    cluster_size: CTAs sharing one signal (1..16; 9..16 are non-portable cluster sizes)."""
     tile: int = 0
     knots_per_block: int = 0
     halo: int = 0

@@ -91,7 +91,8 @@ typedef struct eemd_params {
                                  a negative value -k is the watchdog test mode: every
                                  look-back first waits on a flag nothing sets, gives up
                                  after k polls and the run returns EEMD_E_TIMEOUT */
-    int32_t  cluster_size;    /* CTAs (thread-block cluster) per task, 1..8 (0 = autotune) */
+    int32_t  cluster_size;    /* CTAs (thread-block cluster) per task, 1..16 (0 = autotune; 9..16 are
+                                 non-portable cluster sizes the device must support) */
     int32_t  reserved;
 } eemd_params;
 

@@ -190,7 +190,7 @@ def test_determinism_and_seed(sweep):
     assert np.max(np.abs(a.imfs[:m] - c.imfs[:m])) > 0
 
 
-@pytest.mark.parametrize("cluster_size", [1, 2, 4])
+@pytest.mark.parametrize("cluster_size", [1, 2, 4, 9])
 def test_cluster_size_invariance(sweep, cluster_size):
     """Launch shape must not change results: the knot lists, the solve windows
     and the per-sample arithmetic do not depend on how many CTAs share a
