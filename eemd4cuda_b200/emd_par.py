@@ -35,6 +35,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib as L
+from .hostcopy import fresh_copy
 
 __all__ = ["decompose", "decompose_many", "EMDResult", "make_reference_sweep", "gpu_eemd_full", "EngineConfig"]
 
@@ -245,7 +246,7 @@ def _run_ensemble(x, *, E, eps, tau, max_sifts, max_imf, min_extrema, end, seed,
         h_n.copy_(n_modes_d, non_blocking=True)
         ch = cnt.cpu()  # synchronises the stream: every copy above has landed
         n_modes = int(h_n[0])
-        imfs = h_mean[:n_modes].numpy().copy()
+        imfs = fresh_copy(h_mean[:n_modes].numpy())
         residual = h_resid.numpy().copy()
     per_trial_sifts, per_trial_modes, flags_all = ch[0].tolist(), ch[1].tolist(), ch[2].tolist()
     dt_s = time.time() - t0

@@ -54,6 +54,7 @@ from . import _lib as L
 from . import _sg as SG
 from . import emd_par as M
 from . import signals
+from .hostcopy import fresh_copy
 
 CH = 16           # padded channels of the network's input and output
 K_IMF = 10        # IMF channels
@@ -487,8 +488,8 @@ class SurrogateEEMD:
         torch.cuda.current_stream().synchronize()
         self.net.check()
         # fresh arrays: the pinned buffers are reused by the next call
-        imfs = hb["imfs"][:S].numpy().copy()
-        resid = hb["resid"][:S].numpy().copy()
+        imfs = fresh_copy(hb["imfs"][:S].numpy())
+        resid = fresh_copy(hb["resid"][:S].numpy())
         met = hb["met"][:S].numpy().copy()
         fb = hb["fb"][:S].numpy().astype(bool)
         flagged = [i for i in range(S) if fb[i]]
