@@ -1,4 +1,4 @@
-"""Result files written from device buffers (result formats).
+"""Result files written from device buffers.
 
 Two formats of the reference, byte-compatible in their keys and dtypes:
 

@@ -5,7 +5,7 @@
  * 256-trial ensemble mean with a dilated 1-D convolution network.  The
  * reference has no learned component: these entry points have no counterpart
  * in it.  The plain full-ensemble EEMD (eemd_b200.h) produces the training
- * pairs and remains the fallback and the judge of the surrogate's output.
+ * pairs and remains both the fallback and the yardstick of the surrogate's output.
  *
  * Tensors are device pointers.  Activations are bfloat16, channels-last
  * ([batch][time][C], C = 16 or 64).  Packed weights are the bfloat16 image of
