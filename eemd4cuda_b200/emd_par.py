@@ -24,13 +24,21 @@ Keyword-only extensions:
     rules  'ref' (emd_ref.py stop rules, default) or 'numba' (emd_gpu.py).
     exact  True: reference float64 operation order (parity mode).
     dtype  np.float64 (default) or np.float32 storage.
+    checkpoint  path of a .npz that an ensemble (E > 1) run updates after
+           every trial batch (device sums, mode counts, per-trial counters,
+           next trial); a later call with the same arguments and signal
+           resumes from it, with results bit-identical to an uninterrupted
+           run, and the file is removed once the run completes.
 """
 from __future__ import annotations
 
+import hashlib
+import json
 import math
+import os
 import threading
 import time
-from dataclasses import dataclass, field
+from dataclasses import asdict, dataclass, field
 
 import numpy as np
 
@@ -189,10 +197,55 @@ def _staging(torch, slots, N):
     return _STAGE[key]
 
 
+class Checkpoint:
+    """Batch-granularity state of one ensemble run in a .npz file.
+
+    `key` identifies the run (every argument that changes the result, and a
+    SHA-256 of the signal); a file written by a different run is refused
+    rather than mixed in.  Writes go to a temporary file that replaces the
+    old one, so an interruption leaves the previous complete state."""
+
+    def __init__(self, path, key: dict):
+        self.path = os.fspath(path)
+        self.key = json.dumps(key, sort_keys=True)
+
+    def load(self):
+        """The saved state (dict) or None when there is no file."""
+        if not os.path.exists(self.path):
+            return None
+        with np.load(self.path, allow_pickle=False) as z:
+            if str(z["key"]) != self.key:
+                raise ValueError(f"checkpoint {self.path} was written by a different run "
+                                 "(other arguments or signal)")
+            return {k: z[k] for k in ("batch", "next", "imf_sum", "mode_count", "counters")}
+
+    def save(self, *, batch, next_trial, imf_sum, mode_count, counters):
+        tmp = self.path + ".tmp"
+        with open(tmp, "wb") as f:
+            np.savez(f, key=np.array(self.key), batch=np.int64(batch), next=np.int64(next_trial),
+                     imf_sum=imf_sum, mode_count=mode_count, counters=counters)
+        os.replace(tmp, self.path)
+
+    def remove(self):
+        if os.path.exists(self.path):
+            os.remove(self.path)
+
+
+def checkpoint_key(x, **kw) -> dict:
+    """Identity of an ensemble run for Checkpoint: the arguments and the signal's hash."""
+    cfg = kw.pop("config", None)
+    kw["config"] = asdict(cfg) if cfg is not None else None
+    kw["dtype"] = np.dtype(kw["dtype"]).str
+    kw["x_sha256"] = hashlib.sha256(np.ascontiguousarray(x, dtype=np.float64).tobytes()).hexdigest()
+    kw["N"] = int(len(x))
+    return kw
+
+
 def _run_ensemble(x, *, E, eps, tau, max_sifts, max_imf, min_extrema, end, seed, batch,
-                  noise, rules, exact, dtype, config):
+                  noise, rules, exact, dtype, config, checkpoint=None):
     """EEMD of one signal: batches of trials into device sums, then mean/residual."""
     torch = _torch()
+    nvtx = torch.cuda.nvtx
     N = len(x)
     slots = imf_slots(N, max_imf)
     dt = np.dtype(dtype)
@@ -209,21 +262,39 @@ def _run_ensemble(x, *, E, eps, tau, max_sifts, max_imf, min_extrema, end, seed,
     p = make_params(dtype=dt, noise_mode=nmode_kind, eps=eps, seed=seed, tau=tau,
                     max_sifts=max_sifts, max_imf=slots, min_extrema=min_extrema, end=end,
                     rules=rules, exact=exact, config=config)
+    ck = state = None
+    if checkpoint is not None:
+        ck = Checkpoint(checkpoint, checkpoint_key(
+            x, E=E, eps=float(eps), tau=float(tau), max_sifts=int(max_sifts), max_imf=int(slots),
+            min_extrema=int(min_extrema), end=end, seed=int(seed), noise=noise, rules=rules,
+            exact=bool(exact), dtype=dt, config=config))
+        state = ck.load()
+        if state is not None:
+            if batch is not None and int(batch) != int(state["batch"]):
+                raise ValueError(f"checkpoint {ck.path} was written with batch={int(state['batch'])}")
+            batch = int(state["batch"])  # the same batch boundaries, so the same sums
     if batch is None:
         batch = _auto_batch(torch, p, N, E, dt.itemsize)
     batch = max(1, min(int(batch), E))
     host_noise = (reference_noise(x, E, eps, seed, noise)
                   if nmode_kind == L.EEMD_NOISE_INJECTED else None)
 
-    xd = torch.from_numpy(np.ascontiguousarray(x, dtype=dt)).to(dev)
-    imf_sum = torch.zeros((slots, N), dtype=torch.float64, device=dev)
-    mode_count = torch.zeros((slots,), dtype=torch.int32, device=dev)
-    # the per-trial sift counts, mode counts and flags of every batch in one
-    # device array, copied back with the outputs (no wait between launches)
-    cnt = torch.empty((3, E), dtype=torch.int32, device=dev)
+    with nvtx.range("eemd.upload"):
+        xd = torch.from_numpy(np.ascontiguousarray(x, dtype=dt)).to(dev)
+        imf_sum = torch.zeros((slots, N), dtype=torch.float64, device=dev)
+        mode_count = torch.zeros((slots,), dtype=torch.int32, device=dev)
+        # the per-trial sift counts, mode counts and flags of every batch in one
+        # device array, copied back with the outputs (no wait between launches)
+        cnt = torch.empty((3, E), dtype=torch.int32, device=dev)
+        first = 0
+        if state is not None:
+            first = int(state["next"])
+            imf_sum.copy_(torch.from_numpy(state["imf_sum"]))
+            mode_count.copy_(torch.from_numpy(state["mode_count"]))
+            cnt[:, :first].copy_(torch.from_numpy(state["counters"]))
     ws = None
     t0 = time.time()
-    for b0 in range(0, E, batch):
+    for b0 in range(first, E, batch):
         b1 = min(E, b0 + batch)
         Eb = b1 - b0
         need = L.workspace_size(p, [N], Eb, False)
@@ -232,14 +303,20 @@ def _run_ensemble(x, *, E, eps, tau, max_sifts, max_imf, min_extrema, end, seed,
         nz = None
         if host_noise is not None:
             nz = torch.from_numpy(np.ascontiguousarray(host_noise[b0:b1], dtype=dt)).to(dev)
-        L.run(p, xd, [N], b0, Eb, ws, noise=nz, imf_sum=imf_sum, mode_count=mode_count,
-              nsift=cnt[0, b0:b1], nmode=cnt[1, b0:b1], flags=cnt[2, b0:b1])
+        with nvtx.range("eemd.batch"):
+            L.run(p, xd, [N], b0, Eb, ws, noise=nz, imf_sum=imf_sum, mode_count=mode_count,
+                  nsift=cnt[0, b0:b1], nmode=cnt[1, b0:b1], flags=cnt[2, b0:b1])
+        if ck is not None:
+            with nvtx.range("eemd.checkpoint"):
+                ck.save(batch=batch, next_trial=b1, imf_sum=imf_sum.cpu().numpy(),
+                        mode_count=mode_count.cpu().numpy(), counters=cnt[:, :b1].cpu().numpy())
     imf_mean = torch.empty((slots, N), dtype=torch.float64, device=dev)
     resid = torch.empty((N,), dtype=torch.float64, device=dev)
     n_modes_d = torch.empty((1,), dtype=torch.int32, device=dev)
-    L.finalize(p, xd, [N], imf_sum, mode_count, imf_mean, resid, n_modes_d)
+    with nvtx.range("eemd.finalize"):
+        L.finalize(p, xd, [N], imf_sum, mode_count, imf_mean, resid, n_modes_d)
     # all outputs through pinned staging with one synchronisation
-    with _STAGE_LOCK:  # callers on several threads share the buffers
+    with _STAGE_LOCK, nvtx.range("eemd.download"):  # callers on several threads share the buffers
         h_mean, h_resid, h_n = _staging(torch, slots, N)
         h_mean.copy_(imf_mean, non_blocking=True)
         h_resid.copy_(resid, non_blocking=True)
@@ -249,6 +326,8 @@ def _run_ensemble(x, *, E, eps, tau, max_sifts, max_imf, min_extrema, end, seed,
         imfs = fresh_copy(h_mean[:n_modes].numpy())
         residual = h_resid.numpy().copy()
     per_trial_sifts, per_trial_modes, flags_all = ch[0].tolist(), ch[1].tolist(), ch[2].tolist()
+    if ck is not None:
+        ck.remove()
     dt_s = time.time() - t0
     reached = any(f & 1 for f in flags_all)
     stats = dict(method="gpu", backend="b200", E=E, n_modes=n_modes, batch=batch,
@@ -299,7 +378,7 @@ def _run_single(x, *, tau, max_sifts, max_imf, min_extrema, end, rules, exact, d
 def decompose(x, method="auto", E=64, eps=0.2, tau=0.25, max_sifts=50, max_imf=-1,
               min_extrema=4, end="natural", n_workers=None, seed=0, parallel=True, batch=None,
               nthreads=128, *, noise="philox", rules="ref", exact=False, dtype=np.float64,
-              config: EngineConfig | None = None):
+              config: EngineConfig | None = None, checkpoint=None):
     """Decompose a 1-D signal x into IMFs (+ residual) on the B200 engine.
 
     Arguments follow emd_par.decompose; n_workers, parallel and nthreads are
@@ -329,7 +408,8 @@ def decompose(x, method="auto", E=64, eps=0.2, tau=0.25, max_sifts=50, max_imf=-
         imfs, resid, stats = _run_ensemble(x, E=E, eps=eps, tau=tau, max_sifts=max_sifts,
                                            max_imf=max_imf, min_extrema=min_extrema, end=end,
                                            seed=seed, batch=batch, noise=noise, rules=rules,
-                                           exact=exact, dtype=dtype, config=config)
+                                           exact=exact, dtype=dtype, config=config,
+                                           checkpoint=checkpoint)
     return EMDResult(imfs=imfs, residual=resid, n_modes=imfs.shape[0], stats=stats)
 
 
