@@ -73,3 +73,26 @@ def test_bad_input_raises():
     with pytest.raises(EEMDError) as ei:
         run_eemd(np.ones(5), method="gpu", E=1)
     assert ei.value.code == "eemd.bad_input"
+
+
+def test_injected_allocation_failure_is_a_backend_error(two_tones, monkeypatch):
+    """A device allocation that fails (injected on the host: torch.zeros on the
+    device raises the out-of-memory error) surfaces as eemd.backend, and the
+    next call runs normally."""
+    import torch
+    x, sr = two_tones
+    real = torch.zeros
+
+    def failing(*a, **k):
+        dev = k.get("device")
+        if dev is not None and torch.device(dev).type == "cuda":
+            raise torch.OutOfMemoryError("injected allocation failure")
+        return real(*a, **k)
+
+    monkeypatch.setattr(torch, "zeros", failing)
+    with pytest.raises(EEMDError) as ei:
+        run_eemd(x, method="gpu", E=4, seed=1)
+    assert ei.value.code == "eemd.backend"
+    monkeypatch.setattr(torch, "zeros", real)
+    d = run_eemd(x, method="gpu", E=4, seed=1)
+    assert d.n_modes >= 1 and d.recon < 1e-6 * np.abs(x).max()
