@@ -190,7 +190,8 @@ class CpuBaseline:
 
     def describe(self, v: float) -> dict:
         wl = self.wl
-        what = (f"{len(self.tasks)} (signal, trial) tasks of the workload (emd_1d, float64, "
+        what = (f"{len(self.tasks)} (signal, trial) tasks of the workload (emd_1d, float64 "
+                f"arithmetic on the workload's {'float32-rounded ' if wl.dtype == 'f32' else ''}signal, "
                 f"tau={wl.tau}, max_sifts={self.kw['max_sifts']}, max_imf={self.kw['max_imf']}, "
                 f"{wl.end} ends) in a {self.cores}-process pool")
         if wl.cpu_max_imf or wl.cpu_max_sifts:
@@ -221,7 +222,9 @@ def run_reference(args, wl: Workload):
             "n_gpus": args.gpus, "steps": steps, "warmup": warm,
             "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(wl.config, storage="float64", sample_tasks=len(cb.tasks)),
+            # the workload as the GPU arm names it; the CPU specifics (float64
+            # arithmetic, the bounded sample of tasks) are in cpu_baseline.sample
+            "config": dict(wl.config),
             "cpu_baseline": cb.describe(v),
             "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
