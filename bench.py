@@ -319,6 +319,24 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
+def measured_traffic(workload: str, tasks_per_launch: int):
+    """DRAM bytes (read + write) of one k_emd launch from an ncu capture
+    summarised in profiles/emd_traffic.json: the launch itself, or a smaller
+    launch of the same workload scaled by its (signal, trial) tasks when the
+    full launch is too large to capture (traffic grows with the tasks, since
+    every task streams its own buffers).  None when there is no capture."""
+    tf = ROOT / "profiles" / "emd_traffic.json"
+    try:
+        ent = json.loads(tf.read_text()).get(workload) or {}
+    except (OSError, ValueError):
+        return None
+    if "bytes_per_launch" in ent:
+        return int(ent["bytes_per_launch"])
+    if "bytes_per_task" in ent:
+        return int(round(ent["bytes_per_task"] * tasks_per_launch))
+    return None
+
+
 def emd_algorithmic_bytes(klog: np.ndarray, nmode: np.ndarray, lengths, trials: int,
                           bytes_el: int) -> float:
     """Algorithmic bytes of one k_emd launch, from the per-sift knot log.
@@ -464,13 +482,7 @@ def run_ours(args, wl: Workload):
     emd_gbs = emd_bytes / (ev["ms"] / 1e3) / 1e9 if ev["ms"] > 0 else 0.0
     gpu_sifts_per_task = float(nsift.float().mean().item())
     peak, peak_kind = measured_peak_hbm()
-    traffic = None
-    tf = ROOT / "profiles" / "emd_traffic.json"
-    if wl.name == "harmonic48k" and tf.exists():
-        try:
-            traffic = json.loads(tf.read_text()).get("bytes_per_launch")
-        except ValueError:
-            traffic = None
+    traffic = measured_traffic(wl.name, n_first)
 
     # ---- end to end through the public API (host buffers) ----
     if wl.name in ("harmonic48k", "plain8k"):
