@@ -1,0 +1,35 @@
+"""Host-side arithmetic of bench.py (CPU): the algorithmic-byte count of a
+k_emd launch and the per-workload measured traffic."""
+import sys
+from pathlib import Path
+
+import numpy as np
+
+sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+import bench  # noqa: E402
+
+
+def test_algorithmic_bytes_by_hand():
+    # 2 tasks (1 signal of 1000 samples, 2 trials), float32 (b = 4)
+    klog = np.full((2, 3, 4, 2), -1, dtype=np.int32)
+    klog[0, 0, :2] = [[100, 99], [90, 91]]   # task 0, IMF 0: two sifts
+    klog[0, 1, :1] = [[40, 41]]              # task 0, IMF 1: one sift
+    klog[1, 0, :1] = [[120, 118]]            # task 1, IMF 0: one sift
+    nmode = np.array([2, 1], dtype=np.int32)
+    n, b = 1000, 4
+    per_knot = 3 * (4 + b) + 16
+    want = (2 * n * b                                   # task 0 input / perturbed input
+            + 3 * (3 * n * b) + (199 + 181 + 81) * per_knot + 2 * (4 * n * b)
+            + 2 * n * b                                 # task 1
+            + 3 * n * b + 238 * per_knot + 4 * n * b)
+    got = bench.emd_algorithmic_bytes(klog, nmode, [n], 2, b)
+    assert got == want
+
+
+def test_measured_traffic_per_workload():
+    full = bench.measured_traffic("harmonic48k", 100)
+    assert isinstance(full, int) and full > 0
+    assert bench.measured_traffic("harmonic48k", 7) == full  # a launch capture is not rescaled
+    a64, a32 = bench.measured_traffic("amfm4m", 64), bench.measured_traffic("amfm4m", 32)
+    assert a64 > 0 and abs(a64 - 2 * a32) <= 1
+    assert bench.measured_traffic("plain8k", 1) is None
