@@ -130,3 +130,20 @@ def test_stft_shape_matches_the_reference_frame_count():
         assert T == (N + 2 * (nper // 2) - nov) // (nper - nov)
     with pytest.raises(_sp.SpectraError):
         _sp.stft_shape(100, 64, 64)
+
+
+def test_headers_are_plain_c99(tmp_path):
+    """Every public header compiles as ISO C99 (no C++, no CUDA types), so
+    cgo, cffi or any C toolchain can bind the libraries."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("gcc not available")
+    inc = HEADER.parent
+    src = tmp_path / "abi.c"
+    src.write_text("".join(f'#include "{h.name}"\n' for h in sorted(inc.glob("*.h")))
+                   + "int main(void) { return 0; }\n")
+    r = subprocess.run([gcc, "-std=c99", "-pedantic-errors", "-Wall", "-Werror", "-fsyntax-only",
+                        "-I", str(inc), str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
