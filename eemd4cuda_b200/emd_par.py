@@ -86,8 +86,11 @@ class EngineConfig:
     """Engine knobs beyond the reference's signature (0 = default / autotune).
 
     tile: samples per warp tile; only 32 x 8 (float32) or 32 x 4 (float64).
-    knots_per_block, halo: exact-mode solve window and decay halo.
-    watchdog: spin limit of the device waits (negative: test mode).
+    knots_per_block: owned rows of an exact-mode seam window; halo: the decay
+        halo of every seam window (exact and fast).
+    watchdog: negative -k is the test mode (each task first polls a flag that
+        nothing sets k times, then the run fails with EEMD_E_TIMEOUT); 0 or
+        positive has no effect.
     cluster_size: CTAs sharing one signal (1..16; 9..16 are non-portable cluster sizes)."""
     tile: int = 0
     knots_per_block: int = 0

@@ -39,7 +39,8 @@ extern "C" {
 #define EEMD_E_BADARG          -1  /* invalid argument (maps to ValueError) */
 #define EEMD_E_NOMEM           -2  /* workspace smaller than eemd_workspace_size() */
 #define EEMD_E_KNOT_OVERFLOW   -3  /* knot buffer capacity exceeded (internal bound violated) */
-#define EEMD_E_TIMEOUT         -4  /* a bounded device wait gave up (watchdog) */
+#define EEMD_E_TIMEOUT         -4  /* a task exceeded its step bound, or the watchdog test
+                                         mode's bounded wait gave up */
 #define EEMD_E_CUDA            -5  /* CUDA runtime error */
 #define EEMD_E_NOTSUP          -6  /* unsupported combination (e.g. exact mode with float32) */
 #define EEMD_E_STATIC_CAPACITY -7  /* eemd_run_static(): the problem needs more scratch than
@@ -84,13 +85,17 @@ typedef struct eemd_params {
     int32_t  end_mode;        /* EEMD_END_* */
     int32_t  rules;           /* EEMD_RULES_* */
     int32_t  exact;           /* 1: reference operation order, IEEE division, no FMA (float64 only) */
-    int32_t  tile;            /* samples per tile of the fused sift pass (0 = autotune) */
-    int32_t  knots_per_block; /* owned rows per decay-seamed Thomas window (0 = autotune) */
-    int32_t  halo;            /* seam halo rows on each side of a window (0 = 32) */
-    int64_t  watchdog;        /* iteration limit of every bounded device wait (0 = 2^24);
-                                 a negative value -k is the watchdog test mode: every
-                                 look-back first waits on a flag nothing sets, gives up
-                                 after k polls and the run returns EEMD_E_TIMEOUT */
+    int32_t  tile;            /* samples per warp tile of the fused sift pass: 0, or the only
+                                 supported value (256 for float32, 128 for float64) */
+    int32_t  knots_per_block; /* owned rows per exact-mode seam window (0 = 16; the fast
+                                 solve owns 3 rows per window) */
+    int32_t  halo;            /* seam halo rows on each side of a window (0 = 32 exact,
+                                 24 fast float64, 16 fast float32) */
+    int64_t  watchdog;        /* >= 0: no effect (the engine has no device waits on its data
+                                 path; every loop is bounded by the sift and IMF caps);
+                                 a negative value -k is the watchdog test mode: every task
+                                 first waits on a flag nothing sets, gives up after k polls
+                                 and the run returns EEMD_E_TIMEOUT */
     int32_t  cluster_size;    /* CTAs (thread-block cluster) per task, 1..16 (0 = autotune; 9..16 are
                                  non-portable cluster sizes the device must support) */
     int32_t  reserved;
