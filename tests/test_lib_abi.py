@@ -147,3 +147,44 @@ def test_headers_are_plain_c99(tmp_path):
     r = subprocess.run([gcc, "-std=c99", "-pedantic-errors", "-Wall", "-Werror", "-fsyntax-only",
                         "-I", str(inc), str(src)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_c_program_links_and_calls_host_entry_points(tmp_path):
+    """A plain C program links against libeemd_b200.so through the header and
+    calls its host-only entry points (no GPU work): defaults, version,
+    workspace sizing, argument refusal and status strings."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("gcc not available")
+    lib = Path(L.lib_path())
+    src = tmp_path / "host.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include <string.h>
+#include "eemd_b200.h"
+int main(void) {
+    eemd_params p;
+    eemd_default_params(&p);
+    if (p.dtype != EEMD_F64 || p.max_sifts != 50 || p.tau != 0.25) return 1;
+    if (eemd_version() <= 0) return 2;
+    int64_t n[2] = {48000, 1000};
+    size_t ws = 0;
+    if (eemd_workspace_size(&p, n, 2, 10, 0, &ws) != EEMD_OK || ws == 0) return 3;
+    p.max_sifts = 0;
+    if (eemd_workspace_size(&p, n, 2, 10, 0, &ws) != EEMD_E_BADARG) return 4;
+    if (strlen(eemd_strerror(EEMD_E_BADARG)) == 0) return 5;
+    printf("%zu\n", ws);
+    return 0;
+}
+''')
+    exe = tmp_path / "host"
+    r = subprocess.run([gcc, "-std=c99", "-Wall", "-Werror", "-I", str(HEADER.parent), str(src),
+                        "-L", str(lib.parent), "-l:" + lib.name, "-Wl,-rpath," + str(lib.parent),
+                        "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert run.returncode == 0, (run.returncode, run.stderr)
+    p = L.default_params()
+    assert int(run.stdout) == L.workspace_size(p, [48000, 1000], 10, False)
