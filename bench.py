@@ -204,7 +204,11 @@ class CpuBaseline:
         self.pool.shutdown()
 
 
-def run_reference(args, wl: Workload):
+def run_reference(args, wl: Workload, metric: str = None, config: dict = None):
+    """The reference's CPU algorithm (the oracle port) on a bounded sample of
+    the workload, on all host cores; `metric` and `config` default to the
+    EEMD workload's and are passed where the GPU arm names its line
+    differently (CEEMDAN, the surrogate)."""
     rank, _, world = rank_env()
     if rank != 0:
         return 0
@@ -218,13 +222,13 @@ def run_reference(args, wl: Workload):
     cb.close()
     sec = sum(ts) / len(ts)
     v = cb.value(sec)
-    line = {"impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT,
+    line = {"impl": "reference", "metric": metric or METRIC, "value": round(v, 4), "unit": UNIT,
             "n_gpus": args.gpus, "steps": steps, "warmup": warm,
             "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             # the workload as the GPU arm names it; the CPU specifics (float64
             # arithmetic, the bounded sample of tasks) are in cpu_baseline.sample
-            "config": dict(wl.config),
+            "config": dict(config) if config is not None else dict(wl.config),
             "cpu_baseline": cb.describe(v),
             "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -629,6 +633,20 @@ def _surrogate_signal():
     return SU.make_signals([30000], 65536)
 
 
+SURROGATE_METRIC = "surrogate EEMD Msamples*trials/s (256-trial equivalent)"
+CEEMDAN_METRIC = "CEEMDAN Msamples*trials/s (per stage)"
+
+
+def surrogate_config(weights: str) -> dict:
+    """The surrogate workload as both arms name it."""
+    from eemd4cuda_b200 import surrogate as SU
+    return {"workload": "surrogate_8_to_256_trials", "N": 65536, "signals": SG_SIGNALS, "trials_small": 8,
+            "trials_equivalent": 256, "max_imf": 10, "sifts_per_imf": 10, "corrected_modes": SU.P_CORR,
+            "network": "dilated conv 8 layers x 64 ch, k=3, d=1..128, bf16 / f32 accumulate",
+            "weights": weights, "signals_seeds": "30000..30127 (held out)",
+            "l2": "flushed between timed steps (256 MiB write)"}
+
+
 def surrogate_cpu_workload() -> Workload:
     """The plain 256-trial EEMD the surrogate stands in for, as a CPU sample:
     tasks of one held-out 65536-sample signal, the first 2 of 10 IMFs (10
@@ -796,15 +814,11 @@ def run_surrogate(args):
         cb.close()
 
     line = {
-        "metric": "surrogate EEMD Msamples*trials/s (256-trial equivalent)", "value": round(value, 3),
+        "metric": SURROGATE_METRIC, "value": round(value, 3),
         "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32+f64",
         "data": "synthetic",
-        "config": {"workload": "surrogate_8_to_256_trials", "N": N, "signals": S, "trials_small": E_small,
-                   "trials_equivalent": E_big, "max_imf": 10, "sifts_per_imf": 10, "corrected_modes": SU.P_CORR,
-                   "network": "dilated conv 8 layers x 64 ch, k=3, d=1..128, bf16 / f32 accumulate",
-                   "weights": weights, "signals_seeds": "30000..30127 (held out)",
-                   "l2": "flushed between timed steps (256 MiB write)"},
+        "config": surrogate_config(weights),
         "speedup_vs_plain_256": round(plain_ms / ms, 2), "plain_256_ms": round(plain_ms, 3),
         "split_ms": {"ensemble_8": round(ens_ms, 3), "prepare": round(stage_ms, 3), "network": round(net_ms, 3)},
         "median_rel_l2_per_imf": {"surrogate": [round(float(v), 4) for v in es],
@@ -929,7 +943,7 @@ def run_ceemdan(args):
         cpu["sample"] += "; stage-1 tasks (first IMF of x + eps*std(x)*w), the unit of this line"
         cb.close()
     line = {
-        "metric": "CEEMDAN Msamples*trials/s (per stage)", "value": round(value, 3), "unit": UNIT, "n_gpus": 1,
+        "metric": CEEMDAN_METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": dict(wl.config, stages=stages, parallelism="replicas1",
@@ -1076,11 +1090,14 @@ def main():
         return run_spectra(args)
     if args.workload == "ceemdan48k":
         if args.impl == "reference":
-            return run_reference(args, CEEMDAN_WL)
+            return run_reference(args, CEEMDAN_WL, metric=CEEMDAN_METRIC)
         return run_ceemdan(args)
     if args.workload == "surrogate":
         if args.impl == "reference":
-            return run_reference(args, surrogate_cpu_workload())
+            w = (f"{SURROGATE_WEIGHTS.relative_to(ROOT)}" if SURROGATE_WEIGHTS.exists()
+                 else "trained in this run (256 signals, 2 candidates x 3000 steps)")
+            return run_reference(args, surrogate_cpu_workload(), metric=SURROGATE_METRIC,
+                                 config=surrogate_config(w))
         return run_surrogate(args)
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
