@@ -25,6 +25,7 @@ pool, on a bounded sample of the same workload.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -135,13 +136,45 @@ def rank_env():
 
 
 # ---------------------------------------------------------------------------
-# CPU side (reference algorithm, numpy port)
+# CPU side: the reference's own CPU code (baseline/_ref), else the numpy port
 # ---------------------------------------------------------------------------
-class CpuBaseline:
-    """emd_1d of (signal, trial) tasks of the workload in a spawn process pool.
+REF_DIR = ROOT / "baseline" / "_ref"
 
-    The sample is a bounded set of tasks (x + its trial noise, float64) so that
-    one step takes seconds.  With cpu_max_imf / cpu_max_sifts the sample runs
+
+def reference_installed() -> bool:
+    return (REF_DIR / "emd_ref.py").exists() and (REF_DIR / "emd_par.py").exists()
+
+
+def _ref_trial(args):
+    """One trial of the reference's CPU EEMD, run by the reference's own code:
+    emd_ref.emd_1d of the unmodified reference installed in baseline/_ref, on
+    x + the reference CPU path's per-trial noise (emd_par.py:112-119: numpy
+    default_rng((seed * 1000003 + e) mod 2^64), standard normals times
+    eps*std(x)); no noise for plain EMD (emd_par.py:148-151)."""
+    x, seed, e, sigma, kw = args
+    if str(REF_DIR) not in sys.path:
+        sys.path.insert(0, str(REF_DIR))
+    import emd_ref
+    t0 = time.perf_counter()
+    if sigma > 0:
+        rng = np.random.default_rng((seed * 1000003 + e) & 0xFFFFFFFFFFFFFFFF)
+        x = x + rng.standard_normal(len(x)) * sigma
+    imfs, resid, st = emd_ref.emd_1d(x, **kw)
+    return len(imfs), st["total_sifts"], time.perf_counter() - t0
+
+
+class CpuBaseline:
+    """The reference's CPU algorithm on (signal, trial) tasks of the workload
+    in a spawn process pool with dynamic scheduling.
+
+    kind "reference": the reference's own emd_ref.emd_1d (baseline/_ref) with
+    the reference CPU path's noise stream, as emd_par._cpu_decompose runs it
+    (emd_par.py:139-183); the pool passes max_imf on, which the stock ensemble
+    path does not (emd_par.py:118-119 drops it, so decompose(method='cpu',
+    E>1) would decompose every mode rather than the workload's).  kind
+    "port": the numpy restatement in oracle/ when the reference is not
+    installed.  The sample is a bounded set of tasks (float64) so that one
+    step takes seconds.  With cpu_max_imf / cpu_max_sifts the sample runs
     only the first sifts, and `value` scales the time per sift to a full
     task's sift count."""
 
@@ -150,21 +183,23 @@ class CpuBaseline:
         from concurrent.futures import ProcessPoolExecutor
 
         self.wl = wl
+        self.kind = "reference" if reference_installed() else "port"
         self.cores = 1 if wl.E == 1 else (os.cpu_count() or 1)
         sig = wl.signals()
         rng = np.random.default_rng(wl.seed)
         n_tasks = wl.cpu_tasks or max(4, min(self.cores, 32))
-        self.tasks = []
-        for _ in range(n_tasks):
-            s = int(rng.integers(len(sig))) if len(sig) > 1 else 0
-            x = sig[s].astype(wl.np_dtype).astype(np.float64)
-            if wl.E > 1:
-                noise = rng.standard_normal(len(x)) * (wl.eps * np.std(x))
-            else:
-                noise = np.zeros(len(x))
-            self.tasks.append((x, noise))
         self.kw = dict(tau=wl.tau, max_sifts=wl.cpu_max_sifts or wl.max_sifts,
                        max_imf=wl.cpu_max_imf or wl.max_imf, end=wl.end)
+        self.tasks = []
+        for e in range(n_tasks):
+            s = int(rng.integers(len(sig))) if len(sig) > 1 else 0
+            x = sig[s].astype(wl.np_dtype).astype(np.float64)
+            sigma = wl.eps * np.std(x) if wl.E > 1 else 0.0
+            if self.kind == "reference":
+                self.tasks.append((x, wl.seed, e, sigma, self.kw))
+            else:
+                noise = rng.standard_normal(len(x)) * sigma if wl.E > 1 else np.zeros(len(x))
+                self.tasks.append((x, noise, self.kw))
         self.pool = ProcessPoolExecutor(max_workers=self.cores, mp_context=mp.get_context("spawn"))
         self.sifts_done = 0
         self.full_sifts = None
@@ -173,8 +208,9 @@ class CpuBaseline:
         from concurrent.futures import as_completed
         from oracle import emd_oracle as O
 
+        fn = _ref_trial if self.kind == "reference" else O._trial_worker
         t0 = time.perf_counter()
-        futs = [self.pool.submit(O._trial_worker, (x, nz, self.kw)) for x, nz in self.tasks]
+        futs = [self.pool.submit(fn, t) for t in self.tasks]
         sifts = 0
         for f in as_completed(futs):
             sifts += f.result()[1]
@@ -182,7 +218,7 @@ class CpuBaseline:
         return time.perf_counter() - t0
 
     def value(self, seconds: float, full_sifts_per_task: float | None = None) -> float:
-        samples = sum(len(x) for x, _ in self.tasks)
+        samples = sum(len(t[0]) for t in self.tasks)
         if self.wl.cpu_max_imf or self.wl.cpu_max_sifts:
             self.full_sifts = full_sifts_per_task or self.wl.max_imf * self.wl.max_sifts / 2
             seconds *= self.full_sifts / max(self.sifts_done / len(self.tasks), 1e-9)
@@ -190,14 +226,17 @@ class CpuBaseline:
 
     def describe(self, v: float) -> dict:
         wl = self.wl
-        what = (f"{len(self.tasks)} (signal, trial) tasks of the workload (emd_1d, float64 "
+        who = ("the reference's own emd_ref.emd_1d (unmodified, installed in baseline/_ref) with its "
+               "CPU path's per-trial noise stream" if self.kind == "reference"
+               else "emd_1d of the numpy restatement in oracle/")
+        what = (f"{len(self.tasks)} (signal, trial) tasks of the workload ({who}, float64 "
                 f"arithmetic on the workload's {'float32-rounded ' if wl.dtype == 'f32' else ''}signal, "
                 f"tau={wl.tau}, max_sifts={self.kw['max_sifts']}, max_imf={self.kw['max_imf']}, "
-                f"{wl.end} ends) in a {self.cores}-process pool")
+                f"{wl.end} ends) in a {self.cores}-process pool with dynamic scheduling")
         if wl.cpu_max_imf or wl.cpu_max_sifts:
             what += (f"; the time per sift of IMF 1 scaled to {self.full_sifts:.1f} sifts per task "
                      "(IMF-1 sifts are the slowest, so this bounds the CPU time from above)")
-        return {"value": round(v, 4), "unit": UNIT, "cores": self.cores, "kind": "port",
+        return {"value": round(v, 4), "unit": UNIT, "cores": self.cores, "kind": self.kind,
                 "sample": what}
 
     def close(self):
@@ -222,13 +261,21 @@ def run_reference(args, wl: Workload, metric: str = None, config: dict = None):
     cb.close()
     sec = sum(ts) / len(ts)
     v = cb.value(sec)
+    # the workload as the GPU arm names it, with what this arm actually runs:
+    # float64 storage and arithmetic, the reference CPU path's noise stream, a
+    # bounded sample of tasks (cpu_baseline.sample)
+    cfg = dict(config) if config is not None else dict(wl.config)
+    if "storage" in cfg:
+        cfg["storage"] = "float64"
+    if "noise" in cfg:
+        cfg["noise"] = ("numpy default_rng per trial (the reference CPU path's stream, emd_par.py:112-119)"
+                        if cb.kind == "reference" else "numpy default_rng")
+    cfg["tasks_per_step"] = len(cb.tasks)
     line = {"impl": "reference", "metric": metric or METRIC, "value": round(v, 4), "unit": UNIT,
             "n_gpus": args.gpus, "steps": steps, "warmup": warm,
             "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            # the workload as the GPU arm names it; the CPU specifics (float64
-            # arithmetic, the bounded sample of tasks) are in cpu_baseline.sample
-            "config": dict(config) if config is not None else dict(wl.config),
+            "config": cfg,
             "cpu_baseline": cb.describe(v),
             "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -413,6 +460,86 @@ class Engine:
         return (self.wl.E + self.batch - 1) // self.batch
 
 
+def accuracy_check(wl: Workload, dev, pool, seed: int) -> dict:
+    """Error of the engine against the float64 CPU oracle (emd_ref.py's
+    algorithm, oracle/emd_oracle.py) on identical trial inputs: the
+    workload's Philox noise for a few trials is drawn on the device, the
+    perturbed inputs are rounded to the storage type, and both sides
+    decompose exactly those rows with the workload's settings (the engine in
+    its default fast mode, as timed).  Runs outside the timed region; the
+    oracle is the checker here, never the thing measured."""
+    import torch
+    from eemd4cuda_b200 import _lib as L
+    from eemd4cuda_b200 import emd_par as M
+    from oracle import emd_oracle as O
+
+    sig = wl.signals()
+    max_imf, max_sifts, tau = wl.max_imf, wl.max_sifts, wl.tau
+    if wl.name == "uneven512":
+        picks, trials, scope = sorted(range(len(sig)), key=lambda i: len(sig[i]))[:4], 1, \
+            "full decomposition of trial 0 of the 4 shortest signals"
+    elif wl.name == "amfm4m":
+        # a full float64 oracle decomposition of 2^22 samples takes hours on one core
+        picks, trials, max_imf, max_sifts = [0], 1, 1, 2
+        scope = "first 2 sifts of IMF 1 of trial 0 (the float64 oracle runs about 5 s per sift here)"
+    else:
+        picks, trials = [0], (4 if wl.E > 1 else 1)
+        scope = f"full decomposition of trials 0..{trials - 1}"
+    rows, keys = [], []
+    for s in picks:
+        x = sig[s].astype(wl.np_dtype).astype(np.float64)
+        for e in range(trials):
+            if wl.E > 1:
+                nz = torch.empty((len(x),), dtype=torch.float64, device=dev)
+                L.philox_normals(seed, s, e, 1, len(x), nz)
+                row = x + wl.eps * np.std(x) * nz.cpu().numpy()
+            else:
+                row = x
+            rows.append(row.astype(wl.np_dtype))
+            keys.append((s, e))
+    cfg = M.EngineConfig(halo=wl.halo) if wl.halo else None
+    p = M.make_params(dtype=wl.np_dtype, noise_mode=L.EEMD_NOISE_PREPERTURBED, tau=tau,
+                      max_sifts=max_sifts, max_imf=max_imf, end=wl.end, config=cfg)
+    lengths = [len(r) for r in rows]
+    tdt = torch.float32 if wl.dtype == "f32" else torch.float64
+    xd = torch.from_numpy(np.concatenate(rows)).to(dev)
+    imfs = torch.zeros((max_imf * sum(lengths),), dtype=tdt, device=dev)
+    nmode = torch.zeros((len(rows),), dtype=torch.int32, device=dev)
+    klog = torch.full((len(rows), max_imf, max_sifts, 2), -1, dtype=torch.int32, device=dev)
+    ws = torch.empty((L.workspace_size(p, lengths, 1, True),), dtype=torch.uint8, device=dev)
+    L.run(p, xd, lengths, 0, 1, ws, imfs=imfs, nmode=nmode, knot_log=klog)
+    im = imfs.double().cpu().numpy()
+    nm = nmode.cpu().numpy()
+    kl = klog.cpu().numpy()
+    del ws, imfs, xd
+    kw = dict(tau=tau, max_sifts=max_sifts, max_imf=max_imf, end=wl.end)
+    ref = list(pool.map(O._imfs_worker, [(r.astype(np.float64), kw) for r in rows]))
+    per_imf = np.zeros(max_imf)
+    stack, same, total, modes_equal, off = 0.0, 0, 0, True, 0
+    for i, (r, (o, olog)) in enumerate(zip(rows, ref)):
+        n = len(r)
+        g = im[off:off + max_imf * n].reshape(max_imf, n)
+        off += max_imf * n
+        modes_equal = modes_equal and int(nm[i]) == len(o)
+        m = min(int(nm[i]), len(o))
+        for k in range(m):
+            den = np.linalg.norm(o[k])
+            if den > 0:
+                per_imf[k] = max(per_imf[k], float(np.linalg.norm(g[k] - o[k]) / den))
+        stack = max(stack, float(np.linalg.norm(g[:m] - o[:m]) / np.linalg.norm(r.astype(np.float64))))
+        for mm, mode in enumerate(olog):
+            for k, ab in enumerate(mode):
+                total += 1
+                same += int(mm < max_imf and kl[i, mm, k].tolist() == list(ab))
+    return {"reference": "float64 CPU oracle (emd_ref.py algorithm) on the same storage-rounded trial inputs",
+            "scope": scope, "trials_checked": len(rows),
+            "max_rel_l2_vs_fp64_oracle": float(per_imf.max()),
+            "max_rel_l2_per_imf": [float(f"{v:.3e}") for v in per_imf],
+            "stack_rel_l2_vs_fp64_oracle": float(f"{stack:.3e}"),
+            "mode_counts_equal": bool(modes_equal),
+            "sifts_with_identical_knot_counts": f"{same}/{total}"}
+
+
 def run_ours(args, wl: Workload):
     import torch
 
@@ -568,6 +695,58 @@ def run_ours(args, wl: Workload):
         del engs
         torch.cuda.empty_cache()
 
+    # ---- float64 storage beside the float32 headline (the reference's own precision) ----
+    f64_line = None
+    if wl.dtype == "f32" and wl.name == "harmonic48k":
+        wl64 = dataclasses.replace(wl, dtype="f64", _signals=wl.signals())
+        eng64 = Engine(wl64, dev, wl.seed + rank)
+        for _ in range(args.warmup):
+            eng64.step()
+        torch.cuda.synchronize()
+        ms64 = 0.0
+        for _ in range(args.steps):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            eng64.step()
+            e1.record(stream)
+            e1.synchronize()
+            ms64 += e0.elapsed_time(e1)
+        ms64 /= args.steps
+        t64 = L.KernelTimes()
+        kl64 = torch.full((n_first, wl.max_imf, wl.max_sifts, 2), -1, dtype=torch.int32, device=dev)
+        nm64 = torch.zeros((n_first,), dtype=torch.int32, device=dev)
+        flush.fill_(1)
+        eng64.step(times=t64, klog=kl64, nmode=nm64)
+        torch.cuda.synchronize()
+        ev64 = t64.as_dict()["emd"]
+        b64 = emd_algorithmic_bytes(kl64.cpu().numpy(), nm64.cpu().numpy(), eng64.lengths, eng64.batch, 8)
+        gbs64 = b64 / (ev64["ms"] / 1e3) / 1e9 if ev64["ms"] > 0 else 0.0
+        f64_line = {"dtype": "f64", "value": round(world * samples_trials / (ms64 / 1e3) / 1e6, 3),
+                    "unit": UNIT, "ms_per_step": round(ms64, 4),
+                    "roofline": {"kernel": "k_emd", "achieved": round(gbs64, 2), "peak": peak,
+                                 "unit": "GB/s", "frac": round(gbs64 / peak, 4),
+                                 "algorithmic_bytes_per_launch": round(b64 / max(ev64["launches"], 1)),
+                                 "avg_launch_ms": round(ev64["ms"] / max(ev64["launches"], 1), 5)}}
+        del eng64
+        torch.cuda.empty_cache()
+
+    # ---- error against the float64 CPU oracle (rank 0, outside the timed region) ----
+    accuracy, acc64 = None, None
+    if rank == 0:
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        pool = cb.pool if cb is not None else ProcessPoolExecutor(
+            max_workers=min(8, os.cpu_count() or 1), mp_context=mp.get_context("spawn"))
+        accuracy = accuracy_check(wl, dev, pool, wl.seed + rank)
+        if f64_line is not None:
+            acc64 = accuracy_check(dataclasses.replace(wl, dtype="f64", _signals=wl.signals()), dev, pool,
+                                   wl.seed + rank)
+            f64_line["accuracy"] = acc64
+        if cb is None:
+            pool.shutdown()
+
     cpu = None
     if cb is not None:
         cb.step()  # warm the pool's imports
@@ -604,6 +783,10 @@ def run_ours(args, wl: Workload):
     }
     if per_signal is not None:
         line["per_signal_launches"] = per_signal
+    if accuracy is not None:
+        line["accuracy"] = accuracy
+    if f64_line is not None:
+        line["float64_storage"] = f64_line
     if cpu is not None:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)

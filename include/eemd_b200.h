@@ -4,10 +4,13 @@
  * The engine runs Ensemble Empirical Mode Decomposition of many signals x
  * many noise trials on one sm_100a GPU.  Every pointer argument marked
  * "device" is a CUDA device pointer owned by the caller; "host" pointers are
- * read during the call only.  The library allocates no device memory: all
- * scratch lives in the caller's workspace (size from eemd_workspace_size()).
- * It keeps no global state; calls on different workspaces may overlap, calls
- * on the same workspace must not.
+ * read during the call only.  The library allocates no device memory: the
+ * scratch of eemd_run() lives in the caller's workspace (size from
+ * eemd_workspace_size()); calls on different workspaces may overlap, calls on
+ * the same workspace must not.  The one piece of library-owned device memory
+ * and global state is the fixed-size static scratch array of eemd_run_static()
+ * (EEMD_STATIC_SCRATCH_BYTES on every GPU that loads the library, plus a
+ * per-device cache of its address); nothing else is kept between calls.
  *
  * Reference interface this replaces (misureaudio/EEMD4CUDA, Python):
  *   - emd_gpu.py:301-334 gpu_eemd_full(x[E,N], E, tau, max_sifts, max_imf)
@@ -19,8 +22,7 @@
  *       (extrema scan, spline system, Thomas / seam-window Thomas, spline
  *       evaluation, SD stop rule, IMF store)           => internal kernels
  * Python binds these through ctypes (eemd4cuda_b200/_lib.py); the same
- * declarations are what a cffi / ctypes stub in the reference would bind
- * (see INTEGRATION.md).
+ * declarations are what a cffi / ctypes stub in the reference would bind.
  */
 #ifndef EEMD_B200_H
 #define EEMD_B200_H
@@ -186,15 +188,20 @@ int32_t eemd_run_traced(const eemd_params* p, const void* x, const int64_t* leng
 #define EEMD_STATIC_SCRATCH_BYTES (64u * 1024u * 1024u)
 
 /* eemd_run() without a workspace argument, for callers that cannot allocate
- * device memory: code running inside a CUDA-graph capture or a real-time audio
- * callback (where cudaMalloc would break the capture or block the thread), and
- * host applications whose device memory is owned by another allocator.  The
- * engine's scratch is the library's own static device array of
- * EEMD_STATIC_SCRATCH_BYTES; problems whose eemd_workspace_size() exceeds it are
- * rejected with EEMD_E_STATIC_CAPACITY before any GPU work.  The caller still
- * passes x and the outputs.  The first call on each device looks the array up
- * (cudaGetSymbolAddress with that device current), so make that first call
- * before any stream capture.  All calls share the one array and it keeps the
+ * device memory themselves: host applications whose device memory is owned by
+ * another allocator or framework (a memory pool that hands out no raw
+ * buffers, a plugin host that forbids device allocations from plugins), or
+ * code that has no allocator at hand at all.  The engine's scratch is the
+ * library's own static device array of EEMD_STATIC_SCRATCH_BYTES; problems
+ * whose eemd_workspace_size() exceeds it are rejected with
+ * EEMD_E_STATIC_CAPACITY before any GPU work.  The caller still passes x and
+ * the outputs.  The first call on each device looks the array up
+ * (cudaGetSymbolAddress with that device current) and caches the address for
+ * the life of the process, so make that first call before any stream capture,
+ * and do not reset the device (cudaDeviceReset) between calls: the cached
+ * address would then be stale.  The call is synchronous like eemd_run(): it
+ * copies the task descriptors from host memory, waits for the stream and reads
+ * the device status back.  All calls share the one array and it keeps the
  * previous call's contents (the engine re-initialises what it reads), so calls
  * that overlap on the GPU -- on different streams or host threads -- race and
  * must be serialised by the caller.  No cudaMalloc, cudaFree or allocating

@@ -351,6 +351,14 @@ def _trial_worker(args):
     return len(imfs), st["total_sifts"], time.perf_counter() - t0
 
 
+def _imfs_worker(args):
+    """emd_1d of one prepared trial input (float64): the IMF stack [n_modes, N]
+    and the per-sift knot counts, for accuracy checks against the engine."""
+    x, kw = args
+    imfs, _, st = emd_1d(np.asarray(x, dtype=np.float64), record_knots=True, **kw)
+    return np.array(imfs), st["knot_log"]
+
+
 def timed_pool_eemd(x, noises, n_workers, **kw):
     """Run emd_1d on x + noises[e] in a spawn process pool with dynamic
     scheduling; returns (wall seconds, per-trial (n_modes, sifts, seconds))."""

@@ -1,6 +1,6 @@
 """Generate the CEEMDAN fixtures from the reference implementation itself.
 
-    python tests/golden/make_ceemdan_golden.py /root/reference
+    python tests/golden/make_ceemdan_golden.py <reference checkout>
 
 Imports the reference's emd_ref.py and runs its ceemdan() serially
 (parallel=False) on small seeded signals, and its emd_1d() on the stage-0
@@ -52,4 +52,6 @@ def main(ref_dir: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <path of the reference checkout>")
+    main(sys.argv[1])

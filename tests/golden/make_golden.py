@@ -2,7 +2,7 @@
 
 Run in a container that holds the reference checkout (misureaudio/EEMD4CUDA):
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout>
 
 It imports the reference's emd_ref.py / refsignal.py / emd_gpu.py (the last
 under numba's CUDA simulator, NUMBA_ENABLE_CUDASIM=1, so the reference GPU
@@ -187,4 +187,6 @@ def main(ref: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <path of the reference checkout>")
+    main(sys.argv[1])

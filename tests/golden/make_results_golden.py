@@ -1,6 +1,6 @@
 """Generate the result-format fixtures from the reference implementation itself.
 
-    python tests/golden/make_results_golden.py /root/reference
+    python tests/golden/make_results_golden.py <reference checkout>
 
 Runs the reference's audio_eemd/report.py write_imfs_npz (loaded as a module
 under a bare package stand-in, so the package's audio dependencies are not
@@ -56,4 +56,6 @@ def main(ref_dir: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <path of the reference checkout>")
+    main(sys.argv[1])

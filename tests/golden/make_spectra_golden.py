@@ -1,6 +1,6 @@
 """Generate the spectra fixtures from the reference implementation itself.
 
-    python tests/golden/make_spectra_golden.py /root/reference
+    python tests/golden/make_spectra_golden.py <reference checkout>
 
 Loads the reference's audio_eemd/spectra.py (its stft_block and hilbert_if,
 on scipy.signal) as a module and runs them on small seeded IMF-like signals;
@@ -62,4 +62,6 @@ def main(ref_dir: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <path of the reference checkout>")
+    main(sys.argv[1])

@@ -1,11 +1,11 @@
 """Host-side logic of the drop-in API (no GPU needed): validation and error
-mapping (emd_par.py:282-286, eemd_stage.py:66-77), result container,
-reference noise streams, IMF slot bound."""
+mapping (emd_par.py:282-286; the reference's own eemd_stage.py:66-77 on top),
+result container, reference noise streams, IMF slot bound."""
 import numpy as np
 import pytest
 
 from eemd4cuda_b200 import emd_par as M
-from eemd4cuda_b200.eemd_stage import EEMDError, run_eemd
+import ref_stage
 from oracle import emd_oracle as O
 
 
@@ -20,13 +20,16 @@ def test_bad_input_raises_value_error():
         M.decompose(np.ones(100), method="quantum")
 
 
-def test_stage_maps_bad_input():
-    """audio_eemd/tests/test_eemd_stage.py:65-69: np.ones(5) -> eemd.bad_input."""
-    with pytest.raises(EEMDError) as ei:
-        run_eemd(np.ones(5), method="gpu", E=1)
+def test_stage_maps_bad_input(monkeypatch):
+    """audio_eemd/tests/test_eemd_stage.py:65-69 through the reference's own
+    stage adapter on the compat module: np.ones(5) -> eemd.bad_input, and the
+    CPU method this engine does not offer -> eemd.bad_input."""
+    stage = ref_stage.load(monkeypatch)
+    with pytest.raises(stage.EEMDError) as ei:
+        stage.run_eemd(np.ones(5), method="gpu", E=1)
     assert ei.value.code == "eemd.bad_input"
-    with pytest.raises(EEMDError) as ei:
-        run_eemd(np.ones(100), method="cpu", E=1)
+    with pytest.raises(stage.EEMDError) as ei:
+        stage.run_eemd(np.ones(100), method="cpu", E=1)
     assert ei.value.code == "eemd.bad_input"
 
 

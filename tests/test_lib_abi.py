@@ -37,6 +37,25 @@ def test_checked_build_exports_too():
         assert hasattr(lib, name), name
 
 
+def test_header_constants_match_the_binding():
+    """Every status code, mode constant and the static scratch size that the
+    ctypes binding hard-codes equal the header's #defines."""
+    text = HEADER.read_text()
+    defs = {}
+    for name, val in re.findall(r"#define\s+(EEMD_[A-Z0-9_]+)\s+(\S[^/\n]*)", text):
+        defs[name] = val.strip()
+    m = re.fullmatch(r"\((\d+)u \* (\d+)u \* (\d+)u\)", defs["EEMD_STATIC_SCRATCH_BYTES"])
+    assert m, defs["EEMD_STATIC_SCRATCH_BYTES"]
+    assert int(m[1]) * int(m[2]) * int(m[3]) == L.STATIC_SCRATCH_BYTES
+    checked = 0
+    for name, val in defs.items():
+        if hasattr(L, name) and re.fullmatch(r"-?\d+", val):
+            assert getattr(L, name) == int(val), name
+            checked += 1
+    assert int(defs["EEMD_ABI_VERSION"]) == L.ABI_VERSION
+    assert checked >= 19
+
+
 def test_version_and_strerror():
     lib = L.load()
     assert lib.eemd_version() == L.ABI_VERSION
