@@ -102,7 +102,14 @@ def load() -> ctypes.CDLL:
     global _LIB
     if _LIB is not None:
         return _LIB
-    path = lib_path()
+    _LIB = load_variant(lib_path())
+    return _LIB
+
+
+def load_variant(path) -> ctypes.CDLL:
+    """Load and type a build of the engine library at `path` (for example the
+    bounds-checked build) next to the default one; raise if it is absent."""
+    path = Path(path)
     if not path.exists():
         raise RuntimeError(
             f"EEMD engine library not found at {path}; build it with "
@@ -138,7 +145,6 @@ def load() -> ctypes.CDLL:
     v = lib.eemd_version()
     if v != ABI_VERSION:
         raise RuntimeError(f"{path}: ABI version {v}, expected {ABI_VERSION}")
-    _LIB = lib
     return lib
 
 
@@ -189,9 +195,10 @@ def _ptr(t) -> int | None:
 def run(p: EemdParams, x, lengths, trial_begin: int, trial_count: int, ws, *, noise=None,
         imfs=None, resid_out=None, imf_sum=None, mode_count=None, nsift=None, nmode=None,
         mode_sifts=None, knot_log=None, flags=None, stream=None, times: KernelTimes | None = None,
-        ws_bytes: int | None = None) -> None:
+        ws_bytes: int | None = None, lib: ctypes.CDLL | None = None) -> None:
     """eemd_run on torch device tensors (all optional outputs may be None).
-    With `times`, runs eemd_run_traced and fills per-kernel event timings."""
+    With `times`, runs eemd_run_traced and fills per-kernel event timings.
+    `lib`: another build of the library (load_variant) instead of the default."""
     import torch
 
     la = lengths_array(lengths)
@@ -201,10 +208,11 @@ def run(p: EemdParams, x, lengths, trial_begin: int, trial_count: int, ws, *, no
             int(trial_count), _ptr(noise), _ptr(imfs), _ptr(resid_out), _ptr(imf_sum),
             _ptr(mode_count), _ptr(nsift), _ptr(nmode), _ptr(mode_sifts),
             _ptr(knot_log), _ptr(flags), _ptr(ws), nb, c_void_p(st))
+    lib = lib or load()
     if times is None:
-        rc = load().eemd_run(*args)
+        rc = lib.eemd_run(*args)
     else:
-        rc = load().eemd_run_traced(*args, ctypes.byref(times))
+        rc = lib.eemd_run_traced(*args, ctypes.byref(times))
     check(rc, "eemd_run")
 
 

@@ -211,6 +211,7 @@ constexpr int MAXSEG = MAXC * NWARP;  // knot segments per task: one per warp of
 struct Xchg {              // one CTA's published segment results (DSMEM-visible)
     double num, den;       // SD partial sums of the segment
     int cnt[2][NWARP];     // new knots (maxima, minima) found by each warp
+    int err;               // this CTA raised an error during the step: the task stops
 };
 
 struct TaskSm {
@@ -223,7 +224,34 @@ struct TaskSm {
     double yfirst[2], ylast[2];  // values of the virtual mirror knots
     double cval[2];            // constant envelope when P == 1
     int rcur;                  // current residual: 0 = the task's residual array, 1 = slot scratch
+    int err;                   // this CTA raised an error during the current step
+    int setup_fail;            // step_setup found a capacity exceeded (identical in every CTA)
 };
+
+// An error of the running task: recorded in the header (first error wins) and
+// in the CTA's step flag, which decide() ORs over the cluster so that every
+// CTA stops the task at the same step (no further step reads what the failed
+// step left behind).
+__device__ __forceinline__ void task_error(const Ctx& C, TaskSm& S, int code) {
+    raise_error(C.hdr, code, S.task);
+    S.err = 1;
+}
+
+#ifdef EEMD_CHECKED
+// checked build: an interval record index outside [0, hi] is reported and
+// clamped instead of read out of bounds
+#define EEMD_CHECK_IV(k, hi)                                     \
+    do {                                                         \
+        if ((k) < 0 || (k) > (hi)) {                             \
+            task_error(C, S, EEMD_E_KNOT_OVERFLOW);              \
+            (k) = max(0, min((k), (hi)));                        \
+        }                                                        \
+    } while (0)
+#else
+#define EEMD_CHECK_IV(k, hi) \
+    do {                     \
+    } while (0)
+#endif
 
 // Per-warp sweep geometry for storage type T.  A warp tile is WT = 32*RUN
 // samples; each warp owns, in dynamic shared memory, two tile buffers per
@@ -239,7 +267,12 @@ struct Geo {
     static constexpr size_t RI_BYTES = (size_t)2 * 32 * 16;             // [buf][lane]
     static constexpr int KCAP = WT / 2 + 4;                              // knots of one kind in a tile
     static constexpr size_t KN_BYTES = (size_t)2 * KCAP * (4 + sizeof(T));  // [kind][KCAP] index, value
-    static constexpr size_t WARP_BYTES = TB_BYTES + RI_BYTES + KN_BYTES;
+    // fast mode: the interval records a tile's runs read, staged in shared
+    // memory one tile ahead ([env][CAPR] records; a tile with more knots reads
+    // the rest from global memory)
+    static constexpr int CAPR = 48;
+    static constexpr size_t RST_BYTES = STAGE_RECS ? (size_t)2 * CAPR * RS * sizeof(T) : 0;
+    static constexpr size_t WARP_BYTES = TB_BYTES + RI_BYTES + KN_BYTES + RST_BYTES;
     static_assert(TB_BYTES % 16 == 0 && (RS * sizeof(T)) % 16 == 0 && KN_BYTES % 16 == 0,
                   "16-byte aligned layouts");
 };
@@ -259,10 +292,14 @@ __host__ __device__ inline int stage_slot(int k) {
 
 __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 
-// per-warp solve staging: slopes (double), knot times (int), knot values (storage type)
+// rows of one fast-solve pass: 32 lanes of FAST_B rows
+constexpr int FAST_ROWS = 32 * FAST_B;
+
+// per-warp solve staging: slopes (double), knot times (int), knot values
+// (storage type), and the fast solve's forward (c, d) of a pass's rows
 __host__ __device__ inline size_t wsolve_bytes(size_t bt) {
     const size_t sp = (size_t)stage_pad(WSCAP);
-    return align16(sp * 8) + align16(sp * 4) + align16(sp * bt);
+    return align16(sp * 8) + align16(sp * 4) + align16(sp * bt) + (size_t)FAST_ROWS * 16;
 }
 
 // dynamic shared memory of k_emd: the sweep's and the solve's per-warp areas overlay
@@ -318,7 +355,7 @@ __device__ __forceinline__ void real_knot(const Ctx& C, const Slot& sl, const Ta
 // finds the segment of its first real knot by binary search and then walks
 // forward, since its later knots follow in the same or later segments.
 template <typename T, bool EXACT>
-__device__ __forceinline__ void stage_range(const Ctx& C, const Slot& sl, const TaskSm& S, int env, int rlo,
+__device__ __forceinline__ void stage_range(const Ctx& C, const Slot& sl, TaskSm& S, int env, int rlo,
                                             int kcount, int* skt, T* sky, int lane) {
     const int* pr = S.pref[S.kpar][env];
     const int nseg = S.csize * NWARP;
@@ -343,6 +380,12 @@ __device__ __forceinline__ void stage_range(const Ctx& C, const Slot& sl, const 
         }
         if (r < 0) r = seg_of(pr, 0, nseg, i2);
         while (r + 1 < nseg && i2 >= pr[r + 1]) ++r;
+#ifdef EEMD_CHECKED
+        if (i2 < 0 || i2 >= P || i2 - pr[r] >= C.segcap) {
+            task_error(C, S, EEMD_E_KNOT_OVERFLOW);
+            continue;
+        }
+#endif
         const int64_t o = knot_index(C, S.kpar, env, r, i2 - pr[r]);
         cp_async4(kt_s, sl.kt + o);
         cp_async_el<T>(ky_s, static_cast<const T*>(sl.ky) + o);
@@ -458,72 +501,51 @@ __device__ void window_exact(const Ctx& C, const int* skt, const T* sky, const d
     if (o1 == n - 1) put(p2 - 1, 0.0);
 }
 
-// fast: twisted factorisation of the window.  A left sweep (LU, coupling
-// dropped at w0) keeps its (c, d) for the owned rows in registers; a right
-// sweep (UL, coupling dropped at w1) meets it, and each owned unknown is
-//   x_i = (r_i - l_i d_{i-1} - u_i g_{i+1}) / (dg_i - l_i c_{i-1} - u_i e_{i+1}).
+// fast: each lane owns FAST_B consecutive rows of a pass.  The forward
+// elimination (coupling dropped S rows before the lane's first row, where the
+// influence of the neglected rows has decayed like prod c_i) stores (c_i, d_i)
+// of the owned rows in the warp's shared memory; after __syncwarp each
+// committing lane back-substitutes from S rows past its last row (x there
+// truncated to d, the neglected term decaying the same way) down to its first
+// row and writes the monomial interval records of its rows.  The lanes of a
+// pass's last H = ceil(S / FAST_B) windows only provide that right halo
+// (unless the pass reaches the envelope's last row) and are solved for good
+// by the next pass.  Per owned row: (S + FAST_B) / FAST_B eliminated rows and
+// as many back-substitution steps (one fused multiply-add each).
 template <typename T>
-__device__ void window_fast(const Ctx& C, const int* skt, const T* sky, const double* ssl, int base, int n,
-                            int w, const Rec<T>& R, int p2) {
+__device__ __forceinline__ void window_fast_fwd(const int* skt, const double* ssl, int base, int n, int w, int S,
+                                                double2* cd, int cdbase) {
     constexpr bool kExact = false;
-    const int S = C.S;
     const int o0 = w * FAST_B;
-    const int cnt = min(FAST_B, n - o0);
-    const int o1 = o0 + cnt - 1;
-    const int w0 = max(0, o0 - S);
-    const int w1 = min(n - 1, o1 + S);
-    double fc[FAST_B], fd[FAST_B];
-    double cp = 0.0, dp = 0.0, cq = 0.0, dq = 0.0;  // (cq, dq): forward state after row o0-2
-    int ta = SKT(w0 - base), tb = SKT(w0 + 1 - base);
-    double sa = SSL(w0 - base);
-    for (int i = w0; i <= o0 - 2; ++i) {
+    const int o1 = min(n, o0 + FAST_B) - 1;
+    const int r0 = max(0, o0 - S);
+    double cp = 0.0, dp = 0.0;
+    int ta = SKT(r0 - base), tb = SKT(r0 + 1 - base);
+    double sa = SSL(r0 - base);
+    for (int i = r0; i <= o1; ++i) {
         const int tc = SKT(i + 2 - base);
         const double sb = SSL(i + 1 - base);
         const Row rw = row_of(ta, tb, tc, sa, sb, i, n);
         const double inv = fast_rcp(fma(-rw.l, cp, rw.dg));
         cp = rw.u * inv;
         dp = fma(-rw.l, dp, rw.r) * inv;
+        if (i >= o0) cd[i - cdbase] = make_double2(cp, dp);
         ta = tb;
         tb = tc;
         sa = sb;
     }
-    cq = cp;
-    dq = dp;
-    // forward state after rows o0-1 .. o1-1 (row -1 does not exist: zero state)
-#pragma unroll
-    for (int k = 0; k < FAST_B; ++k) {
-        const int i = o0 - 1 + k;
-        if (k < cnt) {
-            if (i >= 0) {
-                const int tc = SKT(i + 2 - base);
-                const double sb = SSL(i + 1 - base);
-                const Row rw = row_of(ta, tb, tc, sa, sb, i, n);
-                const double inv = fast_rcp(fma(-rw.l, cp, rw.dg));
-                cp = rw.u * inv;
-                dp = fma(-rw.l, dp, rw.r) * inv;
-                ta = tb;
-                tb = tc;
-                sa = sb;
-            }
-            fc[k] = cp;
-            fd[k] = dp;
-        }
-    }
-    // right sweep from w1 down to o1+1, then combine over the owned rows
-    double e = 0.0, g = 0.0;
-    int ub = SKT(w1 + 1 - base), uc = SKT(w1 + 2 - base);
-    double vb = SSL(w1 + 1 - base);
-    for (int i = w1; i > o1; --i) {
-        const int ua = SKT(i - base);
-        const double va = SSL(i - base);
-        const Row rw = row_of(ua, ub, uc, va, vb, i, n);
-        const double inv = fast_rcp(fma(-rw.u, e, rw.dg));
-        e = rw.l * inv;
-        g = fma(-rw.u, g, rw.r) * inv;
-        uc = ub;
-        ub = ua;
-        vb = va;
-    }
+}
+
+// Back substitution of window w (rows o0..o1; x_i = M at mirror knot i+1) and
+// its interval records: interval i+1 for every owned row i (knots i+1, i+2),
+// and interval 0 (M_0 = 0 at the natural end) for the first window.
+template <typename T>
+__device__ __forceinline__ void window_fast_back(const int* skt, const T* sky, const double* ssl, int base, int n,
+                                                 int w, int S, const double2* cd, int cdbase, const Rec<T>& R) {
+    constexpr bool kExact = false;
+    const int o0 = w * FAST_B;
+    const int o1 = min(n, o0 + FAST_B) - 1;
+    const int rh = min(n - 1, o1 + S);
     // monomial record of interval k (knots k, k+1; M_k = Ma, M_{k+1} = Mb):
     // y_k + s(c1 + s(c2 + s c3)), s = t - t_k, c1 = slope - h(2Ma + Mb)/6,
     // c2 = Ma/2, c3 = (Mb - Ma)/(6h)
@@ -536,40 +558,14 @@ __device__ void window_fast(const Ctx& C, const int* skt, const T* sky, const do
         R.at(k, 3) = (T)(0.5 * Ma);
         R.at(k, 4) = (T)((Mb - Ma) * fast_rcp(h) * (1.0 / 6.0));
     };
-    double xnext = 0.0;  // x_{i+1} of the previous iteration
-#pragma unroll
-    for (int k = FAST_B - 1; k >= 0; --k) {
-        if (k < cnt) {
-            const int i = o0 + k;
-            const int ua = SKT(i - base);
-            const double va = SSL(i - base);
-            const Row rw = row_of(ua, ub, uc, va, vb, i, n);
-            const double num = fma(-rw.u, g, fma(-rw.l, fd[k], rw.r));
-            const double den = fma(-rw.u, e, fma(-rw.l, fc[k], rw.dg));
-            const double xi = num * fast_rcp(den);  // M at mirror knot i+1
-            if (i < o1) put(i + 1, xi, xnext);
-            else if (i == n - 1) put(n, xi, 0.0);   // last interval ends at the M = 0 knot
-            xnext = xi;
-            const double inv = fast_rcp(fma(-rw.u, e, rw.dg));
-            e = rw.l * inv;
-            g = fma(-rw.u, g, rw.r) * inv;
-            uc = ub;
-            ub = ua;
-            vb = va;
-        }
+    double xn = 0.0;  // x_{i+1}: zero past the natural end (M = 0) or at the truncation
+    for (int i = rh; i >= o0; --i) {
+        const double2 c = cd[i - cdbase];
+        const double xi = fma(-c.x, xn, c.y);
+        if (i <= o1) put(i + 1, xi, xn);
+        xn = xi;
     }
-    // M at knot o0 (x_{o0-1}) closes interval o0; zero at the natural end
-    double xm = 0.0;
-    if (o0 >= 1) {
-        const int i = o0 - 1;
-        const int ua = SKT(i - base);
-        const double va = SSL(i - base);
-        const Row rw = row_of(ua, ub, uc, va, vb, i, n);
-        const double num = fma(-rw.u, g, fma(-rw.l, dq, rw.r));
-        const double den = fma(-rw.u, e, fma(-rw.l, cq, rw.dg));
-        xm = num * fast_rcp(den);
-    }
-    put(o0, xm, xnext);
+    if (o0 == 0) put(0, 0.0, xn);
 }
 
 #undef SKT
@@ -622,19 +618,39 @@ __device__ void solve_task(const Ctx& C, const Slot& sl, TaskSm& S, unsigned cha
     const int ca = (int)((int64_t)S.rank * nwt / S.csize), cb = (int)((int64_t)(S.rank + 1) * nwt / S.csize);
     const int wa = ca + (int)((int64_t)wid * (cb - ca) / NWARP);
     const int wb = ca + (int)((int64_t)(wid + 1) * (cb - ca) / NWARP);
-    const int per = min(32, (WSCAP - 2 * C.S - 8) / Bw);  // windows per pass
     unsigned char* ws = smem + (size_t)wid * wsolve_bytes(sizeof(T));
     double* ssl = reinterpret_cast<double*>(ws);
     int* skt = reinterpret_cast<int*>(ws + align16(stage_pad(WSCAP) * 8));
     T* sky = reinterpret_cast<T*>(ws + align16(stage_pad(WSCAP) * 8) + align16(stage_pad(WSCAP) * 4));
+    double2* cd = reinterpret_cast<double2*>(ws + align16(stage_pad(WSCAP) * 8) + align16(stage_pad(WSCAP) * 4) +
+                                             align16(stage_pad(WSCAP) * sizeof(T)));
+    // exact: windows of B rows with halos on both sides, one per lane;
+    // fast: lanes of FAST_B rows, the last H lanes of a pass as right halo
+    const int H = (C.S + FAST_B - 1) / FAST_B;
+    const int nlmax = min(32, (WSCAP - C.S - 3) / FAST_B);
+    const int per = min(32, (WSCAP - 2 * C.S - 8) / Bw);  // exact windows per pass
     for (int g = wa; g < wb;) {
         const int env = (g < nw0) ? 0 : 1;
         const int w0 = env ? g - nw0 : g;  // first window of the pass (within its envelope)
-        const int wend = min(w0 + per, min(env ? nw1 : nw0, w0 + (wb - g)));  // one past the last
+        const int nwe = env ? nw1 : nw0;
         const int n = env ? n1 : n0;
         const int p2 = S.p2[env];
-        const int rlo = max(0, w0 * Bw - C.S);
-        const int rhi = min(n - 1, min(n, wend * Bw) - 1 + C.S);
+        int ncommit, nl, rlo, rhi;
+        if (EXACT) {
+            ncommit = nl = min(w0 + per, min(nwe, w0 + (wb - g))) - w0;
+            rlo = max(0, w0 * Bw - C.S);
+            rhi = min(n - 1, min(n, (w0 + nl) * Bw) - 1 + C.S);
+        } else {
+            const int rem = min(wb - g, nwe - w0);  // this warp's windows left in the envelope
+            if (w0 + rem == nwe && rem <= nlmax) {
+                ncommit = nl = rem;  // the pass reaches the envelope's last row
+            } else {
+                ncommit = min(rem, nlmax - H);
+                nl = min(nlmax, min(ncommit + H, nwe - w0));
+            }
+            rlo = max(0, w0 * FAST_B - C.S);
+            rhi = min(n - 1, (w0 + nl) * FAST_B - 1);
+        }
         const int kcount = rhi + 3 - rlo;  // knots rlo .. rhi+2
         stage_range<T, EXACT>(C, sl, S, env, rlo, kcount, skt, sky, lane);
         cp_async_commit();
@@ -652,13 +668,16 @@ __device__ void solve_task(const Ctx& C, const Slot& sl, TaskSm& S, unsigned cha
         Rec<T> R;
         R.rc = static_cast<T*>(sl.M) + (int64_t)env * C.kcap * Geo<T>::RS;
         const int w = w0 + lane;
-        if (w < wend) {
-            if (EXACT) window_exact<T>(C, skt, sky, ssl, rlo, n, w, R, p2);
-            else window_fast<T>(C, skt, sky, ssl, rlo, n, w, R, p2);
+        if (EXACT) {
+            if (lane < nl) window_exact<T>(C, skt, sky, ssl, rlo, n, w, R, p2);
+        } else {
+            if (lane < nl) window_fast_fwd<T>(skt, ssl, rlo, n, w, C.S, cd, w0 * FAST_B);
+            __syncwarp();
+            if (lane < ncommit) window_fast_back<T>(skt, sky, ssl, rlo, n, w, C.S, cd, w0 * FAST_B, R);
         }
         __syncwarp();
         SUB(2);
-        g += wend - w0;
+        g += ncommit;
     }
     __syncthreads();
 #ifdef EEMD_TRACE
@@ -755,6 +774,15 @@ __device__ __forceinline__ void load_iv(Iv<T>& v, const T* R, int k) {
             v.m1 = e.x;
         }
     }
+}
+
+// interval record k from the tile's staged copy (records kf .. kf+cnt-1) when
+// it holds k, else from global memory
+template <typename T, bool EXACT>
+__device__ __forceinline__ void load_iv_st(Iv<T>& v, const T* R, const T* st, int kf, int cnt, int k) {
+    if ((unsigned)(k - kf) < (unsigned)cnt) load_iv<T, EXACT>(v, st, k - kf);
+    else load_iv<T, EXACT>(v, R, k);
+    v.k = k;
 }
 
 template <typename T, bool EXACT>
@@ -981,6 +1009,11 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
     // the tile's new knots, compacted in time order before one coalesced copy out
     int* const kts = reinterpret_cast<int*>(wb + G::TB_BYTES + G::RI_BYTES);  // [kind][KCAP]
     T* const kvs = reinterpret_cast<T*>(wb + G::TB_BYTES + G::RI_BYTES + 2 * G::KCAP * 4);
+    // staged interval records of the current tile: [env][CAPR][RS]
+    T* const rst = reinterpret_cast<T*>(wb + G::TB_BYTES + G::RI_BYTES + G::KN_BYTES);
+    constexpr bool STAGE = STAGE_RECS && !EXACT && SIFTING;
+    int kfc[2] = {0, 0}, kcc[2] = {0, 0};  // first staged record and count, current tile
+    int kfn[2] = {0, 0}, kcn[2] = {0, 0};  // the same for the next tile
     double num = 0.0, den = 0.0;
 #ifdef EEMD_TRACE
     unsigned long long scyc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -1006,11 +1039,42 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
         cp_async_commit();
     };
 
+    // Stage the records tile j's runs read (run records in buffer b): per
+    // envelope the contiguous range from the first run's current interval to
+    // the last run's last knot, at most CAPR records (16-byte copies).
+    auto stage_recs = [&](int j, int b) {
+        const int t0 = s0 + j * WT, tl = min(s1, t0 + WT) - t0;
+        const int4 rf = rib[b * 32];
+        const int4 rl = rib[b * 32 + (tl - 1) / RUN];
+#pragma unroll
+        for (int env = 0; env < 2; ++env) {
+            const int mir = S.mir[env];
+            const int kb = env ? kbase1 : kbase0;
+            const int first = max(0, kb + (env ? rf.y : rf.x) + mir - 1);
+            const unsigned ml = env ? ((unsigned)rl.z >> 16) : ((unsigned)rl.z & 0xffffu);
+            const int last = min(S.p2[env] - 2, kb + (env ? rl.y : rl.x) + __popc(ml) + mir - 1);
+            const int cnt = S.P[env] < 2 ? 0 : max(0, min(G::CAPR, last - first + 1));
+            kfn[env] = first;
+            kcn[env] = cnt;
+            constexpr int CH = RS * (int)sizeof(T) / 16;  // 16-byte chunks per record
+            constexpr int EL = 16 / (int)sizeof(T);       // elements per chunk
+            const T* src = (env ? R1 : R0) + (int64_t)first * RS;
+            T* dst = rst + env * G::CAPR * RS;
+            for (int c = lane; c < cnt * CH; c += 32) cp_async16(dst + c * EL, src + c * EL);
+        }
+    };
+
     int wcx = 0, wcy = 0;  // knots of each kind written to the warp's lists so far
     T gm1 = (T)0, gm2 = (T)0;  // next-knot values at t0-1 and t0-2 of the current tile
     int cpx = 0, cpn = 0, cmask = 0, crun = 0, cbit = 0;  // run record awaiting its last sample
     if (ta < tb) {
         prefetch(ta, 0);
+        if (STAGE) {
+            cp_async_wait<0>();
+            __syncwarp();
+            stage_recs(ta, 0);
+            cp_async_commit();
+        }
         if (r0 > 0) {
             // the sample before the range: its value is the left neighbour of the range's first sample
             int c0 = 0, c1 = 0;
@@ -1032,6 +1096,12 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
         const int last_lane = (tl - 1) / RUN;
         cp_async_wait<0>();
         __syncwarp();
+        if (STAGE) {
+            kfc[0] = kfn[0];
+            kfc[1] = kfn[1];
+            kcc[0] = kcn[0];
+            kcc[1] = kcn[1];
+        }
         if (j + 1 < tb) prefetch(j + 1, b ^ 1);
         SUB(0);
         const T* hb = tbuf + (b * 2) * G::TB;
@@ -1094,22 +1164,38 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
                 n0 = c1 = n1 = c0;
                 int k0 = kb0 + S.mir[0] - 1, k1 = kb1 + S.mir[1] - 1;
                 if (nv > 0) {
-                    load_iv<T, EXACT>(c0, R0, k0);
-                    load_iv<T, EXACT>(c1, R1, k1);
-                    if (kmx) load_iv<T, EXACT>(n0, R0, k0 + 1);
-                    if (kmn) load_iv<T, EXACT>(n1, R1, k1 + 1);
+                    // the interior test above keeps every index of the run in [0, p2 - 2]
+                    EEMD_CHECK_IV(k0, S.p2[0] - 2 - (int)__popc(kmx));
+                    EEMD_CHECK_IV(k1, S.p2[1] - 2 - (int)__popc(kmn));
+                    if (STAGE) {
+                        load_iv_st<T, EXACT>(c0, R0, rst, kfc[0], kcc[0], k0);
+                        load_iv_st<T, EXACT>(c1, R1, rst + G::CAPR * RS, kfc[1], kcc[1], k1);
+                        if (kmx) load_iv_st<T, EXACT>(n0, R0, rst, kfc[0], kcc[0], k0 + 1);
+                        if (kmn) load_iv_st<T, EXACT>(n1, R1, rst + G::CAPR * RS, kfc[1], kcc[1], k1 + 1);
+                    } else {
+                        load_iv<T, EXACT>(c0, R0, k0);
+                        load_iv<T, EXACT>(c1, R1, k1);
+                        if (kmx) load_iv<T, EXACT>(n0, R0, k0 + 1);
+                        if (kmn) load_iv<T, EXACT>(n1, R1, k1 + 1);
+                    }
                 }
 #pragma unroll
                 for (int i = 0; i < RUN; ++i) {
                     if (i > 0 && ((kmx >> (i - 1)) & 1u)) {
                         c0 = n0;
                         ++k0;
-                        if (kmx >> i) load_iv<T, EXACT>(n0, R0, k0 + 1);
+                        if (kmx >> i) {
+                            if (STAGE) load_iv_st<T, EXACT>(n0, R0, rst, kfc[0], kcc[0], k0 + 1);
+                            else load_iv<T, EXACT>(n0, R0, k0 + 1);
+                        }
                     }
                     if (i > 0 && ((kmn >> (i - 1)) & 1u)) {
                         c1 = n1;
                         ++k1;
-                        if (kmn >> i) load_iv<T, EXACT>(n1, R1, k1 + 1);
+                        if (kmn >> i) {
+                            if (STAGE) load_iv_st<T, EXACT>(n1, R1, rst + G::CAPR * RS, kfc[1], kcc[1], k1 + 1);
+                            else load_iv<T, EXACT>(n1, R1, k1 + 1);
+                        }
                     }
                     const int t = t0 + j0 + i;
                     if (i < nv) finish(i, (T)0.5 * (iv_eval<T, EXACT>(c0, t) + iv_eval<T, EXACT>(c1, t)));
@@ -1138,6 +1224,15 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
 #pragma unroll
             for (int i = 0; i < RUN; ++i)
                 if (i < nv) plain_value<T, MODE>(C, S, d, t0 + j0 + i, hv[i], rv[i], fv[i], gv[i]);
+        }
+        if (STAGE && j + 1 < tb) {
+            // this tile's records are consumed: stage the next tile's while
+            // this tile's extrema and writes run (its run records came with
+            // the prefetch issued at the top of this tile)
+            cp_async_wait<0>();
+            __syncwarp();
+            stage_recs(j + 1, b ^ 1);
+            cp_async_commit();
         }
         SUB(1);
 
@@ -1226,7 +1321,7 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
         {
             const int nx = tot & 0xffff, nn = tot >> 16;
             if (wcx + nx > C.segcap || wcy + nn > C.segcap || nx > G::KCAP || nn > G::KCAP) {
-                if (lane == 0) raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
+                if (lane == 0) task_error(C, S, EEMD_E_KNOT_OVERFLOW);
             } else {
                 T* const ky = static_cast<T*>(sl.ky);
                 for (int k = lane; k < nx; k += 32) {
@@ -1281,7 +1376,7 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
                     sl.kt[pmx + wcx] = r1 - 1;
                     static_cast<T*>(sl.ky)[pmx + wcx] = gm1;
                 } else {
-                    raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
+                    task_error(C, S, EEMD_E_KNOT_OVERFLOW);
                 }
             }
             if (dmn) {
@@ -1289,7 +1384,7 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
                     sl.kt[pmn + wcy] = r1 - 1;
                     static_cast<T*>(sl.ky)[pmn + wcy] = gm1;
                 } else {
-                    raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
+                    task_error(C, S, EEMD_E_KNOT_OVERFLOW);
                 }
             }
             ri_nxt[crun] = make_int4(cpx, cpn, cmask | (int)(dmx << cbit) | (int)(dmn << (16 + cbit)), 0);
@@ -1312,6 +1407,7 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
     if (tid == 0) {
         X[q].num = rs.x;
         X[q].den = rs.y;
+        X[q].err = S.err;
     }
 }
 
@@ -1396,14 +1492,20 @@ __device__ void decide(const Ctx& C, TaskSm& S, Xchg* X, cg::cluster_group& cl) 
         }
         if (lane == 0) {
             double num = 0.0, den = 0.0;
+            int err = 0;
             for (int r = 0; r < S.csize; ++r) {
                 const Xchg* xr = cl.map_shared_rank(&X[q], r);
                 num += xr->num;
                 den += xr->den;
+                err |= xr->err;
             }
             const int cmax = tot[0], cmin = tot[1];
             const int mode = S.mode;
-            if (mode == TM_SIFT) {
+            if (err) {
+                // an error of this task (recorded in the header): stop it here
+                S.phase = PH_DONE;
+                S.flags |= 2;
+            } else if (mode == TM_SIFT) {
                 log_sift(C, S);
                 S.mode_sifts_cur += 1;
                 S.nsift_total += 1;
@@ -1474,7 +1576,10 @@ __device__ void step_setup(const Ctx& C, const Slot& sl, TaskSm& S) {
                 S.ylast[env] = yb;
             }
         }
-        if (S.p2[env] > C.kcap) raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
+        if (S.p2[env] > C.kcap) {
+            raise_error(C.hdr, EEMD_E_KNOT_OVERFLOW, S.task);
+            S.setup_fail = 1;  // computed from the same counts in every CTA of the cluster
+        }
     }
     __syncthreads();
 }
@@ -1561,10 +1666,21 @@ __global__ void __launch_bounds__(THREADS, EEMD_MIN_CTAS_PER_SM) k_emd(const __g
                 if (S.phase == PH_INIT) S.mode = TM_INIT;
                 else if (S.phase == PH_TRANS) S.mode = TM_TRANS;
                 else S.mode = (S.sift + 1 >= C.max_sifts) ? TM_LAST : TM_SIFT;
+                S.err = 0;
+                S.setup_fail = 0;
             }
             __syncthreads();
             if (S.mode == TM_SIFT || S.mode == TM_LAST) {
                 step_setup<T>(C, sl, S);
+                if (S.setup_fail) {
+                    // every CTA of the cluster sees the same counts and leaves together
+                    if (tid == 0) {
+                        S.phase = PH_DONE;
+                        S.flags |= 2;
+                    }
+                    __syncthreads();
+                    break;
+                }
                 EEMD_PHASE(0);
                 solve_task<T, EXACT>(C, sl, S, smem_raw);
                 EEMD_PHASE(1);
@@ -1802,8 +1918,12 @@ int make_layout(const eemd_params* p, const int64_t* lengths, int n_signals, int
     // (2 - sqrt 3)^S; 16 rows put it far below float32 rounding
     L.S = p->halo ? p->halo : (p->exact ? 32 : (p->dtype == EEMD_F32 ? 16 : 24));
     L.B = p->knots_per_block ? p->knots_per_block : 16;
-    // a solve pass stages its windows' knots plus both halos in the warp's area
-    if (2 * L.S + L.B + 8 > WSCAP || 2 * L.S + FAST_B + 8 > WSCAP) return EEMD_E_BADARG;
+    // a solve pass stages its windows' knots plus the halos in the warp's area:
+    // exact windows carry both halos; a fast pass needs room for at least one
+    // committing lane besides its ceil(S / FAST_B) right-halo lanes
+    if (p->exact && 2 * L.S + L.B + 8 > WSCAP) return EEMD_E_BADARG;
+    if (!p->exact && (L.S + FAST_B - 1) / FAST_B + 1 > std::min(32, (WSCAP - L.S - 3) / FAST_B))
+        return EEMD_E_BADARG;
     int64_t segmax = 0;
     L.td.resize(n_tasks);
     L.sd.resize(n_signals);
@@ -1845,6 +1965,11 @@ int make_layout(const eemd_params* p, const int64_t* lengths, int n_signals, int
     // knots of one kind in one warp's range: at most half its samples (+ends)
     const int64_t tiles_per_warp = ((segmax + wt - 1) / wt + NWARP - 1) / NWARP;
     L.segcap = (int)(tiles_per_warp * wt / 2 + 2);
+#ifdef EEMD_CHECKED
+    // test hook of the checked build only: params.reserved > 0 shrinks the knot
+    // lists' capacity so that the overflow path can be exercised
+    if (p->reserved > 0 && p->reserved < L.segcap) L.segcap = p->reserved;
+#endif
     L.kcap = (int)(nmax / 2 + 4);
     const int rs = (p->dtype == EEMD_F64) ? Geo<double>::RS : Geo<float>::RS;
     L.slot_n = (nmax + 3) / 4 * 4;

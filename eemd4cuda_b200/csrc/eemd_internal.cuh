@@ -35,19 +35,27 @@ namespace eemd {
 #define EEMD_CTA_WARPS 4
 #endif
 constexpr int THREADS = 32 * EEMD_CTA_WARPS;  // threads per CTA of k_emd
-constexpr int CTAS_PER_SM = 16 / EEMD_CTA_WARPS;  // 16 warps of 128 registers fill an SM
+// resident CTAs per SM the kernel is compiled (launch bounds) and the grid sized for
+#ifndef EEMD_CTAS_PER_SM
+#define EEMD_CTAS_PER_SM (16 / EEMD_CTA_WARPS)  // 16 warps of 128 registers fill an SM
+#endif
+constexpr int CTAS_PER_SM = EEMD_CTAS_PER_SM;
 // largest cluster: portable clusters reach 8 CTAs; 9 to 16 are non-portable
 // and are taken only when the device reports that all of them fit at once
 constexpr int MAXC = 16;
-// owned rows per window of the fast solve (its forward state is register
-// resident): 3 measured fastest (config 2 6.66 ms, 2^22 x 64 trials 143.9 ms,
-// 1024 tasks of 65536 samples 83.5 ms; 8: 7.17 / 147.2 / 92.4; 2, 4, 5, 6,
-// 12 and 16 in between or slower) -- fewer registers outweigh the extra halo
-// rows per owned knot
+// owned rows per lane of the fast solve: the forward (c, d) of a pass's rows
+// live in shared memory, so the width costs no registers; odd widths keep the
+// lanes' strided shared-memory accesses free of bank conflicts
 #ifndef EEMD_FAST_B
-#define EEMD_FAST_B 3
+#define EEMD_FAST_B 9
 #endif
 constexpr int FAST_B = EEMD_FAST_B;
+// fast mode: stage the interval records of the sweep's next warp tile in
+// shared memory (1) or read them from global memory as each run needs them (0)
+#ifndef EEMD_STAGE_RECS
+#define EEMD_STAGE_RECS 1
+#endif
+constexpr bool STAGE_RECS = EEMD_STAGE_RECS != 0;
 #ifndef EEMD_WSCAP
 #define EEMD_WSCAP 352
 #endif

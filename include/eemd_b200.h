@@ -100,7 +100,11 @@ typedef struct eemd_params {
                                  and the run returns EEMD_E_TIMEOUT */
     int32_t  cluster_size;    /* CTAs (thread-block cluster) per task, 1..16 (0 = autotune; 9..16 are
                                  non-portable cluster sizes the device must support) */
-    int32_t  reserved;
+    int32_t  reserved;        /* 0.  Test hook honoured only by the bounds-checked build
+                                 (libeemd_b200_checked.so): a value k > 0 caps the knot
+                                 lists at k knots of one kind per warp segment, so that
+                                 the EEMD_E_KNOT_OVERFLOW path can be exercised; the
+                                 release build ignores it */
 } eemd_params;
 
 /* Fill p with the defaults of emd_par.decompose (emd_par.py:260-262):

@@ -298,3 +298,35 @@ def test_workspace_too_small_is_reported():
     with pytest.raises(L.EngineError) as ei:
         L.run(p, x, [1000], 0, 1, ws)
     assert ei.value.status == L.EEMD_E_NOMEM
+
+
+def test_knot_capacity_overflow_is_reported_and_context_survives():
+    """The survey's forced knot-capacity overflow: the bounds-checked build
+    honours params.reserved as a cap on the knot lists (knots of one kind per
+    warp segment).  A cap far below what a 48 000-sample signal needs returns
+    EEMD_E_KNOT_OVERFLOW as a status (the task stops at the step that
+    overflowed; nothing is written past the cap), and the next call on the
+    same context -- with the cap lifted -- succeeds and equals the release
+    build.  (The reference's own bound is K = max(16, N // 2), emd_gpu.py:297-298.)"""
+    chk = L.load_variant(L.LIB_DIR / "libeemd_b200_checked.so")
+    dev = torch.device("cuda")
+    x = signals.harmonic_clicks(48000, seed=1)
+    N = len(x)
+    xd = torch.from_numpy(x).to(dev)
+    for cap in (16, 64):
+        p = M.make_params(tau=0.0, max_sifts=10, max_imf=8)
+        p.reserved = cap
+        ws = torch.empty((L.workspace_size(p, [N], 1, False),), dtype=torch.uint8, device=dev)
+        with pytest.raises(L.EngineError) as ei:
+            L.run(p, xd, [N], 0, 1, ws, lib=chk)
+        assert ei.value.status == L.EEMD_E_KNOT_OVERFLOW
+    p = M.make_params(tau=0.0, max_sifts=10, max_imf=8)
+    outs = []
+    for lib in (chk, None):
+        ws = torch.empty((L.workspace_size(p, [N], 1, False),), dtype=torch.uint8, device=dev)
+        imfs = torch.zeros((8 * N,), dtype=torch.float64, device=dev)
+        nmode = torch.zeros((1,), dtype=torch.int32, device=dev)
+        L.run(p, xd, [N], 0, 1, ws, imfs=imfs, nmode=nmode, lib=lib)
+        outs.append((imfs.cpu().numpy(), int(nmode.item())))
+    assert outs[0][1] == outs[1][1] == 8
+    assert np.array_equal(outs[0][0], outs[1][0])

@@ -87,7 +87,8 @@ def test_workspace_size_scales():
 @pytest.mark.parametrize("field,value", [("dtype", 7), ("max_sifts", 0), ("max_imf", 0),
                                          ("end_mode", 5), ("rules", 9), ("tile", 300),
                                          ("noise_mode", 11), ("tile", 2048),
-                                         ("cluster_size", 17), ("knots_per_block", 1024)])
+                                         ("cluster_size", 17), ("knots_per_block", 8192),
+                                         ("halo", 300)])
 def test_bad_params_rejected(field, value):
     p = L.default_params()
     setattr(p, field, value)
