@@ -370,22 +370,40 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
+# DRAM traffic of one k_emd launch: ncu dram__bytes_read.sum +
+# dram__bytes_write.sum from a capture of the same workload (a capture cannot
+# run inside the timed bench).  `engine_sha256` is the hash of the engine
+# source the capture ran; the bench reports whether the current source is the
+# same (`traffic_matches_build`), so a change of the kernel since the capture
+# shows.  Workloads too large to capture whole were captured on fewer trials
+# of the same signal and are scaled per (signal, trial) task, since every task
+# streams its own buffers.
+EMD_TRAFFIC = {
+    "harmonic48k": {"bytes_per_launch": 6730622000, "engine_sha256": None,
+                    "capture": "one k_emd launch of the 100-trial 48 kHz workload"},
+    "amfm4m": {"bytes_per_task": 5606744640.0, "engine_sha256": None,
+               "capture": "one k_emd launch of 4 trials of the 2^22-sample signal, per task"},
+}
+
+
+def engine_source_sha256() -> str:
+    import hashlib
+    src = ROOT / "eemd4cuda_b200" / "csrc" / "eemd_engine.cu"
+    return hashlib.sha256(src.read_bytes()).hexdigest()
+
+
 def measured_traffic(workload: str, tasks_per_launch: int):
-    """DRAM bytes (read + write) of one k_emd launch from an ncu capture
-    summarised in profiles/emd_traffic.json: the launch itself, or a smaller
-    launch of the same workload scaled by its (signal, trial) tasks when the
-    full launch is too large to capture (traffic grows with the tasks, since
-    every task streams its own buffers).  None when there is no capture."""
-    tf = ROOT / "profiles" / "emd_traffic.json"
-    try:
-        ent = json.loads(tf.read_text()).get(workload) or {}
-    except (OSError, ValueError):
-        return None
-    if "bytes_per_launch" in ent:
-        return int(ent["bytes_per_launch"])
-    if "bytes_per_task" in ent:
-        return int(round(ent["bytes_per_task"] * tasks_per_launch))
-    return None
+    """(DRAM bytes of one k_emd launch, description) from EMD_TRAFFIC, or
+    (None, None) when the workload has no capture."""
+    ent = EMD_TRAFFIC.get(workload)
+    if not ent:
+        return None, None
+    b = ent.get("bytes_per_launch")
+    if b is None:
+        b = ent["bytes_per_task"] * tasks_per_launch
+    src = {"capture": ent["capture"], "engine_sha256": ent["engine_sha256"],
+           "traffic_matches_build": ent["engine_sha256"] == engine_source_sha256()}
+    return int(round(b)), src
 
 
 def emd_algorithmic_bytes(klog: np.ndarray, nmode: np.ndarray, lengths, trials: int,
@@ -613,7 +631,7 @@ def run_ours(args, wl: Workload):
     emd_gbs = emd_bytes / (ev["ms"] / 1e3) / 1e9 if ev["ms"] > 0 else 0.0
     gpu_sifts_per_task = float(nsift.float().mean().item())
     peak, peak_kind = measured_peak_hbm()
-    traffic = measured_traffic(wl.name, n_first)
+    traffic, traffic_src = measured_traffic(wl.name, n_first)
 
     # ---- end to end through the public API (host buffers) ----
     if wl.name in ("harmonic48k", "plain8k"):
@@ -774,8 +792,8 @@ def run_ours(args, wl: Workload):
         "roofline": {"bound": "hbm", "kernel": "k_emd", "achieved": round(emd_gbs, 2),
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": round(emd_gbs / peak, 4),
-                     "traffic": traffic, "algorithmic_bytes_per_launch":
-                         round(emd_bytes / max(ev["launches"], 1)),
+                     "traffic": traffic, "traffic_source": traffic_src,
+                     "algorithmic_bytes_per_launch": round(emd_bytes / max(ev["launches"], 1)),
                      "avg_launch_ms": round(ev["ms"] / max(ev["launches"], 1), 5)},
         "kernel_split_ms": {k: round(v["ms"], 4) for k, v in kt.items()},
         "kernel_launches": {k: v["launches"] for k, v in kt.items()},

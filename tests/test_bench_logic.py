@@ -27,9 +27,12 @@ def test_algorithmic_bytes_by_hand():
 
 
 def test_measured_traffic_per_workload():
-    full = bench.measured_traffic("harmonic48k", 100)
+    full, src = bench.measured_traffic("harmonic48k", 100)
     assert isinstance(full, int) and full > 0
-    assert bench.measured_traffic("harmonic48k", 7) == full  # a launch capture is not rescaled
-    a64, a32 = bench.measured_traffic("amfm4m", 64), bench.measured_traffic("amfm4m", 32)
+    assert set(src) == {"capture", "engine_sha256", "traffic_matches_build"}
+    assert bench.measured_traffic("harmonic48k", 7)[0] == full  # a launch capture is not rescaled
+    a64, a32 = bench.measured_traffic("amfm4m", 64)[0], bench.measured_traffic("amfm4m", 32)[0]
     assert a64 > 0 and abs(a64 - 2 * a32) <= 1
-    assert bench.measured_traffic("plain8k", 1) is None
+    assert bench.measured_traffic("plain8k", 1) == (None, None)
+    # the flag follows the engine source the capture ran
+    assert len(bench.engine_source_sha256()) == 64
