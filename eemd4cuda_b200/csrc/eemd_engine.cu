@@ -294,18 +294,28 @@ __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t
 
 // rows of one fast-solve pass: 32 lanes of FAST_B rows
 constexpr int FAST_ROWS = 32 * FAST_B;
+// largest seam halo of the fast solve, and the knots one fast pass stages:
+// its rows, the left halo and the two knots past the last row
+constexpr int FAST_SMAX = 64;
+constexpr int WSCAP_FAST = FAST_ROWS + FAST_SMAX + 3;
 
-// per-warp solve staging: slopes (double), knot times (int), knot values
-// (storage type), and the fast solve's forward (c, d) of a pass's rows
-__host__ __device__ inline size_t wsolve_bytes(size_t bt) {
-    const size_t sp = (size_t)stage_pad(WSCAP);
-    return align16(sp * 8) + align16(sp * 4) + align16(sp * bt) + (size_t)FAST_ROWS * 16;
+// knots a solve pass stages per warp: exact windows carry both halos (up to
+// WSCAP knots); the fast solve's lanes need WSCAP_FAST
+__host__ __device__ constexpr int stage_cap(bool exact) { return exact ? WSCAP : WSCAP_FAST; }
+
+// per-warp solve area: slopes (double), knot times (int), knot values
+// (storage type), and in fast mode the forward (c, d) of a pass's rows.  It
+// overlays the sweep's area; keeping it no larger leaves the L1 share of the
+// SM's on-chip memory (used by the sweep's record loads) unchanged.
+__host__ __device__ inline size_t wsolve_bytes(size_t bt, bool exact) {
+    const size_t sp = (size_t)stage_pad(stage_cap(exact));
+    return align16(sp * 8) + align16(sp * 4) + align16(sp * bt) + (exact ? 0 : (size_t)FAST_ROWS * 16);
 }
 
 // dynamic shared memory of k_emd: the sweep's and the solve's per-warp areas overlay
-__host__ __device__ inline size_t smem_bytes(int bt) {
+__host__ __device__ inline size_t smem_bytes(int bt, bool exact) {
     const size_t sweep = NWARP * (bt == 8 ? Geo<double>::WARP_BYTES : Geo<float>::WARP_BYTES);
-    const size_t solve = NWARP * wsolve_bytes((size_t)bt);
+    const size_t solve = NWARP * wsolve_bytes((size_t)bt, exact);
     return sweep > solve ? sweep : solve;
 }
 
@@ -618,16 +628,17 @@ __device__ void solve_task(const Ctx& C, const Slot& sl, TaskSm& S, unsigned cha
     const int ca = (int)((int64_t)S.rank * nwt / S.csize), cb = (int)((int64_t)(S.rank + 1) * nwt / S.csize);
     const int wa = ca + (int)((int64_t)wid * (cb - ca) / NWARP);
     const int wb = ca + (int)((int64_t)(wid + 1) * (cb - ca) / NWARP);
-    unsigned char* ws = smem + (size_t)wid * wsolve_bytes(sizeof(T));
+    constexpr int CAP = stage_cap(EXACT);
+    unsigned char* ws = smem + (size_t)wid * wsolve_bytes(sizeof(T), EXACT);
     double* ssl = reinterpret_cast<double*>(ws);
-    int* skt = reinterpret_cast<int*>(ws + align16(stage_pad(WSCAP) * 8));
-    T* sky = reinterpret_cast<T*>(ws + align16(stage_pad(WSCAP) * 8) + align16(stage_pad(WSCAP) * 4));
-    double2* cd = reinterpret_cast<double2*>(ws + align16(stage_pad(WSCAP) * 8) + align16(stage_pad(WSCAP) * 4) +
-                                             align16(stage_pad(WSCAP) * sizeof(T)));
+    int* skt = reinterpret_cast<int*>(ws + align16(stage_pad(CAP) * 8));
+    T* sky = reinterpret_cast<T*>(ws + align16(stage_pad(CAP) * 8) + align16(stage_pad(CAP) * 4));
+    double2* cd = reinterpret_cast<double2*>(ws + align16(stage_pad(CAP) * 8) + align16(stage_pad(CAP) * 4) +
+                                             align16(stage_pad(CAP) * sizeof(T)));
     // exact: windows of B rows with halos on both sides, one per lane;
     // fast: lanes of FAST_B rows, the last H lanes of a pass as right halo
     const int H = (C.S + FAST_B - 1) / FAST_B;
-    const int nlmax = min(32, (WSCAP - C.S - 3) / FAST_B);
+    const int nlmax = min(32, (WSCAP_FAST - C.S - 3) / FAST_B);
     const int per = min(32, (WSCAP - 2 * C.S - 8) / Bw);  // exact windows per pass
     for (int g = wa; g < wb;) {
         const int env = (g < nw0) ? 0 : 1;
@@ -1826,7 +1837,7 @@ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 int active_clusters(int dtype, bool exact, int c) {
     const void* fn = (dtype == EEMD_F32) ? (const void*)k_emd<float, false>
                                          : (exact ? (const void*)k_emd<double, true> : (const void*)k_emd<double, false>);
-    const size_t smem = smem_bytes(dtype == EEMD_F32 ? 4 : 8);
+    const size_t smem = smem_bytes(dtype == EEMD_F32 ? 4 : 8, exact);
     int n = 0;
     bool ok = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess;
     if (ok && c > 8) ok = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess;
@@ -1922,7 +1933,7 @@ int make_layout(const eemd_params* p, const int64_t* lengths, int n_signals, int
     // exact windows carry both halos; a fast pass needs room for at least one
     // committing lane besides its ceil(S / FAST_B) right-halo lanes
     if (p->exact && 2 * L.S + L.B + 8 > WSCAP) return EEMD_E_BADARG;
-    if (!p->exact && (L.S + FAST_B - 1) / FAST_B + 1 > std::min(32, (WSCAP - L.S - 3) / FAST_B))
+    if (!p->exact && (L.S > FAST_SMAX || (L.S + FAST_B - 1) / FAST_B + 1 > std::min(32, (WSCAP_FAST - L.S - 3) / FAST_B)))
         return EEMD_E_BADARG;
     int64_t segmax = 0;
     L.td.resize(n_tasks);
@@ -2048,7 +2059,7 @@ struct Tracer {
 
 template <typename T, bool EXACT>
 int launch_emd(const Ctx& C, const Layout& L, cudaStream_t st, Tracer& tr) {
-    const size_t smem = smem_bytes((int)sizeof(T));
+    const size_t smem = smem_bytes((int)sizeof(T), EXACT);
     if (cudaFuncSetAttribute(k_emd<T, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return EEMD_E_CUDA;

@@ -47,13 +47,13 @@ constexpr int MAXC = 16;
 // live in shared memory, so the width costs no registers; odd widths keep the
 // lanes' strided shared-memory accesses free of bank conflicts
 #ifndef EEMD_FAST_B
-#define EEMD_FAST_B 9
+#define EEMD_FAST_B 5
 #endif
 constexpr int FAST_B = EEMD_FAST_B;
 // fast mode: stage the interval records of the sweep's next warp tile in
 // shared memory (1) or read them from global memory as each run needs them (0)
 #ifndef EEMD_STAGE_RECS
-#define EEMD_STAGE_RECS 1
+#define EEMD_STAGE_RECS 0
 #endif
 constexpr bool STAGE_RECS = EEMD_STAGE_RECS != 0;
 #ifndef EEMD_WSCAP

@@ -92,7 +92,7 @@ typedef struct eemd_params {
     int32_t  knots_per_block; /* owned rows per exact-mode seam window (0 = 16; the fast
                                  solve owns 3 rows per window) */
     int32_t  halo;            /* seam halo rows on each side of a window (0 = 32 exact,
-                                 24 fast float64, 16 fast float32) */
+                                 24 fast float64, 16 fast float32; at most 64 in fast mode) */
     int64_t  watchdog;        /* >= 0: no effect (the engine has no device waits on its data
                                  path; every loop is bounded by the sift and IMF caps);
                                  a negative value -k is the watchdog test mode: every task
