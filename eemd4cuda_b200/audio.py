@@ -1,9 +1,11 @@
 """Audio decode, segmentation and a pipelined segment-by-segment EEMD.
 
 The reference decodes with soundfile (audio_eemd/audio_io.py:71-176), which
-is not installed in this image; this module reads RIFF/WAVE files itself
-(PCM 8/16/24/32-bit and IEEE float 32/64-bit, any channel count) into the
-same float64 [frames, channels] array soundfile returns (PCM scaled by
+is not installed in this image; this module reads FLAC streams through its
+own decoder (libeemd_flac.so, include/eemd_flac.h: RFC 9639, every frame's
+CRCs checked and the stream's MD5 signature compared) and RIFF/WAVE files
+itself (PCM 8/16/24/32-bit and IEEE float 32/64-bit, any channel count) into
+the same float64 [frames, channels] array soundfile returns (PCM scaled by
 2^-(bits-1), unsigned 8-bit centred first) and keeps the reference's
 segment rules: `AudioFile.to_mono` (mean over channels), `select_segment`
 (seconds or samples, stop exclusive, typed SegmentError codes) and
@@ -16,6 +18,8 @@ segment k-1 are copied back and written (results.AsyncWriter).
 """
 from __future__ import annotations
 
+import ctypes
+import hashlib
 import struct
 from dataclasses import dataclass, field
 from pathlib import Path
@@ -96,15 +100,91 @@ def _decode(fmt_tag, bits, data, channels):
     return v[:frames * channels].reshape(frames, channels), sub
 
 
+_FLAC = None
+
+
+class FlacInfo(ctypes.Structure):
+    """Mirror of `eemd_flac_stream_info` (include/eemd_flac.h)."""
+
+    _fields_ = [("sample_rate", ctypes.c_int32), ("channels", ctypes.c_int32),
+                ("bits_per_sample", ctypes.c_int32), ("min_block", ctypes.c_int32),
+                ("max_block", ctypes.c_int32), ("pad", ctypes.c_int32),
+                ("total_frames", ctypes.c_int64), ("first_frame_offset", ctypes.c_int64),
+                ("md5", ctypes.c_uint8 * 16)]
+
+
+def _flac_lib():
+    global _FLAC
+    if _FLAC is None:
+        path = Path(__file__).resolve().parent / "lib" / "libeemd_flac.so"
+        if not path.exists():
+            raise AudioError(f"FLAC decoder library not found at {path}; build it with "
+                             "`python -m eemd4cuda_b200.build`", "audio.unsupported")
+        lib = ctypes.CDLL(str(path))
+        lib.eemd_flac_info.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(FlacInfo)]
+        lib.eemd_flac_info.restype = ctypes.c_int32
+        lib.eemd_flac_decode.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_int64,
+                                         ctypes.POINTER(ctypes.c_int64)]
+        lib.eemd_flac_decode.restype = ctypes.c_int32
+        lib.eemd_flac_strerror.argtypes = [ctypes.c_int32]
+        lib.eemd_flac_strerror.restype = ctypes.c_char_p
+        _FLAC = lib
+    return _FLAC
+
+
+def decode_flac(raw: bytes):
+    """(int32 samples [frames, channels], FlacInfo) of a FLAC stream; AudioError
+    on a malformed stream, a CRC mismatch or an MD5 signature mismatch."""
+    lib = _flac_lib()
+    info = FlacInfo()
+    rc = lib.eemd_flac_info(raw, len(raw), ctypes.byref(info))
+    if rc:
+        raise AudioError(f"not a readable FLAC stream: {lib.eemd_flac_strerror(rc).decode()}")
+    total = int(info.total_frames)
+    if total == 0:
+        # length not recorded: every frame takes at least 8 bytes (header,
+        # one subframe header, CRC-16) and holds at most max_block samples
+        total = (len(raw) // 8 + 1) * int(info.max_block)
+    out = np.empty((total, int(info.channels)), dtype=np.int32)
+    got = ctypes.c_int64(0)
+    rc = lib.eemd_flac_decode(raw, len(raw), out.ctypes.data, total, ctypes.byref(got))
+    if rc:
+        raise AudioError(f"FLAC decode failed after {got.value} frames: {lib.eemd_flac_strerror(rc).decode()}")
+    x = out[:got.value]
+    md5 = bytes(info.md5)
+    if any(md5):
+        nb = (int(info.bits_per_sample) + 7) // 8
+        le = x.astype("<i4").view(np.uint8).reshape(-1, 4)[:, :nb]
+        if hashlib.md5(le.tobytes()).digest() != md5:
+            raise AudioError("FLAC stream's MD5 signature does not match its decoded samples")
+    return x, info
+
+
+def _load_flac(p: Path, raw: bytes) -> AudioFile:
+    x, info = decode_flac(raw)
+    bps = int(info.bits_per_sample)
+    if x.shape[0] == 0:
+        raise AudioError(f"unexpected sample array shape {x.shape} from {p}")
+    v = x.astype(np.float64) / float(1 << (bps - 1))
+    sr, ch, frames = int(info.sample_rate), int(info.channels), int(x.shape[0])
+    sub = {8: "PCM_S8", 16: "PCM_16", 24: "PCM_24"}.get(bps, f"PCM_{bps}")
+    meta = {"format": "FLAC", "subtype": sub, "samplerate": sr, "channels": ch, "frames": frames,
+            "duration_s": frames / float(sr)}
+    return AudioFile(path=p, sr=sr, channels=ch, frames=frames, duration=frames / float(sr), fmt="FLAC",
+                     subtype=sub, x=v, meta=meta)
+
+
 def load_audio(path) -> AudioFile:
-    """Read a RIFF/WAVE file fully into memory (AudioError on failure)."""
+    """Read a FLAC or RIFF/WAVE file fully into memory (AudioError on failure)."""
     p = Path(path)
     try:
         raw = p.read_bytes()
     except OSError as e:
         raise AudioError(f"cannot read audio file {p}: {e}") from e
+    if raw[:4] == b"fLaC":
+        return _load_flac(p, raw)
     if len(raw) < 12 or raw[:4] != b"RIFF" or raw[8:12] != b"WAVE":
-        raise AudioError(f"cannot read audio file {p}: not a RIFF/WAVE file")
+        raise AudioError(f"cannot read audio file {p}: not a FLAC or RIFF/WAVE file")
     pos, fmt, data = 12, None, None
     while pos + 8 <= len(raw):
         cid, size = raw[pos:pos + 4], struct.unpack("<I", raw[pos + 4:pos + 8])[0]

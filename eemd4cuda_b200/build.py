@@ -12,6 +12,7 @@ Outputs (git-ignored, shipped next to the sources):
         (eemd4cuda_b200.trace reads them)
     eemd4cuda_b200/lib/libeemd_surrogate.so     the learned surrogate's kernels
     eemd4cuda_b200/lib/libeemd_spectra.so       Hilbert IF / STFT of the IMFs (links cuFFT)
+    eemd4cuda_b200/lib/libeemd_flac.so          FLAC decoder (host C, gcc)
 """
 from __future__ import annotations
 
@@ -83,6 +84,18 @@ def build(force: bool = False, verbose: bool = False) -> list[Path]:
         cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
                "-I", str(INCLUDE), "-o", str(tmp), *[str(CSRC / s) for s in SP_SOURCES],
                "-L", libdir, "-lcufft", "-Xlinker", "-rpath", "-Xlinker", libdir]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+        os.replace(tmp, out)
+    # the FLAC decoder (host code)
+    out = LIB / "libeemd_flac.so"
+    outs.append(out)
+    fl_deps = [CSRC / "flac_decode.c", INCLUDE / "eemd_flac.h"]
+    if force or _stale(out, fl_deps):
+        tmp = out.with_suffix(".so.tmp")
+        cmd = [os.environ.get("CC", "gcc"), "-std=c99", "-O2", "-Wall", "-fPIC", "-shared", "-I", str(INCLUDE),
+               "-o", str(tmp), str(CSRC / "flac_decode.c")]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

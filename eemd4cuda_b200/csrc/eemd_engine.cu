@@ -93,6 +93,9 @@ __device__ __forceinline__ void cp_async_el(T* smem, const T* gmem) {
     if (sizeof(T) == 8) cp_async8(smem, gmem);
     else cp_async4(smem, gmem);
 }
+__device__ __forceinline__ void prefetch_l1(const void* gmem) {
+    asm volatile("prefetch.global.L1 [%0];\n" ::"l"(gmem));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -264,7 +267,8 @@ struct Geo {
     static constexpr int TB = WT + 4;                   // tile buffer elements (16-byte phase)
     static constexpr int RS = sizeof(T) == 4 ? 8 : 6;   // interval record stride
     static constexpr size_t TB_BYTES = (size_t)2 * 2 * TB * sizeof(T);  // [buf][stream][TB]
-    static constexpr size_t RI_BYTES = (size_t)2 * 32 * 16;             // [buf][lane]
+    static constexpr int NRB = PREFETCH_L1 ? 3 : 2;                      // run-record buffers
+    static constexpr size_t RI_BYTES = (size_t)NRB * 32 * 16;           // [buf][lane]
     static constexpr int KCAP = WT / 2 + 4;                              // knots of one kind in a tile
     static constexpr size_t KN_BYTES = (size_t)2 * KCAP * (4 + sizeof(T));  // [kind][KCAP] index, value
     // fast mode: the interval records a tile's runs read, staged in shared
@@ -1042,11 +1046,20 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
 #endif
 
     // tile j's samples [t0, t1) and run records into buffer b
+    // run records of tile j: buffer (j - ta) mod NRB; with PREFETCH_L1 they
+    // arrive one tile ahead of the tile's samples, so that the interval records
+    // of tile j+1 can be prefetched into L1 while tile j is processed
+    auto rbuf = [&](int j) { return rib + ((j - ta) % G::NRB) * 32; };
+    auto copy_runs = [&](int j) {
+        if (!SIFTING || j >= tb) return;
+        const int t0 = s0 + j * WT, tl = min(s1, t0 + WT) - t0;
+        if (lane * RUN < tl) cp_async16(rbuf(j) + lane, ri_cur + t0 / RUN + lane);
+    };
     auto prefetch = [&](int j, int b) {
         const int t0 = s0 + j * WT, t1 = min(s1, t0 + WT);
         if (needs_h) tile_copy<T>(tbuf + (b * 2) * G::TB, io.hsrc + t0, t1 - t0, lane);
         if (USES_R) tile_copy<T>(tbuf + (b * 2 + 1) * G::TB, io.rcur + t0, t1 - t0, lane);
-        if (SIFTING && lane * RUN < t1 - t0) cp_async16(rib + b * 32 + lane, ri_cur + t0 / RUN + lane);
+        copy_runs(PREFETCH_L1 ? j + 1 : j);
         cp_async_commit();
     };
 
@@ -1055,8 +1068,8 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
     // the last run's last knot, at most CAPR records (16-byte copies).
     auto stage_recs = [&](int j, int b) {
         const int t0 = s0 + j * WT, tl = min(s1, t0 + WT) - t0;
-        const int4 rf = rib[b * 32];
-        const int4 rl = rib[b * 32 + (tl - 1) / RUN];
+        const int4 rf = rbuf(j)[0];
+        const int4 rl = rbuf(j)[(tl - 1) / RUN];
 #pragma unroll
         for (int env = 0; env < 2; ++env) {
             const int mir = S.mir[env];
@@ -1079,6 +1092,7 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
     T gm1 = (T)0, gm2 = (T)0;  // next-knot values at t0-1 and t0-2 of the current tile
     int cpx = 0, cpn = 0, cmask = 0, crun = 0, cbit = 0;  // run record awaiting its last sample
     if (ta < tb) {
+        if (PREFETCH_L1) copy_runs(ta);
         prefetch(ta, 0);
         if (STAGE) {
             cp_async_wait<0>();
@@ -1114,6 +1128,25 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
             kcc[1] = kcn[1];
         }
         if (j + 1 < tb) prefetch(j + 1, b ^ 1);
+        if (PREFETCH_L1 && SIFTING && j + 1 < tb) {
+            // the next tile's run records are here: pull the interval records
+            // its runs will read into L1 (first, middle and last of each run's
+            // range; a run spans at most a few 128-byte lines)
+            const int tn = s0 + (j + 1) * WT, tln = min(s1, tn + WT) - tn;
+            if (lane * RUN < tln) {
+                const int4 rn = rbuf(j + 1)[lane];
+#pragma unroll
+                for (int env = 0; env < 2; ++env) {
+                    const unsigned m = env ? ((unsigned)rn.z >> 16) : ((unsigned)rn.z & 0xffffu);
+                    const int k0 = max(0, (env ? kbase1 + rn.y : kbase0 + rn.x) + S.mir[env] - 1);
+                    const int k1 = max(k0, min(S.p2[env] - 2, k0 + (int)__popc(m)));
+                    const T* R = env ? R1 : R0;
+                    prefetch_l1(R + (int64_t)k0 * RS);
+                    prefetch_l1(R + (int64_t)((k0 + k1) >> 1) * RS);
+                    prefetch_l1(R + (int64_t)k1 * RS);
+                }
+            }
+        }
         SUB(0);
         const T* hb = tbuf + (b * 2) * G::TB;
         const T* rb = tbuf + (b * 2 + 1) * G::TB;
@@ -1131,7 +1164,7 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
             unsigned kmx = 0u, kmn = 0u;
             int kb0 = 0, kb1 = 0;
             if (nv > 0) {
-                const int4 ri = rib[b * 32 + lane];
+                const int4 ri = rbuf(j)[lane];
                 kmx = (unsigned)ri.z & 0xffffu;
                 kmn = (unsigned)ri.z >> 16;
                 kb0 = kbase0 + ri.x;

@@ -56,6 +56,12 @@ constexpr int FAST_B = EEMD_FAST_B;
 #define EEMD_STAGE_RECS 0
 #endif
 constexpr bool STAGE_RECS = EEMD_STAGE_RECS != 0;
+// fast mode: prefetch the interval records of the sweep's next warp tile
+// into L1 (its run records then arrive one tile ahead of its samples)
+#ifndef EEMD_PREFETCH_L1
+#define EEMD_PREFETCH_L1 0
+#endif
+constexpr bool PREFETCH_L1 = EEMD_PREFETCH_L1 != 0;
 #ifndef EEMD_WSCAP
 #define EEMD_WSCAP 352
 #endif

@@ -141,6 +141,15 @@ def test_other_libraries_export_their_headers(header, module):
         assert hasattr(lib, name), name
 
 
+def test_flac_library_exports_its_header():
+    text = re.sub(r"/\*.*?\*/", "", (HEADER.parent / "eemd_flac.h").read_text(), flags=re.S)
+    declared = sorted(set(re.findall(r"\b(eemd_[a-z_]+)\s*\(", text)))
+    assert declared == ["eemd_flac_decode", "eemd_flac_info", "eemd_flac_strerror"]
+    lib = ctypes.CDLL(str(HEADER.parents[1] / "eemd4cuda_b200" / "lib" / "libeemd_flac.so"))
+    for name in declared:
+        assert hasattr(lib, name), name
+
+
 def test_stft_shape_matches_the_reference_frame_count():
     from eemd4cuda_b200 import _sp
     # scipy.signal.stft(boundary='zeros', padded=False): N + 2*(nperseg//2) samples, hop nperseg - noverlap
