@@ -156,6 +156,24 @@ def make_params(*, dtype=np.float64, noise_mode=L.EEMD_NOISE_NONE, eps=0.2, seed
     return p
 
 
+def tuned(p: L.EemdParams, lengths, trial_count: int) -> L.EemdParams:
+    """The parameters of one launch with the threads per trial (CTAs per task)
+    from the autotune table (eemd4cuda_b200/tuning/) when the caller left
+    cluster_size at 0; otherwise, or without a table entry, p unchanged (the
+    engine then applies its own rule)."""
+    from . import autotune
+
+    if p.cluster_size:
+        return p
+    c = autotune.cluster_size(min(int(n) for n in lengths), len(lengths) * int(trial_count),
+                              "f32" if p.dtype == L.EEMD_F32 else "f64")
+    if not c:
+        return p
+    q = L.EemdParams.from_buffer_copy(p)
+    q.cluster_size = c
+    return q
+
+
 def _tdtype(torch, dt):
     return torch.float64 if np.dtype(dt) == np.dtype(np.float64) else torch.float32
 
@@ -300,14 +318,15 @@ def _run_ensemble(x, *, E, eps, tau, max_sifts, max_imf, min_extrema, end, seed,
     for b0 in range(first, E, batch):
         b1 = min(E, b0 + batch)
         Eb = b1 - b0
-        need = L.workspace_size(p, [N], Eb, False)
+        pb = tuned(p, [N], Eb)
+        need = L.workspace_size(pb, [N], Eb, False)
         if ws is None or ws.numel() < need:
             ws = torch.empty((need,), dtype=torch.uint8, device=dev)
         nz = None
         if host_noise is not None:
             nz = torch.from_numpy(np.ascontiguousarray(host_noise[b0:b1], dtype=dt)).to(dev)
         with nvtx.range("eemd.batch"):
-            L.run(p, xd, [N], b0, Eb, ws, noise=nz, imf_sum=imf_sum, mode_count=mode_count,
+            L.run(pb, xd, [N], b0, Eb, ws, noise=nz, imf_sum=imf_sum, mode_count=mode_count,
                   nsift=cnt[0, b0:b1], nmode=cnt[1, b0:b1], flags=cnt[2, b0:b1])
         if ck is not None:
             with nvtx.range("eemd.checkpoint"):
@@ -353,6 +372,7 @@ def _run_single(x, *, tau, max_sifts, max_imf, min_extrema, end, rules, exact, d
     p = make_params(dtype=dt, noise_mode=L.EEMD_NOISE_NONE, tau=tau, max_sifts=max_sifts,
                     max_imf=slots, min_extrema=min_extrema, end=end, rules=rules, exact=exact,
                     config=config)
+    p = tuned(p, [N], 1)
     xd = torch.from_numpy(np.ascontiguousarray(x, dtype=dt)).to(dev)
     ws = torch.empty((L.workspace_size(p, [N], 1, True),), dtype=torch.uint8, device=dev)
     imfs = torch.zeros((1, slots, N), dtype=tdt, device=dev)
@@ -452,6 +472,7 @@ def decompose_many(xs, E=64, eps=0.2, tau=0.25, max_sifts=50, max_imf=-1, min_ex
         per_trial = L.workspace_size(p, lengths, 1, False)
         batch = max(1, int(free * 0.7 // max(per_trial, 1)))
     batch = max(1, min(int(batch), E))
+    p = tuned(p, lengths, batch)
     xd = torch.from_numpy(np.concatenate([x.astype(dt) for x in xs])).to(dev)
     imf_sum = torch.zeros((slots * NS,), dtype=torch.float64, device=dev)
     mode_count = torch.zeros((S * slots,), dtype=torch.int32, device=dev)
@@ -509,6 +530,7 @@ def gpu_eemd_full(x, E=64, tau=0.25, max_sifts=50, max_imf=12, seed=0, K=None, n
     p = make_params(noise_mode=L.EEMD_NOISE_PREPERTURBED, tau=tau, max_sifts=max_sifts,
                     max_imf=int(max_imf), min_extrema=min_extrema, end=end, rules=rules,
                     exact=exact, config=config)
+    p = tuned(p, [N], E)
     xd = torch.from_numpy(np.ascontiguousarray(x)).to(dev)
     out = torch.zeros((E, int(max_imf), N), dtype=torch.float64, device=dev)
     nsift = torch.zeros((E,), dtype=torch.int32, device=dev)

@@ -1,0 +1,44 @@
+"""Lookup of the threads-per-trial table (eemd4cuda_b200/autotune.py) and its
+use by the Python entry points (no GPU needed)."""
+import numpy as np
+
+from eemd4cuda_b200 import _lib as L
+from eemd4cuda_b200 import autotune as A
+from eemd4cuda_b200 import emd_par as M
+
+TABLE = [(4096, 1, 2), (4096, 1024, 1), (65536, 1, 16), (65536, 100, 4), (65536, 4096, 1),
+         (1 << 22, 64, 8)]
+
+
+def test_lookup_nearest_bucket_and_task_count(monkeypatch):
+    monkeypatch.setattr(A, "_table", lambda dtype: TABLE if dtype == "f32" else None)
+    assert A.cluster_size(48000, 100, "f32") == 4       # nearest bucket 65536, 100 tasks
+    assert A.cluster_size(70000, 2, "f32") == 16        # 1 task is the nearest count
+    assert A.cluster_size(70000, 3000, "f32") == 1
+    assert A.cluster_size(5000, 1, "f32") == 2
+    assert A.cluster_size(3_000_000, 256, "f32") == 8
+    assert A.cluster_size(48000, 100, "f64") == 0       # no table: the engine's own rule
+    # never below 2048 samples per CTA
+    assert A.cluster_size(20000, 1, "f32") == 9
+
+
+def test_tuned_params_respect_an_explicit_choice(monkeypatch):
+    monkeypatch.setattr(A, "_table", lambda dtype: TABLE)
+    p = M.make_params(dtype=np.float32)
+    q = M.tuned(p, [48000], 100)
+    assert q.cluster_size == 4 and p.cluster_size == 0 and q.max_sifts == p.max_sifts
+    p2 = M.make_params(dtype=np.float32, config=M.EngineConfig(cluster_size=3))
+    assert M.tuned(p2, [48000], 100).cluster_size == 3
+    monkeypatch.setattr(A, "_table", lambda dtype: None)
+    assert M.tuned(p, [48000], 100).cluster_size == 0
+
+
+def test_committed_tables_are_well_formed():
+    for dt in ("f32", "f64"):
+        path = A.table_path(dt)
+        if not path.exists():
+            continue
+        A._table.cache_clear()
+        tab = A._table(dt)
+        assert tab and all(1 <= c <= 16 and n >= 1024 and t >= 1 for n, t, c in tab)
+        assert L.EEMD_F32 == 1

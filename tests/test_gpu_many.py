@@ -6,6 +6,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 pytest.importorskip("torch")
 
+from eemd4cuda_b200 import _lib as L  # noqa: E402
 from eemd4cuda_b200 import emd_par as M  # noqa: E402
 from eemd4cuda_b200 import signals  # noqa: E402
 
@@ -40,3 +41,28 @@ def test_eemd_of_many():
     half = M.decompose_many(xs, E=8, seed=3, tau=0.25, max_sifts=20, max_imf=8, dtype=np.float32, batch=4)
     for a, b in zip(many, half):
         assert a.n_modes == b.n_modes and np.array_equal(a.imfs, b.imfs)
+
+
+def test_uneven_batch_against_oracle_per_trial():
+    """Eight signals of mixed lengths (4096 - 65536 samples, the uneven
+    workload's kind) with injected noise, all in one launch (float64, the
+    default seam-window solve): every task equals the oracle's emd_1d of its
+    own perturbed input -- identical knot counts in every sift, IMFs within
+    1e-9 of max|x| (emd_ref.py:108-156)."""
+    from oracle import emd_oracle as O
+    from test_gpu_parity import engine_log, max_imf_err, oracle_log, raw_run
+
+    lengths = [int(round(v)) for v in np.geomspace(4096, 65536, 8)]
+    rng = np.random.default_rng(11)
+    rows = []
+    for i, n in enumerate(lengths):
+        x = signals.harmonic_clicks(n, seed=1000 + i)
+        rows.append(x + 0.2 * np.std(x) * rng.standard_normal(n))
+    res = raw_run(None, x=np.concatenate(rows), lengths=lengths, trial_count=1,
+                  noise_mode=L.EEMD_NOISE_PREPERTURBED, tau=0.0, max_sifts=10, max_imf=10, exact=False)
+    for t, row in enumerate(rows):
+        imfs, _, st = O.emd_1d(row, tau=0.0, max_sifts=10, max_imf=10, record_knots=True)
+        assert int(res["nmode"][t]) == st["n_modes"]
+        assert engine_log(res, t) == oracle_log(st), t
+        err = max_imf_err(res["imfs"][t][:st["n_modes"]], imfs, np.abs(row).max())
+        assert err <= 1e-9, (t, err)
