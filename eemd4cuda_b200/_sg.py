@@ -51,7 +51,7 @@ def load() -> ctypes.CDLL:
                                     c_double, c_int32, c_void_p, c_void_p, c_void_p]
     lib.eemd_sg_stat_count.restype = c_int32
     lib.eemd_sg_wgrad.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32,
-                                  c_int32, c_int32, c_int32, c_void_p]
+                                  c_int32, c_int32, c_int32, c_int32, c_void_p, c_int64, c_void_p]
     lib.eemd_sg_loss.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32,
                                  c_int32, c_int32, c_int32, c_float, c_void_p, c_void_p]
     lib.eemd_sg_adam.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_float, c_float, c_float,
@@ -112,9 +112,9 @@ def combine(imf_sum, mode_count, x, scl, net_out, imfs_out, resid_out, partial, 
            "eemd_sg_combine")
 
 
-def wgrad(dy, x, dw, db, B, T, n_rows, c, nv, cv, dil):
-    _check(load().eemd_sg_wgrad(_p(dy), _p(x), _p(dw), _p(db), B, T, n_rows, c, nv, cv, dil, _stream()),
-           "eemd_sg_wgrad")
+def wgrad(dy, x, dw, db, B, T, n_rows, c, nv, cv, dil, tensor_cores=True, err=None, spin_limit=0):
+    _check(load().eemd_sg_wgrad(_p(dy), _p(x), _p(dw), _p(db), B, T, n_rows, c, nv, cv, dil, int(tensor_cores),
+                                _p(err), spin_limit, _stream()), "eemd_sg_wgrad")
 
 
 def loss(out, base, target, dout, acc, B, T, c, cv, margin, project=False, delta=0.0, weights=None):

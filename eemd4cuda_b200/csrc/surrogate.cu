@@ -761,6 +761,153 @@ __global__ void __launch_bounds__(NT) k_wgrad(const __nv_bfloat16* __restrict__ 
     }
 }
 
+// Weight gradient on the tensor cores.  A GEMM with K = time: per tile of 128
+// time samples of one batch row the CTA stages, in the K-major core-matrix
+// layout of the forward kernel (8 rows x 16 bytes, no swizzle),
+//   A_j[r][k] = x[b][t0 + k + (tap - 1) dil][c]   for row m = 128 j + r = tap C + c
+//               (rows past 3C, and times outside [0, T), zero)
+//   Bm[n][k]  = dy[b][t0 + k][n]
+// with plain loads (the time-major image is a transpose of the channels-last
+// tensors), and one thread issues tcgen05.mma kind::f16 (bf16 x bf16 -> f32,
+// M = 128, N = NP, K = 16 per instruction) into NB accumulators D_j[m][n] in
+// tensor memory that stay resident over all the CTA's tiles.  The epilogue
+// reads them with tcgen05.ld and adds them to dw[n][tap][c] with atomics; db
+// is summed from the staged dy on the CUDA cores.  Same operand shapes and
+// descriptors as k_conv_tc (M = 128 rows, N = output channels).
+template <int NB, int NP>
+__global__ void __launch_bounds__(NT) k_wgrad_tc(const __nv_bfloat16* __restrict__ dy,
+                                                 const __nv_bfloat16* __restrict__ x, float* dw, float* db,
+                                                 int B, int T, int N, int C, int nv, int cv, int dil, int* err,
+                                                 long long spin_limit) {
+    constexpr int KT = 128;                  // time samples per tile (the GEMM's K)
+    constexpr int A_BYTES = 128 * KT * 2;    // one M block
+    constexpr int TCOLS = (NB * NP) <= 32 ? 32 : ((NB * NP) <= 64 ? 64 : 128);
+    static_assert(NB >= 1 && NB <= 2 && (NP == 16 || NP == 64), "shape");
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __nv_bfloat16* sA = reinterpret_cast<__nv_bfloat16*>(smem);
+    __nv_bfloat16* sB = reinterpret_cast<__nv_bfloat16*>(smem + NB * A_BYTES);
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ float sdb[NP];
+    const int tid = threadIdx.x, warp = tid >> 5;
+    if (tid < NP) sdb[tid] = 0.f;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                         smem_u32(&tmem_slot)),
+                     "r"(TCOLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mbar)));
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB);
+    constexpr uint32_t IDESC = instr_desc(128, NP);
+    const int tiles_per_b = (T + KT - 1) / KT;
+    const int n_tiles = B * tiles_per_b;
+    uint32_t phase = 0;
+    bool failed = false;
+    int issued = 0;
+    float dbacc = 0.f;  // this thread's share of db (rows n = tid when tid < NP)
+    for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const int b = tile / tiles_per_b, t0 = (tile % tiles_per_b) * KT;
+        const __nv_bfloat16* xb = x + (size_t)b * T * C;
+        const __nv_bfloat16* dyb = dy + (size_t)b * T * N;
+        // A: thread r fills row r of every block, 8 times at a time
+        for (int j = 0; j < NB; ++j) {
+            const int m = 128 * j + tid;
+            const bool row_ok = m < 3 * C;
+            const int tap = row_ok ? m / C : 0, c = row_ok ? m % C : 0;
+            for (int kc = 0; kc < KT / 8; ++kc) {
+                __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const int t = t0 + kc * 8 + i, ts = t + (tap - 1) * dil;
+                    h[i] = (row_ok && t < T && ts >= 0 && ts < T) ? xb[(size_t)ts * C + c] : __float2bfloat16(0.f);
+                }
+                *reinterpret_cast<uint4*>(sA + j * (A_BYTES / 2) + kmaj_off(tid, kc * 8, 128)) =
+                    *reinterpret_cast<const uint4*>(h);
+            }
+        }
+        // B (and the bias gradient): item (n, kc), n fastest
+        for (int it = tid; it < NP * (KT / 8); it += NT) {
+            const int n = it % NP, kc = it / NP;
+            __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int t = t0 + kc * 8 + i;
+                h[i] = (n < N && t < T) ? dyb[(size_t)t * N + n] : __float2bfloat16(0.f);
+                if (n < nv) dbacc += __bfloat162float(h[i]);
+            }
+            *reinterpret_cast<uint4*>(sB + kmaj_off(n, kc * 8, NP)) = *reinterpret_cast<const uint4*>(h);
+        }
+        // generic-proxy shared-memory writes become visible to the tensor cores
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+#pragma unroll
+                for (int s = 0; s < KT / 16; ++s) {
+                    const uint64_t da = smem_desc(a_base + j * A_BYTES + s * 2 * (128 * 16), 128 * 16, 128);
+                    const uint64_t dd = smem_desc(b_base + s * 2 * (NP * 16), NP * 16, 128);
+                    const uint32_t acc = (issued > 0 || s > 0) ? 1u : 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem + (uint32_t)(j * NP)),
+                        "l"(da), "l"(dd), "r"(IDESC), "r"(acc));
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             smem_u32(&mbar))
+                         : "memory");
+        }
+        ++issued;
+        // the next tile's staging overwrites the operands: wait for the MMAs (bounded)
+        if (!wait_parity(&mbar, phase, spin_limit)) failed = true;
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        if (__syncthreads_or(failed ? 1 : 0)) {
+            if (tid == 0) raise(err, EEMD_SG_E_TIMEOUT);
+            break;
+        }
+    }
+    if (!failed && issued > 0) {
+        // epilogue: warp w holds accumulator lanes 32w..32w+31 (rows m of each block)
+        for (int j = 0; j < NB; ++j) {
+            float v[NP];
+            tmem_ld<NP>(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(j * NP), v);
+            const int m = 128 * j + 32 * warp + (tid & 31);
+            if (m < 3 * C) {
+                const int tap = m / C, c = m % C;
+                if (c < cv) {
+#pragma unroll
+                    for (int n = 0; n < NP; ++n)
+                        if (n < nv) atomicAdd(&dw[((size_t)n * 3 + tap) * cv + c], v[n]);
+                }
+            }
+        }
+    }
+    // bias gradient: the per-thread partial sums of the staged dy rows
+    if (NP * (KT / 8) % NT == 0) {
+        // every thread always handled the same row n = tid % NP
+        atomicAdd(&sdb[tid % NP], dbacc);
+    }
+    __syncthreads();
+    if (tid < nv && tid < NP && !failed) atomicAdd(&db[tid], sdb[tid]);
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
+    }
+}
+
 // prediction = base + out (residual form; base may be null) over the first
 // `cv` of `C` channels; loss partial sums over the interior [margin, T - margin)
 // and the gradient d loss / d out as bf16.  The loss per element is d^2 for
@@ -1152,6 +1299,20 @@ int launch_tc(const void* in, const void* wpk, const float* bias, void* out, int
 }
 }  // namespace
 
+template <int NB, int NP>
+int32_t launch_wgrad_tc(const __nv_bfloat16* dy, const __nv_bfloat16* x, float* dw, float* db, int B, int T, int N,
+                        int C, int nv, int cv, int dil, int* err, long long spin, cudaStream_t st) {
+    const size_t smem = (size_t)NB * 128 * 128 * 2 + (size_t)NP * 128 * 2;
+    if (cudaFuncSetAttribute(k_wgrad_tc<NB, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return EEMD_SG_E_CUDA;
+    const long long tiles = (long long)B * ((T + 127) / 128);
+    const int grid = (int)(tiles < 296 ? tiles : 296);  // two CTAs per SM (shared memory and tensor memory allow it)
+    if (grid < 1) return EEMD_SG_OK;
+    k_wgrad_tc<NB, NP><<<grid, NT, smem, st>>>(dy, x, dw, db, B, T, N, C, nv, cv, dil, err, spin);
+    return cudaGetLastError() == cudaSuccess ? EEMD_SG_OK : EEMD_SG_E_CUDA;
+}
+
 extern "C" {
 
 int32_t eemd_sg_version(void) { return EEMD_SG_ABI_VERSION; }
@@ -1204,8 +1365,20 @@ int32_t eemd_sg_pack(const float* w, void* wpk, int32_t n_rows, int32_t c, int32
 }
 
 int32_t eemd_sg_wgrad(const void* dy, const void* x, float* dw, float* db, int32_t B, int32_t T, int32_t n_rows,
-                      int32_t c, int32_t nv, int32_t cv, int32_t dil, void* stream) {
+                      int32_t c, int32_t nv, int32_t cv, int32_t dil, int32_t tensor_cores, int32_t* err,
+                      int64_t spin_limit, void* stream) {
     if (!dy || !x || !dw || !db || n_rows > 64 || c > 64 || nv > n_rows || cv > c) return EEMD_SG_E_BADARG;
+    if (tensor_cores && (n_rows == 64 || n_rows == 16) && c >= 1) {
+        const long long spin = spin_limit > 0 ? spin_limit : (1LL << 24);
+        const cudaStream_t st = static_cast<cudaStream_t>(stream);
+        const auto* pdy = static_cast<const __nv_bfloat16*>(dy);
+        const auto* px = static_cast<const __nv_bfloat16*>(x);
+        if (3 * c <= 128)
+            return n_rows == 64 ? launch_wgrad_tc<1, 64>(pdy, px, dw, db, B, T, n_rows, c, nv, cv, dil, err, spin, st)
+                                : launch_wgrad_tc<1, 16>(pdy, px, dw, db, B, T, n_rows, c, nv, cv, dil, err, spin, st);
+        return n_rows == 64 ? launch_wgrad_tc<2, 64>(pdy, px, dw, db, B, T, n_rows, c, nv, cv, dil, err, spin, st)
+                            : launch_wgrad_tc<2, 16>(pdy, px, dw, db, B, T, n_rows, c, nv, cv, dil, err, spin, st);
+    }
     dim3 grid((unsigned)(B * ((T + 63) / 64)), 3);
     k_wgrad<<<grid, NT, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<const __nv_bfloat16*>(dy),
                                                                  static_cast<const __nv_bfloat16*>(x), dw, db, B, T,

@@ -215,7 +215,7 @@ class Net:
         for li in range(len(self.layers) - 1, -1, -1):
             lay = self.layers[li]
             SG.wgrad(g, acts[li], lay["dw"], lay["db"], B, T, lay["cout_p"], lay["cin_p"], lay["cout_v"],
-                     lay["cin_v"], lay["dil"])
+                     lay["cin_v"], lay["dil"], tensor_cores=tensor_cores)
             if li > 0:
                 gi = self.torch.empty((B, T, lay["cin_p"]), dtype=self.torch.bfloat16, device="cuda")
                 # the input gradient times the ReLU derivative of the layer below (its output > 0)

@@ -61,9 +61,13 @@ int32_t eemd_sg_bias(const float* b, float* bias, int32_t n_rows, int32_t nv, in
 
 /* Accumulates dw[n][tap][c] += sum_t dy[b][t][n] * x[b][t+(tap-1)*dil][c]
  * (n < nv, c < cv) and db[n] += sum_t dy[b][t][n]; dy is [B][T][n_rows],
- * x is [B][T][c] (both bf16, n_rows, c <= 64). */
+ * x is [B][T][c] (both bf16, n_rows, c <= 64).  tensor_cores != 0 (and n_rows
+ * 16 or 64): an implicit GEMM over time on tcgen05 (accumulators in tensor
+ * memory; a wait that gives up after spin_limit polls -- 0 = default -- sets
+ * *err to EEMD_SG_E_TIMEOUT); otherwise the CUDA-core kernel. */
 int32_t eemd_sg_wgrad(const void* dy, const void* x, float* dw, float* db, int32_t B, int32_t T, int32_t n_rows,
-                      int32_t c, int32_t nv, int32_t cv, int32_t dil, void* stream);
+                      int32_t c, int32_t nv, int32_t cv, int32_t dil, int32_t tensor_cores, int32_t* err,
+                      int64_t spin_limit, void* stream);
 
 /* Mean error of base + out (base may be null) against target over channels
  * < cv and time [margin, T - margin): squared (delta <= 0) or Huber with

@@ -74,18 +74,24 @@ def test_input_gradient_conv_with_mask(cin, cout):
     assert np.max(np.abs(f64(dx) - o)) <= 2 ** -7 * np.max(np.abs(o)) + 1e-3
 
 
-def test_weight_gradient():
+@pytest.mark.parametrize("N,C,nv,cv", [(64, 16, 64, 16), (64, 64, 64, 64), (16, 64, 10, 64), (64, 16, 64, 11)])
+@pytest.mark.parametrize("tensor_cores", [True, False])
+def test_weight_gradient(N, C, nv, cv, tensor_cores):
+    """Weight and bias gradients (tcgen05 implicit GEMM over time, and the
+    CUDA-core kernel) against the float64 oracle on the same bf16 operands."""
     rng = np.random.default_rng(3)
-    B, T, dil, N, C = 2, 500, 8, 64, 16
+    B, T, dil = 2, 500, 8
     dy = rng.standard_normal((B, T, N)).astype(np.float32)
     x = rng.standard_normal((B, T, C)).astype(np.float32)
-    dw = torch.zeros((N, 3, C), dtype=torch.float32, device="cuda")
-    db = torch.zeros((N,), dtype=torch.float32, device="cuda")
-    _sg.wgrad(bf16(dy).cuda(), bf16(x).cuda(), dw, db, B, T, N, C, N, C, dil)
+    dw = torch.zeros((nv, 3, cv), dtype=torch.float32, device="cuda")
+    db = torch.zeros((nv,), dtype=torch.float32, device="cuda")
+    err = torch.zeros((1,), dtype=torch.int32, device="cuda")
+    _sg.wgrad(bf16(dy).cuda(), bf16(x).cuda(), dw, db, B, T, N, C, nv, cv, dil, tensor_cores=tensor_cores, err=err)
     torch.cuda.synchronize()
+    assert int(err.item()) == 0
     ow, ob = SO.conv_weight_grad(f64(bf16(dy)), f64(bf16(x)), dil)
-    assert np.allclose(dw.cpu().numpy(), ow, rtol=1e-4, atol=1e-3)
-    assert np.allclose(db.cpu().numpy(), ob, rtol=1e-4, atol=1e-3)
+    assert np.allclose(dw.cpu().numpy(), ow[:nv, :, :cv], rtol=1e-4, atol=1e-3)
+    assert np.allclose(db.cpu().numpy(), ob[:nv], rtol=1e-4, atol=1e-3)
 
 
 def test_loss_and_adam():
