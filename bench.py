@@ -116,7 +116,7 @@ WORKLOADS = {
         "amfm4m",
         {"workload": "amfm_2^22_eemd", "N": 1 << 22, "trials": 256, "eps": 0.2, "max_imf": 12,
          "tau": 0.2, "max_sifts": 20, "storage": "float64", "solve": "float64",
-         "seam_halo": 30, "noise": "philox", "signals": 1, "trials_per_launch": 64},
+         "seam_halo": 30, "knots_per_block": 5, "noise": "philox", "signals": 1, "trials_per_launch": 64},
         E=256, eps=0.2, max_imf=12, max_sifts=20, tau=0.2, dtype="f64", seed=2, halo=30,
         trial_batch=64, cpu_tasks=16, cpu_max_imf=1, cpu_max_sifts=2, signals_fn=_amfm),
     "uneven512": Workload(
