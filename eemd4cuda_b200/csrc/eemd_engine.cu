@@ -93,9 +93,6 @@ __device__ __forceinline__ void cp_async_el(T* smem, const T* gmem) {
     if (sizeof(T) == 8) cp_async8(smem, gmem);
     else cp_async4(smem, gmem);
 }
-__device__ __forceinline__ void prefetch_l1(const void* gmem) {
-    asm volatile("prefetch.global.L1 [%0];\n" ::"l"(gmem));
-}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -266,17 +263,12 @@ struct Geo {
     static constexpr int WT = 32 * RUN;                 // samples per warp tile
     static constexpr int TB = WT + 4;                   // tile buffer elements (16-byte phase)
     static constexpr int RS = sizeof(T) == 4 ? 8 : 6;   // interval record stride
-    static constexpr size_t TB_BYTES = (size_t)2 * 2 * TB * sizeof(T);  // [buf][stream][TB]
-    static constexpr int NRB = PREFETCH_L1 ? 3 : 2;                      // run-record buffers
-    static constexpr size_t RI_BYTES = (size_t)NRB * 32 * 16;           // [buf][lane]
+    static constexpr int NBUF = TILE_BUFS;               // tiles in flight per warp (ring)
+    static constexpr size_t TB_BYTES = (size_t)NBUF * 2 * TB * sizeof(T);  // [buf][stream][TB]
+    static constexpr size_t RI_BYTES = (size_t)NBUF * 32 * 16;          // [buf][lane]
     static constexpr int KCAP = WT / 2 + 4;                              // knots of one kind in a tile
     static constexpr size_t KN_BYTES = (size_t)2 * KCAP * (4 + sizeof(T));  // [kind][KCAP] index, value
-    // fast mode: the interval records a tile's runs read, staged in shared
-    // memory one tile ahead ([env][CAPR] records; a tile with more knots reads
-    // the rest from global memory)
-    static constexpr int CAPR = 48;
-    static constexpr size_t RST_BYTES = STAGE_RECS ? (size_t)2 * CAPR * RS * sizeof(T) : 0;
-    static constexpr size_t WARP_BYTES = TB_BYTES + RI_BYTES + KN_BYTES + RST_BYTES;
+    static constexpr size_t WARP_BYTES = TB_BYTES + RI_BYTES + KN_BYTES;
     static_assert(TB_BYTES % 16 == 0 && (RS * sizeof(T)) % 16 == 0 && KN_BYTES % 16 == 0,
                   "16-byte aligned layouts");
 };
@@ -791,15 +783,6 @@ __device__ __forceinline__ void load_iv(Iv<T>& v, const T* R, int k) {
     }
 }
 
-// interval record k from the tile's staged copy (records kf .. kf+cnt-1) when
-// it holds k, else from global memory
-template <typename T, bool EXACT>
-__device__ __forceinline__ void load_iv_st(Iv<T>& v, const T* R, const T* st, int kf, int cnt, int k) {
-    if ((unsigned)(k - kf) < (unsigned)cnt) load_iv<T, EXACT>(v, st, k - kf);
-    else load_iv<T, EXACT>(v, R, k);
-    v.k = k;
-}
-
 template <typename T, bool EXACT>
 __device__ __forceinline__ T iv_eval(const Iv<T>& v, int t) {
     if (EXACT)
@@ -1014,6 +997,11 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
     const T* R0 = static_cast<const T*>(sl.M);
     const T* R1 = R0 + (int64_t)C.kcap * RS;
     const int kbase0 = S.pref[S.kpar][0][seg], kbase1 = S.pref[S.kpar][1][seg];
+    // the step's envelope constants, read from shared memory once per sweep
+    const bool both_splines = S.P[0] >= 2 && S.P[1] >= 2;
+    const int mir0 = S.mir[0], mir1 = S.mir[1];
+    const int tf0 = S.tfirst[0], tf1 = S.tfirst[1], tl0 = S.tlast[0], tl1 = S.tlast[1];
+    const int p2m0 = S.p2[0] - 1, p2m1 = S.p2[1] - 1;
     const int nt = (s1 - s0 + WT - 1) / WT;
     const int ta = wid * nt / NWARP, tb = (wid + 1) * nt / NWARP;
     const int r0 = s0 + ta * WT, r1 = min(s1, s0 + tb * WT);  // the warp's range [r0, r1)
@@ -1024,11 +1012,6 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
     // the tile's new knots, compacted in time order before one coalesced copy out
     int* const kts = reinterpret_cast<int*>(wb + G::TB_BYTES + G::RI_BYTES);  // [kind][KCAP]
     T* const kvs = reinterpret_cast<T*>(wb + G::TB_BYTES + G::RI_BYTES + 2 * G::KCAP * 4);
-    // staged interval records of the current tile: [env][CAPR][RS]
-    T* const rst = reinterpret_cast<T*>(wb + G::TB_BYTES + G::RI_BYTES + G::KN_BYTES);
-    constexpr bool STAGE = STAGE_RECS && !EXACT && SIFTING;
-    int kfc[2] = {0, 0}, kcc[2] = {0, 0};  // first staged record and count, current tile
-    int kfn[2] = {0, 0}, kcn[2] = {0, 0};  // the same for the next tile
     double num = 0.0, den = 0.0;
 #ifdef EEMD_TRACE
     unsigned long long scyc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -1046,60 +1029,22 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
 #endif
 
     // tile j's samples [t0, t1) and run records into buffer b
-    // run records of tile j: buffer (j - ta) mod NRB; with PREFETCH_L1 they
-    // arrive one tile ahead of the tile's samples, so that the interval records
-    // of tile j+1 can be prefetched into L1 while tile j is processed
-    auto rbuf = [&](int j) { return rib + ((j - ta) % G::NRB) * 32; };
-    auto copy_runs = [&](int j) {
-        if (!SIFTING || j >= tb) return;
-        const int t0 = s0 + j * WT, tl = min(s1, t0 + WT) - t0;
-        if (lane * RUN < tl) cp_async16(rbuf(j) + lane, ri_cur + t0 / RUN + lane);
-    };
-    auto prefetch = [&](int j, int b) {
-        const int t0 = s0 + j * WT, t1 = min(s1, t0 + WT);
-        if (needs_h) tile_copy<T>(tbuf + (b * 2) * G::TB, io.hsrc + t0, t1 - t0, lane);
-        if (USES_R) tile_copy<T>(tbuf + (b * 2 + 1) * G::TB, io.rcur + t0, t1 - t0, lane);
-        copy_runs(PREFETCH_L1 ? j + 1 : j);
+    // tile j's samples and run records live in ring buffer (j - ta) mod NBUF;
+    // NBUF - 1 tiles are in flight while one is processed
+    auto bufi = [&](int j) { return (j - ta) % G::NBUF; };
+    auto prefetch = [&](int j) {
+        const int t0 = s0 + j * WT, t1 = min(s1, t0 + WT), bi = bufi(j);
+        if (needs_h) tile_copy<T>(tbuf + (bi * 2) * G::TB, io.hsrc + t0, t1 - t0, lane);
+        if (USES_R) tile_copy<T>(tbuf + (bi * 2 + 1) * G::TB, io.rcur + t0, t1 - t0, lane);
+        if (SIFTING && lane * RUN < t1 - t0) cp_async16(rib + bi * 32 + lane, ri_cur + t0 / RUN + lane);
         cp_async_commit();
-    };
-
-    // Stage the records tile j's runs read (run records in buffer b): per
-    // envelope the contiguous range from the first run's current interval to
-    // the last run's last knot, at most CAPR records (16-byte copies).
-    auto stage_recs = [&](int j, int b) {
-        const int t0 = s0 + j * WT, tl = min(s1, t0 + WT) - t0;
-        const int4 rf = rbuf(j)[0];
-        const int4 rl = rbuf(j)[(tl - 1) / RUN];
-#pragma unroll
-        for (int env = 0; env < 2; ++env) {
-            const int mir = S.mir[env];
-            const int kb = env ? kbase1 : kbase0;
-            const int first = max(0, kb + (env ? rf.y : rf.x) + mir - 1);
-            const unsigned ml = env ? ((unsigned)rl.z >> 16) : ((unsigned)rl.z & 0xffffu);
-            const int last = min(S.p2[env] - 2, kb + (env ? rl.y : rl.x) + __popc(ml) + mir - 1);
-            const int cnt = S.P[env] < 2 ? 0 : max(0, min(G::CAPR, last - first + 1));
-            kfn[env] = first;
-            kcn[env] = cnt;
-            constexpr int CH = RS * (int)sizeof(T) / 16;  // 16-byte chunks per record
-            constexpr int EL = 16 / (int)sizeof(T);       // elements per chunk
-            const T* src = (env ? R1 : R0) + (int64_t)first * RS;
-            T* dst = rst + env * G::CAPR * RS;
-            for (int c = lane; c < cnt * CH; c += 32) cp_async16(dst + c * EL, src + c * EL);
-        }
     };
 
     int wcx = 0, wcy = 0;  // knots of each kind written to the warp's lists so far
     T gm1 = (T)0, gm2 = (T)0;  // next-knot values at t0-1 and t0-2 of the current tile
     int cpx = 0, cpn = 0, cmask = 0, crun = 0, cbit = 0;  // run record awaiting its last sample
     if (ta < tb) {
-        if (PREFETCH_L1) copy_runs(ta);
-        prefetch(ta, 0);
-        if (STAGE) {
-            cp_async_wait<0>();
-            __syncwarp();
-            stage_recs(ta, 0);
-            cp_async_commit();
-        }
+        for (int q = 0; q < G::NBUF - 1 && ta + q < tb; ++q) prefetch(ta + q);
         if (r0 > 0) {
             // the sample before the range: its value is the left neighbour of the range's first sample
             int c0 = 0, c1 = 0;
@@ -1113,40 +1058,20 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
         }
     }
 
-    int b = 0;
-    for (int j = ta; j < tb; ++j, b ^= 1) {
+    for (int j = ta; j < tb; ++j) {
         const int t0 = s0 + j * WT, t1 = min(s1, t0 + WT), tl = t1 - t0;
         const int j0 = lane * RUN;
         const int nv = max(0, min(RUN, tl - j0));  // valid samples of this lane's run
         const int last_lane = (tl - 1) / RUN;
-        cp_async_wait<0>();
+        const int b = bufi(j);
+        // tile j's copies are complete when at most the later tiles' groups
+        // (up to NBUF - 2 of them) are still pending
+        const int later = min(G::NBUF - 2, tb - 1 - j);
+        if (later >= 2) cp_async_wait<2>();
+        else if (later == 1) cp_async_wait<1>();
+        else cp_async_wait<0>();
         __syncwarp();
-        if (STAGE) {
-            kfc[0] = kfn[0];
-            kfc[1] = kfn[1];
-            kcc[0] = kcn[0];
-            kcc[1] = kcn[1];
-        }
-        if (j + 1 < tb) prefetch(j + 1, b ^ 1);
-        if (PREFETCH_L1 && SIFTING && j + 1 < tb) {
-            // the next tile's run records are here: pull the interval records
-            // its runs will read into L1 (first, middle and last of each run's
-            // range; a run spans at most a few 128-byte lines)
-            const int tn = s0 + (j + 1) * WT, tln = min(s1, tn + WT) - tn;
-            if (lane * RUN < tln) {
-                const int4 rn = rbuf(j + 1)[lane];
-#pragma unroll
-                for (int env = 0; env < 2; ++env) {
-                    const unsigned m = env ? ((unsigned)rn.z >> 16) : ((unsigned)rn.z & 0xffffu);
-                    const int k0 = max(0, (env ? kbase1 + rn.y : kbase0 + rn.x) + S.mir[env] - 1);
-                    const int k1 = max(k0, min(S.p2[env] - 2, k0 + (int)__popc(m)));
-                    const T* R = env ? R1 : R0;
-                    prefetch_l1(R + (int64_t)k0 * RS);
-                    prefetch_l1(R + (int64_t)((k0 + k1) >> 1) * RS);
-                    prefetch_l1(R + (int64_t)k1 * RS);
-                }
-            }
-        }
+        if (j + G::NBUF - 1 < tb) prefetch(j + G::NBUF - 1);
         SUB(0);
         const T* hb = tbuf + (b * 2) * G::TB;
         const T* rb = tbuf + (b * 2 + 1) * G::TB;
@@ -1164,7 +1089,7 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
             unsigned kmx = 0u, kmn = 0u;
             int kb0 = 0, kb1 = 0;
             if (nv > 0) {
-                const int4 ri = rbuf(j)[lane];
+                const int4 ri = rib[b * 32 + lane];
                 kmx = (unsigned)ri.z & 0xffffu;
                 kmn = (unsigned)ri.z >> 16;
                 kb0 = kbase0 + ri.x;
@@ -1172,14 +1097,14 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
             }
             // interior tile: every sample's interval is (knots before it) + mir - 1, no clipping
             const int ta0 = t0 + j0, ta1 = t0 + j0 + nv - 1;
-            bool ok = S.P[0] >= 2 && S.P[1] >= 2;
+            bool ok = both_splines;
 #pragma unroll
             for (int env = 0; env < 2; ++env) {
                 const int kb = env ? kb1 : kb0;
                 const int kc = __popc(env ? kmn : kmx);
-                const int mir = S.mir[env];
-                ok = ok && (!mir || (S.tfirst[env] < ta0 && S.tlast[env] >= ta1));
-                ok = ok && (kb + mir >= 1) && (kb + kc + mir <= S.p2[env] - 1);
+                const int mir = env ? mir1 : mir0;
+                ok = ok && (!mir || ((env ? tf1 : tf0) < ta0 && (env ? tl1 : tl0) >= ta1));
+                ok = ok && (kb + mir >= 1) && (kb + kc + mir <= (env ? p2m1 : p2m0));
             }
             const bool fast = __all_sync(FULL, ok || nv == 0);
             T tnum = (T)0, tden = (T)0;  // fast mode: this tile's SD partial sums
@@ -1206,40 +1131,27 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
                 c0.t0 = c0.t1 = 0;
                 c0.y0 = c0.c1 = c0.c2 = c0.c3 = c0.y1 = c0.m1 = (T)0;
                 n0 = c1 = n1 = c0;
-                int k0 = kb0 + S.mir[0] - 1, k1 = kb1 + S.mir[1] - 1;
+                int k0 = kb0 + mir0 - 1, k1 = kb1 + mir1 - 1;
                 if (nv > 0) {
                     // the interior test above keeps every index of the run in [0, p2 - 2]
                     EEMD_CHECK_IV(k0, S.p2[0] - 2 - (int)__popc(kmx));
                     EEMD_CHECK_IV(k1, S.p2[1] - 2 - (int)__popc(kmn));
-                    if (STAGE) {
-                        load_iv_st<T, EXACT>(c0, R0, rst, kfc[0], kcc[0], k0);
-                        load_iv_st<T, EXACT>(c1, R1, rst + G::CAPR * RS, kfc[1], kcc[1], k1);
-                        if (kmx) load_iv_st<T, EXACT>(n0, R0, rst, kfc[0], kcc[0], k0 + 1);
-                        if (kmn) load_iv_st<T, EXACT>(n1, R1, rst + G::CAPR * RS, kfc[1], kcc[1], k1 + 1);
-                    } else {
-                        load_iv<T, EXACT>(c0, R0, k0);
-                        load_iv<T, EXACT>(c1, R1, k1);
-                        if (kmx) load_iv<T, EXACT>(n0, R0, k0 + 1);
-                        if (kmn) load_iv<T, EXACT>(n1, R1, k1 + 1);
-                    }
+                    load_iv<T, EXACT>(c0, R0, k0);
+                    load_iv<T, EXACT>(c1, R1, k1);
+                    if (kmx) load_iv<T, EXACT>(n0, R0, k0 + 1);
+                    if (kmn) load_iv<T, EXACT>(n1, R1, k1 + 1);
                 }
 #pragma unroll
                 for (int i = 0; i < RUN; ++i) {
                     if (i > 0 && ((kmx >> (i - 1)) & 1u)) {
                         c0 = n0;
                         ++k0;
-                        if (kmx >> i) {
-                            if (STAGE) load_iv_st<T, EXACT>(n0, R0, rst, kfc[0], kcc[0], k0 + 1);
-                            else load_iv<T, EXACT>(n0, R0, k0 + 1);
-                        }
+                        if (kmx >> i) load_iv<T, EXACT>(n0, R0, k0 + 1);
                     }
                     if (i > 0 && ((kmn >> (i - 1)) & 1u)) {
                         c1 = n1;
                         ++k1;
-                        if (kmn >> i) {
-                            if (STAGE) load_iv_st<T, EXACT>(n1, R1, rst + G::CAPR * RS, kfc[1], kcc[1], k1 + 1);
-                            else load_iv<T, EXACT>(n1, R1, k1 + 1);
-                        }
+                        if (kmn >> i) load_iv<T, EXACT>(n1, R1, k1 + 1);
                     }
                     const int t = t0 + j0 + i;
                     if (i < nv) finish(i, (T)0.5 * (iv_eval<T, EXACT>(c0, t) + iv_eval<T, EXACT>(c1, t)));
@@ -1268,15 +1180,6 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
 #pragma unroll
             for (int i = 0; i < RUN; ++i)
                 if (i < nv) plain_value<T, MODE>(C, S, d, t0 + j0 + i, hv[i], rv[i], fv[i], gv[i]);
-        }
-        if (STAGE && j + 1 < tb) {
-            // this tile's records are consumed: stage the next tile's while
-            // this tile's extrema and writes run (its run records came with
-            // the prefetch issued at the top of this tile)
-            cp_async_wait<0>();
-            __syncwarp();
-            stage_recs(j + 1, b ^ 1);
-            cp_async_commit();
         }
         SUB(1);
 

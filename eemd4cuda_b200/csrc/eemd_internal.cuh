@@ -50,18 +50,13 @@ constexpr int MAXC = 16;
 #define EEMD_FAST_B 5
 #endif
 constexpr int FAST_B = EEMD_FAST_B;
-// fast mode: stage the interval records of the sweep's next warp tile in
-// shared memory (1) or read them from global memory as each run needs them (0)
-#ifndef EEMD_STAGE_RECS
-#define EEMD_STAGE_RECS 0
+// warp tiles of samples in flight per sweep warp (a ring of buffers: the
+// copies of the next TILE_BUFS - 1 tiles run while one tile is processed)
+#ifndef EEMD_TILE_BUFS
+#define EEMD_TILE_BUFS 2
 #endif
-constexpr bool STAGE_RECS = EEMD_STAGE_RECS != 0;
-// fast mode: prefetch the interval records of the sweep's next warp tile
-// into L1 (its run records then arrive one tile ahead of its samples)
-#ifndef EEMD_PREFETCH_L1
-#define EEMD_PREFETCH_L1 0
-#endif
-constexpr bool PREFETCH_L1 = EEMD_PREFETCH_L1 != 0;
+constexpr int TILE_BUFS = EEMD_TILE_BUFS;
+static_assert(TILE_BUFS >= 2 && TILE_BUFS <= 4, "two to four tile buffers");
 #ifndef EEMD_WSCAP
 #define EEMD_WSCAP 352
 #endif
