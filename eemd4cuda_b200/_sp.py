@@ -8,9 +8,9 @@ from pathlib import Path
 LIB_DIR = Path(__file__).resolve().parent / "lib"
 SP_OK = 0
 ABI_VERSION = 1
-EXPORTS = ("eemd_sp_version", "eemd_sp_hilbert_workspace", "eemd_sp_hilbert_if", "eemd_sp_stft_shape",
-           "eemd_sp_stft_workspace", "eemd_sp_stft")
-_ERR = {-1: "bad argument", -2: "workspace too small", -5: "CUDA error", -6: "cuFFT error"}
+EXPORTS = ("eemd_sp_version", "eemd_sp_fft_workspace", "eemd_sp_fft", "eemd_sp_hilbert_workspace",
+           "eemd_sp_hilbert_if", "eemd_sp_stft_shape", "eemd_sp_stft_workspace", "eemd_sp_stft")
+_ERR = {-1: "bad argument", -2: "workspace too small", -5: "CUDA error"}
 
 _lib = None
 
@@ -36,6 +36,8 @@ def load() -> ctypes.CDLL:
     lib.eemd_sp_version.restype = c_int32
     if lib.eemd_sp_version() != ABI_VERSION:
         raise RuntimeError("libeemd_spectra.so ABI version mismatch")
+    lib.eemd_sp_fft_workspace.argtypes = [c_int32, c_int64, ctypes.POINTER(c_size_t)]
+    lib.eemd_sp_fft.argtypes = [c_void_p, c_void_p, c_int32, c_int64, c_int32, c_void_p, c_size_t, c_void_p]
     lib.eemd_sp_hilbert_workspace.argtypes = [c_int32, c_int64, ctypes.POINTER(c_size_t)]
     lib.eemd_sp_hilbert_if.argtypes = [c_void_p, c_int32, c_int64, c_double, c_void_p, c_void_p, c_void_p, c_size_t,
                                        c_void_p]
@@ -86,3 +88,19 @@ def stft_workspace(M, N, nperseg, noverlap) -> int:
 def stft(x, M, N, nperseg, noverlap, Z, ws):
     _check(load().eemd_sp_stft(c_void_p(x.data_ptr()), M, N, nperseg, noverlap, c_void_p(Z.data_ptr()),
                                c_void_p(ws.data_ptr()), ws.numel(), _stream()), "eemd_sp_stft")
+
+
+def fft_device(z, sign=-1):
+    """FFT of every row of a complex128 CUDA tensor [M, N] (sign -1: numpy.fft.fft;
+    +1: the unnormalised inverse), through eemd_sp_fft; returns a new tensor."""
+    import torch
+    lib = load()
+    z = z.contiguous()
+    M, N = int(z.shape[0]), int(z.shape[1])
+    nb = c_size_t(0)
+    _check(lib.eemd_sp_fft_workspace(M, N, ctypes.byref(nb)), "eemd_sp_fft_workspace")
+    ws = torch.empty((max(int(nb.value), 1),), dtype=torch.uint8, device=z.device)
+    out = torch.empty_like(z)
+    _check(lib.eemd_sp_fft(z.data_ptr(), out.data_ptr(), M, N, int(sign), ws.data_ptr(), int(nb.value), _stream()),
+           "eemd_sp_fft")
+    return out

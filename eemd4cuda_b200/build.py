@@ -11,7 +11,7 @@ Outputs (git-ignored, shipped next to the sources):
         kernel sums clock64() cycles per phase into the workspace header
         (eemd4cuda_b200.trace reads them)
     eemd4cuda_b200/lib/libeemd_surrogate.so     the learned surrogate's kernels
-    eemd4cuda_b200/lib/libeemd_spectra.so       Hilbert IF / STFT of the IMFs (links cuFFT)
+    eemd4cuda_b200/lib/libeemd_spectra.so       Hilbert IF / STFT of the IMFs (its own FFT)
     eemd4cuda_b200/lib/libeemd_flac.so          FLAC decoder (host C, gcc)
 """
 from __future__ import annotations
@@ -74,16 +74,14 @@ def build(force: bool = False, verbose: bool = False) -> list[Path]:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
         os.replace(tmp, out)
-    # the spectra stage (cuFFT, found through the toolkit's library directory)
+    # the spectra stage (its own FFT; no FFT library)
     out = LIB / "libeemd_spectra.so"
     outs.append(out)
     sp_deps = [CSRC / s for s in SP_SOURCES] + [INCLUDE / "eemd_spectra.h"]
     if force or _stale(out, sp_deps):
         tmp = out.with_suffix(".so.tmp")
-        libdir = _cuda_lib_dir()
         cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-               "-I", str(INCLUDE), "-o", str(tmp), *[str(CSRC / s) for s in SP_SOURCES],
-               "-L", libdir, "-lcufft", "-Xlinker", "-rpath", "-Xlinker", libdir]
+               "-I", str(INCLUDE), "-o", str(tmp), *[str(CSRC / s) for s in SP_SOURCES]]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

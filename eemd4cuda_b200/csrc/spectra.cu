@@ -1,23 +1,21 @@
 // spectra.cu -- the IMF spectra stage on the device (sm_100a): Hilbert
 // instantaneous frequency / amplitude and the STFT of batched float64 rows.
 //
-// Hilbert:  x -> (copy) -> cuFFT D2Z -> k_analytic (one-sided spectrum to the
-//           full analytic spectrum, weights 1 / 2 / 0, 1/N) -> cuFFT Z2Z
-//           inverse in place -> k_if_amp (phase differences wrapped as
+// Hilbert:  x -> k_promote (complex rows) -> FFT -> k_analytic (weights
+//           1 / 2 / 0 on DC (and Nyquist) / positive / negative frequencies,
+//           1/N) -> inverse FFT -> k_if_amp (phase differences wrapped as
 //           np.unwrap does, centred differences as np.gradient does, |z|).
 //           The frequency needs only neighbouring phase differences, so no
 //           scan over the unwrapped phase is formed.
 // STFT:     x -> k_frames (zero-extended by nperseg/2 at both ends, periodic
-//           Hann window) -> cuFFT D2Z batched over rows x frames ->
-//           k_stft_out (transpose to [F][T], divide by the window sum).
-// The FFTs are library calls; everything between them is one pass per step.
+//           Hann window, complex rows) -> FFT batched over rows x frames ->
+//           k_stft_out (one-sided half, transposed to [F][T], divided by the
+//           window sum).
+// The FFTs are this file's own (below): no FFT library is linked.
 #include <cuda_runtime.h>
-#include <cufft.h>
 #include <stdint.h>
 
-#include <map>
-#include <mutex>
-#include <tuple>
+#include <vector>
 
 #include "../../include/eemd_spectra.h"
 
@@ -25,16 +23,14 @@ namespace sp {
 
 constexpr double PI = 3.141592653589793238462643383279502884;
 
-// full analytic spectrum from the one-sided one: z[k] = w_k X[k] / N with
-// w = 1 at DC (and at N/2 for even N), 2 on 1 <= k < N/2 (k < (N+1)/2 for
-// odd N), 0 above
-__global__ void k_analytic(const double2* __restrict__ half, double2* full, int M, int64_t N) {
-    const int64_t H = N / 2 + 1;
+// analytic spectrum from the full one: z[k] = w_k X[k] / N with w = 1 at DC
+// (and at N/2 for even N), 2 on 1 <= k < N/2 (k < (N+1)/2 for odd N), 0 above
+__global__ void k_analytic(const double2* __restrict__ spec, double2* out, int M, int64_t N) {
     const int64_t total = (int64_t)M * N;
     const double inv = 1.0 / (double)N;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t m = i / N, k = i % N;
+        const int64_t k = i % N;
         double w;
         if (k == 0) w = 1.0;
         else if ((N & 1) == 0 && k == N / 2) w = 1.0;
@@ -42,11 +38,18 @@ __global__ void k_analytic(const double2* __restrict__ half, double2* full, int 
         else w = 0.0;
         double2 z = make_double2(0.0, 0.0);
         if (w != 0.0) {
-            const double2 X = half[m * H + k];
+            const double2 X = spec[i];
             z = make_double2(X.x * w * inv, X.y * w * inv);
         }
-        full[i] = z;
+        out[i] = z;
     }
+}
+
+// complex rows from real ones
+__global__ void k_promote(const double* __restrict__ x, double2* z, int64_t total) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x)
+        z[i] = make_double2(x[i], 0.0);
 }
 
 // the unwrapped difference of two wrapped phases (np.unwrap, period 2 pi,
@@ -86,8 +89,8 @@ __global__ void k_if_amp(const double2* __restrict__ z, double* inst_freq, doubl
     }
 }
 
-// frames[m][j][n] = w[n] * x[m][j*step + n - half] (zero outside the row)
-__global__ void k_frames(const double* __restrict__ x, double* frames, int M, int64_t N, int nperseg, int step,
+// frames[m][j][n] = w[n] * x[m][j*step + n - half] (zero outside the row), complex
+__global__ void k_frames(const double* __restrict__ x, double2* frames, int M, int64_t N, int nperseg, int step,
                          int T) {
     const int half = nperseg / 2;
     const int64_t total = (int64_t)M * T * nperseg;
@@ -99,12 +102,13 @@ __global__ void k_frames(const double* __restrict__ x, double* frames, int M, in
         const int64_t m = mj / T;
         const int64_t s = (int64_t)j * step + n - half;
         const double w = 0.5 - 0.5 * cos(2.0 * PI * (double)n / (double)nperseg);
-        frames[i] = (s >= 0 && s < N) ? x[m * N + s] * w : 0.0;
+        frames[i] = make_double2((s >= 0 && s < N) ? x[m * N + s] * w : 0.0, 0.0);
     }
 }
 
-// Z[m][f][t] = spec[m][t][f] / wsum
-__global__ void k_stft_out(const double2* __restrict__ spec, double2* Z, int M, int F, int T, double inv_wsum) {
+// Z[m][f][t] = spec[m][t][f] / wsum (f < F of each frame's nperseg bins)
+__global__ void k_stft_out(const double2* __restrict__ spec, double2* Z, int M, int F, int T, int nperseg,
+                           double inv_wsum) {
     const int64_t total = (int64_t)M * F * T;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -112,60 +116,9 @@ __global__ void k_stft_out(const double2* __restrict__ spec, double2* Z, int M, 
         const int64_t mf = i / T;
         const int f = (int)(mf % F);
         const int64_t m = mf / F;
-        const double2 v = spec[(m * T + t) * F + f];
+        const double2 v = spec[(m * T + t) * nperseg + f];
         Z[i] = make_double2(v.x * inv_wsum, v.y * inv_wsum);
     }
-}
-
-// ---------------------------------------------------------------------------
-// cuFFT plans, cached per (device, type, n, batch); no automatic work area
-// ---------------------------------------------------------------------------
-struct Plan {
-    cufftHandle h = 0;
-    size_t work = 0;
-};
-
-std::mutex g_mu;
-std::map<std::tuple<int, int, long long, long long>, Plan> g_plans;
-
-int get_plan(cufftType type, long long n, long long batch, Plan& out) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return EEMD_SP_E_CUDA;
-    const auto key = std::make_tuple(dev, (int)type, n, batch);
-    std::lock_guard<std::mutex> lk(g_mu);
-    auto it = g_plans.find(key);
-    if (it != g_plans.end()) {
-        out = it->second;
-        return EEMD_SP_OK;
-    }
-    Plan p;
-    if (cufftCreate(&p.h) != CUFFT_SUCCESS) return EEMD_SP_E_CUFFT;
-    if (cufftSetAutoAllocation(p.h, 0) != CUFFT_SUCCESS) {
-        cufftDestroy(p.h);
-        return EEMD_SP_E_CUFFT;
-    }
-    long long nn = n;
-    if (cufftMakePlanMany64(p.h, 1, &nn, nullptr, 1, 0, nullptr, 1, 0, type, batch, &p.work) != CUFFT_SUCCESS) {
-        cufftDestroy(p.h);
-        return EEMD_SP_E_CUFFT;
-    }
-    g_plans[key] = p;
-    out = p;
-    return EEMD_SP_OK;
-}
-
-// runs one transform with the plan's work area at `work` (under the cache lock:
-// the stream and the work area are plan state)
-int exec_plan(const Plan& p, cufftType type, void* in, void* out, int dir, void* work, cudaStream_t st) {
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (cufftSetStream(p.h, st) != CUFFT_SUCCESS) return EEMD_SP_E_CUFFT;
-    if (cufftSetWorkArea(p.h, work) != CUFFT_SUCCESS) return EEMD_SP_E_CUFFT;
-    cufftResult r;
-    if (type == CUFFT_D2Z)
-        r = cufftExecD2Z(p.h, static_cast<cufftDoubleReal*>(in), static_cast<cufftDoubleComplex*>(out));
-    else
-        r = cufftExecZ2Z(p.h, static_cast<cufftDoubleComplex*>(in), static_cast<cufftDoubleComplex*>(out), dir);
-    return r == CUFFT_SUCCESS ? EEMD_SP_OK : EEMD_SP_E_CUFFT;
 }
 
 size_t al(size_t b) { return (b + 255) / 256 * 256; }
@@ -175,30 +128,285 @@ unsigned grid_for(int64_t total) {
     return (unsigned)(b < 148 * 32 ? (b > 0 ? b : 1) : 148 * 32);
 }
 
-struct HilbertLayout {
-    size_t copy, half, full, work, total;
-    Plan fwd, inv;
+// ---------------------------------------------------------------------------
+// Complex FFT of batched rows, this library's own (no FFT library):
+// Stockham autosort passes of radix 4, 2, 3, 5 and of the odd primes up to 31
+// (the formulation of Govindaraju et al., "High performance discrete Fourier
+// transforms on graphics processors", SC'08: pass s reads x[j + q N/R],
+// multiplies by the twiddle w^(q k) of the current sub-transform length
+// Ns R (k = j mod Ns), takes a radix-R DFT and writes the results sorted, so
+// no bit reversal is needed); a length with a prime factor above 31 goes
+// through Bluestein's chirp-z identity, n k = (n^2 + k^2 - (k-n)^2) / 2, as a
+// circular convolution of power-of-two length.  Unnormalised; sign -1 is the
+// forward transform X[k] = sum_n x[n] exp(-2 pi i n k / N) (numpy's and
+// scipy's), +1 the inverse.  Twiddles and chirps are formed on the fly with
+// sincospi of an exactly reduced argument.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+// i * sign * z
+__device__ __forceinline__ double2 cisg(double2 z, int sign) {
+    return sign < 0 ? make_double2(z.y, -z.x) : make_double2(-z.y, z.x);
+}
+// exp(sign 2 pi i num / den), num reduced exactly into [0, den)
+__device__ __forceinline__ double2 twiddle(int64_t num, int64_t den, int sign) {
+    int64_t r = num % den;
+    if (r < 0) r += den;
+    double s, c;
+    sincospi(2.0 * ((double)r / (double)den), &s, &c);
+    return make_double2(c, sign < 0 ? -s : s);
+}
+
+template <int R>
+__device__ __forceinline__ void dft_small(double2 (&a)[R], int sign) {
+    if constexpr (R == 2) {
+        const double2 t = a[1];
+        a[1] = csub(a[0], t);
+        a[0] = cadd(a[0], t);
+    } else if constexpr (R == 3) {
+        // w = exp(sign 2 pi i / 3) = -1/2 + sign i sqrt(3)/2
+        const double h = 0.86602540378443864676;  // sqrt(3) / 2
+        const double2 t1 = cadd(a[1], a[2]), t2 = csub(a[1], a[2]);
+        const double2 m = make_double2(fma(-0.5, t1.x, a[0].x), fma(-0.5, t1.y, a[0].y));
+        const double2 r = cisg(make_double2(h * t2.x, h * t2.y), sign);
+        a[0] = cadd(a[0], t1);
+        a[1] = cadd(m, r);
+        a[2] = csub(m, r);
+    } else if constexpr (R == 4) {
+        const double2 t0 = cadd(a[0], a[2]), t1 = csub(a[0], a[2]);
+        const double2 t2 = cadd(a[1], a[3]), t3 = cisg(csub(a[1], a[3]), sign);
+        a[0] = cadd(t0, t2);
+        a[2] = csub(t0, t2);
+        a[1] = cadd(t1, t3);
+        a[3] = csub(t1, t3);
+    } else if constexpr (R == 5) {
+        // cos and sin of 2 pi / 5 and 4 pi / 5 from their closed forms
+        const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
+        const double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;
+        const double2 t1 = cadd(a[1], a[4]), t2 = cadd(a[2], a[3]);
+        const double2 t3 = csub(a[1], a[4]), t4 = csub(a[2], a[3]);
+        const double2 m1 = make_double2(a[0].x + c1 * t1.x + c2 * t2.x, a[0].y + c1 * t1.y + c2 * t2.y);
+        const double2 m2 = make_double2(a[0].x + c2 * t1.x + c1 * t2.x, a[0].y + c2 * t1.y + c1 * t2.y);
+        const double2 r1 = cisg(make_double2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y), sign);
+        const double2 r2 = cisg(make_double2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y), sign);
+        a[0] = cadd(a[0], cadd(t1, t2));
+        a[1] = cadd(m1, r1);
+        a[4] = csub(m1, r1);
+        a[2] = cadd(m2, r2);
+        a[3] = csub(m2, r2);
+    }
+}
+
+// one Stockham pass of radix R over M rows of N: in -> out (distinct buffers)
+template <int R>
+__global__ void k_fft_pass(const double2* __restrict__ in, double2* __restrict__ out, int M, int64_t N, int64_t Ns,
+                           int sign) {
+    const int64_t nb = N / R;
+    const int64_t total = (int64_t)M * nb;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t m = i / nb, j = i % nb;
+        const double2* x = in + m * N;
+        double2* y = out + m * N;
+        const int64_t k = j % Ns;
+        double2 a[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) a[q] = x[j + q * nb];
+        if (Ns > 1) {
+#pragma unroll
+            for (int q = 1; q < R; ++q) a[q] = cmul(a[q], twiddle((int64_t)q * k, Ns * R, sign));
+        }
+        dft_small<R>(a, sign);
+        const int64_t base = (j / Ns) * Ns * R + k;
+#pragma unroll
+        for (int q = 0; q < R; ++q) y[base + q * Ns] = a[q];
+    }
+}
+
+// the same pass for an odd prime radix r <= 31 (a direct DFT of the r points)
+__global__ void k_fft_pass_prime(const double2* __restrict__ in, double2* __restrict__ out, int M, int64_t N,
+                                 int64_t Ns, int r, int sign) {
+    const int64_t nb = N / r;
+    const int64_t total = (int64_t)M * nb;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t m = i / nb, j = i % nb;
+        const double2* x = in + m * N;
+        double2* y = out + m * N;
+        const int64_t k = j % Ns;
+        double2 a[31];
+        for (int q = 0; q < r; ++q) {
+            a[q] = x[j + q * nb];
+            if (q > 0 && Ns > 1) a[q] = cmul(a[q], twiddle((int64_t)q * k, Ns * r, sign));
+        }
+        const int64_t base = (j / Ns) * Ns * r + k;
+        for (int q = 0; q < r; ++q) {
+            double2 s = a[0];
+            for (int p = 1; p < r; ++p) s = cadd(s, cmul(a[p], twiddle((int64_t)p * q, r, sign)));
+            y[base + q * Ns] = s;
+        }
+    }
+}
+
+// Bluestein: chirp c_n = exp(sign pi i n^2 / N) (n^2 reduced mod 2N exactly)
+__device__ __forceinline__ double2 chirp(int64_t n, int64_t N, int sign) {
+    const int64_t r = (int64_t)(((unsigned long long)n * (unsigned long long)n) % (unsigned long long)(2 * N));
+    double s, c;
+    sincospi((double)r / (double)N, &s, &c);
+    return make_double2(c, sign < 0 ? -s : s);
+}
+
+// a[m][n] = x[m][n] c_n for n < N, 0 up to L
+__global__ void k_blue_pre(const double2* __restrict__ x, double2* a, int M, int64_t N, int64_t L, int sign) {
+    const int64_t total = (int64_t)M * L;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t m = i / L, n = i % L;
+        a[i] = n < N ? cmul(x[m * N + n], chirp(n, N, sign)) : make_double2(0.0, 0.0);
+    }
+}
+
+// b[n] = conj(c_n) for n < N, b[L-n] = conj(c_n) for 0 < n < N, 0 elsewhere
+__global__ void k_blue_kernel(double2* b, int64_t N, int64_t L, int sign) {
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < L; n += (int64_t)gridDim.x * blockDim.x) {
+        double2 v = make_double2(0.0, 0.0);
+        if (n < N) v = chirp(n, N, -sign);
+        else if (L - n < N) v = chirp(L - n, N, -sign);
+        b[n] = v;
+    }
+}
+
+// A[m][n] *= B[n] / L
+__global__ void k_blue_mul(double2* A, const double2* __restrict__ B, int M, int64_t L) {
+    const int64_t total = (int64_t)M * L;
+    const double inv = 1.0 / (double)L;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 v = cmul(A[i], B[i % L]);
+        A[i] = make_double2(v.x * inv, v.y * inv);
+    }
+}
+
+// y[m][k] = c_k C[m][k] for k < N
+__global__ void k_blue_post(const double2* __restrict__ Cv, double2* y, int M, int64_t N, int64_t L, int sign) {
+    const int64_t total = (int64_t)M * N;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t m = i / N, k = i % N;
+        y[i] = cmul(Cv[m * L + k], chirp(k, N, sign));
+    }
+}
+
+struct FftPlan {
+    int64_t n = 0, L = 0;        // length; Bluestein's power-of-two length (0 = direct)
+    std::vector<int> radices;    // of n (direct) or of L (Bluestein)
 };
 
-int hilbert_layout(int M, int64_t N, HilbertLayout& L) {
-    if (M < 1 || N < 2) return EEMD_SP_E_BADARG;
-    int rc = get_plan(CUFFT_D2Z, N, M, L.fwd);
-    if (rc) return rc;
-    rc = get_plan(CUFFT_Z2Z, N, M, L.inv);
-    if (rc) return rc;
-    L.copy = al((size_t)M * N * sizeof(double));
-    L.half = al((size_t)M * (N / 2 + 1) * sizeof(double2));
-    L.full = al((size_t)M * N * sizeof(double2));
-    L.work = al(L.fwd.work > L.inv.work ? L.fwd.work : L.inv.work);
-    L.total = L.copy + L.half + L.full + L.work;
+bool factor(int64_t n, std::vector<int>& rad) {
+    rad.clear();
+    while (n % 4 == 0) { rad.push_back(4); n /= 4; }
+    while (n % 2 == 0) { rad.push_back(2); n /= 2; }
+    for (int p = 3; p <= 31; p += 2) {
+        while (n % p == 0) { rad.push_back(p); n /= p; }
+    }
+    return n == 1;
+}
+
+FftPlan make_fft_plan(int64_t n) {
+    FftPlan P;
+    P.n = n;
+    if (!factor(n, P.radices)) {
+        int64_t L = 1;
+        while (L < 2 * n - 1) L <<= 1;
+        P.L = L;
+        factor(L, P.radices);
+    }
+    return P;
+}
+
+// complex elements of scratch an FFT of M rows needs beyond its two ping-pong buffers
+int64_t fft_extra(const FftPlan& P, int M) { return P.L ? 2 * (int64_t)M * P.L + 2 * P.L : 0; }
+
+// Stockham passes of length len over M rows: src -> (b1, b2 alternately); returns the result buffer
+double2* stockham(const double2* src, double2* b1, double2* b2, int M, int64_t len, const std::vector<int>& rad,
+                  int sign, cudaStream_t st) {
+    const double2* cur = src;
+    double2* dst = b1;
+    int64_t Ns = 1;
+    if (rad.empty()) {  // length 1: the transform is the identity
+        cudaMemcpyAsync(b1, src, sizeof(double2) * (size_t)M * (size_t)len, cudaMemcpyDeviceToDevice, st);
+        return b1;
+    }
+    for (int r : rad) {
+        const unsigned g = grid_for((int64_t)M * (len / r));
+        switch (r) {
+            case 2: k_fft_pass<2><<<g, 256, 0, st>>>(cur, dst, M, len, Ns, sign); break;
+            case 3: k_fft_pass<3><<<g, 256, 0, st>>>(cur, dst, M, len, Ns, sign); break;
+            case 4: k_fft_pass<4><<<g, 256, 0, st>>>(cur, dst, M, len, Ns, sign); break;
+            case 5: k_fft_pass<5><<<g, 256, 0, st>>>(cur, dst, M, len, Ns, sign); break;
+            default: k_fft_pass_prime<<<g, 256, 0, st>>>(cur, dst, M, len, Ns, r, sign); break;
+        }
+        Ns *= r;
+        cur = dst;
+        dst = (dst == b1) ? b2 : b1;
+    }
+    return const_cast<double2*>(cur);
+}
+
+// FFT of M rows of length P.n: `in` is read only; b1, b2 hold M*n each and
+// `extra` fft_extra(P, M) elements; returns the buffer (b1 or b2) with the result
+double2* fft_rows(const double2* in, double2* b1, double2* b2, double2* extra, int M, const FftPlan& P, int sign,
+                  cudaStream_t st) {
+    if (!P.L) return stockham(in, b1, b2, M, P.n, P.radices, sign, st);
+    const int64_t N = P.n, L = P.L;
+    double2* A = extra;                 // M * L
+    double2* T = extra + (int64_t)M * L;  // M * L
+    double2* Bk = T + (int64_t)M * L;   // L
+    double2* Bt = Bk + L;               // L
+    k_blue_pre<<<grid_for((int64_t)M * L), 256, 0, st>>>(in, A, M, N, L, sign);
+    k_blue_kernel<<<grid_for(L), 256, 0, st>>>(Bk, N, L, sign);
+    double2* Af = stockham(A, T, A, M, L, P.radices, -1, st);
+    double2* Bf = stockham(Bk, Bt, Bk, 1, L, P.radices, -1, st);
+    k_blue_mul<<<grid_for((int64_t)M * L), 256, 0, st>>>(Af, Bf, M, L);
+    double2* other = (Af == A) ? T : A;
+    double2* Cv = stockham(Af, other, Af, M, L, P.radices, +1, st);
+    k_blue_post<<<grid_for((int64_t)M * N), 256, 0, st>>>(Cv, b1, M, N, L, sign);
+    return b1;
+}
+
+// three complex buffers of `rows` x `len` plus the FFT's extra scratch
+struct FftLayout {
+    FftPlan P;
+    int64_t rows = 0;
+    size_t buf = 0, extra = 0, total = 0;
+};
+
+int fft_layout(int64_t rows, int64_t len, FftLayout& L) {
+    if (rows < 1 || len < 1 || rows > (1LL << 31)) return EEMD_SP_E_BADARG;
+    L.P = make_fft_plan(len);
+    L.rows = rows;
+    L.buf = al((size_t)rows * (size_t)len * sizeof(double2));
+    L.extra = al((size_t)fft_extra(L.P, (int)rows) * sizeof(double2));
+    L.total = 3 * L.buf + L.extra;
     return EEMD_SP_OK;
 }
 
-struct StftLayout {
-    int F, T, step;
-    size_t frames, spec, work, total;
-    Plan fwd;
+struct Bufs {
+    double2 *x, *y, *z, *extra;
 };
+
+Bufs carve(void* ws, const FftLayout& L) {
+    char* base = static_cast<char*>(ws);
+    Bufs b;
+    b.x = reinterpret_cast<double2*>(base);
+    b.y = reinterpret_cast<double2*>(base + L.buf);
+    b.z = reinterpret_cast<double2*>(base + 2 * L.buf);
+    b.extra = reinterpret_cast<double2*>(base + 3 * L.buf);
+    return b;
+}
 
 int stft_shape(int64_t N, int nperseg, int noverlap, int& F, int& T) {
     if (N < 1 || nperseg < 2 || noverlap < 0 || noverlap >= nperseg) return EEMD_SP_E_BADARG;
@@ -211,20 +419,6 @@ int stft_shape(int64_t N, int nperseg, int noverlap, int& F, int& T) {
     return EEMD_SP_OK;
 }
 
-int stft_layout(int M, int64_t N, int nperseg, int noverlap, StftLayout& L) {
-    if (M < 1) return EEMD_SP_E_BADARG;
-    int rc = stft_shape(N, nperseg, noverlap, L.F, L.T);
-    if (rc) return rc;
-    L.step = nperseg - noverlap;
-    rc = get_plan(CUFFT_D2Z, nperseg, (long long)M * L.T, L.fwd);
-    if (rc) return rc;
-    L.frames = al((size_t)M * L.T * nperseg * sizeof(double));
-    L.spec = al((size_t)M * L.T * L.F * sizeof(double2));
-    L.work = al(L.fwd.work);
-    L.total = L.frames + L.spec + L.work;
-    return EEMD_SP_OK;
-}
-
 }  // namespace sp
 
 using namespace sp;
@@ -233,38 +427,52 @@ extern "C" {
 
 int32_t eemd_sp_version(void) { return EEMD_SP_ABI_VERSION; }
 
-int32_t eemd_sp_hilbert_workspace(int32_t M, int64_t N, size_t* bytes) {
+int32_t eemd_sp_fft_workspace(int32_t M, int64_t N, size_t* bytes) {
     if (!bytes) return EEMD_SP_E_BADARG;
-    HilbertLayout L;
-    const int rc = hilbert_layout(M, N, L);
+    FftLayout L;
+    const int rc = fft_layout(M, N, L);
     if (rc) return rc;
     *bytes = L.total;
     return EEMD_SP_OK;
 }
 
-int32_t eemd_sp_hilbert_if(const double* x, int32_t M, int64_t N, double sr, double* inst_freq, double* inst_amp,
-                           void* ws, size_t ws_bytes, void* stream) {
-    if (!x || !inst_freq || !inst_amp || !ws || !(sr > 0.0)) return EEMD_SP_E_BADARG;
-    HilbertLayout L;
-    int rc = hilbert_layout(M, N, L);
+int32_t eemd_sp_fft(const double* in, double* out, int32_t M, int64_t N, int32_t sign, void* ws, size_t ws_bytes,
+                    void* stream) {
+    if (!in || !out || !ws || (sign != -1 && sign != 1)) return EEMD_SP_E_BADARG;
+    FftLayout L;
+    int rc = fft_layout(M, N, L);
     if (rc) return rc;
     if (ws_bytes < L.total) return EEMD_SP_E_NOMEM;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    char* base = static_cast<char*>(ws);
-    double* copy = reinterpret_cast<double*>(base);
-    double2* half = reinterpret_cast<double2*>(base + L.copy);
-    double2* full = reinterpret_cast<double2*>(base + L.copy + L.half);
-    void* work = base + L.copy + L.half + L.full;
-    // the transform's input is a scratch copy: the caller's rows stay untouched
-    if (cudaMemcpyAsync(copy, x, (size_t)M * N * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-        return EEMD_SP_E_CUDA;
-    rc = exec_plan(L.fwd, CUFFT_D2Z, copy, half, 0, work, st);
+    const Bufs b = carve(ws, L);
+    const size_t nb = sizeof(double2) * (size_t)M * (size_t)N;
+    if (cudaMemcpyAsync(b.x, in, nb, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return EEMD_SP_E_CUDA;
+    double2* r = fft_rows(b.x, b.y, b.z, b.extra, M, L.P, sign, st);
+    if (cudaMemcpyAsync(out, r, nb, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return EEMD_SP_E_CUDA;
+    return cudaGetLastError() == cudaSuccess ? EEMD_SP_OK : EEMD_SP_E_CUDA;
+}
+
+int32_t eemd_sp_hilbert_workspace(int32_t M, int64_t N, size_t* bytes) {
+    if (!bytes || N < 2) return EEMD_SP_E_BADARG;
+    return eemd_sp_fft_workspace(M, N, bytes);
+}
+
+int32_t eemd_sp_hilbert_if(const double* x, int32_t M, int64_t N, double sr, double* inst_freq, double* inst_amp,
+                           void* ws, size_t ws_bytes, void* stream) {
+    if (!x || !inst_freq || !inst_amp || !ws || !(sr > 0.0) || N < 2) return EEMD_SP_E_BADARG;
+    FftLayout L;
+    int rc = fft_layout(M, N, L);
     if (rc) return rc;
-    k_analytic<<<grid_for((int64_t)M * N), 256, 0, st>>>(half, full, M, N);
-    if (cudaGetLastError() != cudaSuccess) return EEMD_SP_E_CUDA;
-    rc = exec_plan(L.inv, CUFFT_Z2Z, full, full, CUFFT_INVERSE, work, st);
-    if (rc) return rc;
-    k_if_amp<<<grid_for((int64_t)M * N), 256, 0, st>>>(full, inst_freq, inst_amp, M, N, sr);
+    if (ws_bytes < L.total) return EEMD_SP_E_NOMEM;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const Bufs b = carve(ws, L);
+    const int64_t total = (int64_t)M * N;
+    // the caller's rows stay untouched: the transform runs on complex copies
+    k_promote<<<grid_for(total), 256, 0, st>>>(x, b.x, total);
+    double2* spec = fft_rows(b.x, b.y, b.z, b.extra, M, L.P, -1, st);
+    k_analytic<<<grid_for(total), 256, 0, st>>>(spec, b.x, M, N);
+    double2* z = fft_rows(b.x, b.y, b.z, b.extra, M, L.P, +1, st);
+    k_if_amp<<<grid_for(total), 256, 0, st>>>(z, inst_freq, inst_amp, M, N, sr);
     return cudaGetLastError() == cudaSuccess ? EEMD_SP_OK : EEMD_SP_E_CUDA;
 }
 
@@ -279,9 +487,12 @@ int32_t eemd_sp_stft_shape(int64_t N, int32_t nperseg, int32_t noverlap, int32_t
 }
 
 int32_t eemd_sp_stft_workspace(int32_t M, int64_t N, int32_t nperseg, int32_t noverlap, size_t* bytes) {
-    if (!bytes) return EEMD_SP_E_BADARG;
-    StftLayout L;
-    const int rc = stft_layout(M, N, nperseg, noverlap, L);
+    if (!bytes || M < 1) return EEMD_SP_E_BADARG;
+    int F = 0, T = 0;
+    int rc = stft_shape(N, nperseg, noverlap, F, T);
+    if (rc) return rc;
+    FftLayout L;
+    rc = fft_layout((int64_t)M * T, nperseg, L);
     if (rc) return rc;
     *bytes = L.total;
     return EEMD_SP_OK;
@@ -289,25 +500,23 @@ int32_t eemd_sp_stft_workspace(int32_t M, int64_t N, int32_t nperseg, int32_t no
 
 int32_t eemd_sp_stft(const double* x, int32_t M, int64_t N, int32_t nperseg, int32_t noverlap, double* Z, void* ws,
                      size_t ws_bytes, void* stream) {
-    if (!x || !Z || !ws) return EEMD_SP_E_BADARG;
-    StftLayout L;
-    int rc = stft_layout(M, N, nperseg, noverlap, L);
+    if (!x || !Z || !ws || M < 1) return EEMD_SP_E_BADARG;
+    int F = 0, T = 0;
+    int rc = stft_shape(N, nperseg, noverlap, F, T);
+    if (rc) return rc;
+    FftLayout L;
+    rc = fft_layout((int64_t)M * T, nperseg, L);
     if (rc) return rc;
     if (ws_bytes < L.total) return EEMD_SP_E_NOMEM;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    char* base = static_cast<char*>(ws);
-    double* frames = reinterpret_cast<double*>(base);
-    double2* spec = reinterpret_cast<double2*>(base + L.frames);
-    void* work = base + L.frames + L.spec;
+    const Bufs b = carve(ws, L);
     // the window's sum, added in index order (as the reference's window sum is formed)
     double wsum = 0.0;
     for (int n = 0; n < nperseg; ++n) wsum += 0.5 - 0.5 * cos(2.0 * PI * (double)n / (double)nperseg);
-    k_frames<<<grid_for((int64_t)M * L.T * nperseg), 256, 0, st>>>(x, frames, M, N, nperseg, L.step, L.T);
-    if (cudaGetLastError() != cudaSuccess) return EEMD_SP_E_CUDA;
-    rc = exec_plan(L.fwd, CUFFT_D2Z, frames, spec, 0, work, st);
-    if (rc) return rc;
-    k_stft_out<<<grid_for((int64_t)M * L.F * L.T), 256, 0, st>>>(spec, reinterpret_cast<double2*>(Z), M, L.F, L.T,
-                                                                  1.0 / wsum);
+    k_frames<<<grid_for((int64_t)M * T * nperseg), 256, 0, st>>>(x, b.x, M, N, nperseg, nperseg - noverlap, T);
+    double2* spec = fft_rows(b.x, b.y, b.z, b.extra, M * T, L.P, -1, st);
+    k_stft_out<<<grid_for((int64_t)M * F * T), 256, 0, st>>>(spec, reinterpret_cast<double2*>(Z), M, F, T, nperseg,
+                                                             1.0 / wsum);
     return cudaGetLastError() == cudaSuccess ? EEMD_SP_OK : EEMD_SP_E_CUDA;
 }
 

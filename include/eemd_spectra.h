@@ -11,13 +11,16 @@
  *   eemd_sp_stft        replaces spectra.py:18-29 stft_block:
  *       scipy.signal.stft(window='hann', boundary='zeros', padded=False),
  *       one-sided, divided by the window's sum.
+ *   eemd_sp_fft         the complex FFT both use (numpy.fft.fft's convention
+ *       for sign -1, unnormalised), this library's own: Stockham passes of
+ *       radix 4, 2, 3, 5 and odd primes up to 31, Bluestein's chirp-z for a
+ *       length with a larger prime factor.
  *
  * Rows are batched: M signals of N samples each, float64, row-major.  All
  * pointers are device pointers owned by the caller, including the workspace
- * (size from the *_workspace queries).  The FFTs are cuFFT plans that the
- * library creates once per (device, shape) and caches; their work area is
- * taken from the caller's workspace.  Calls are asynchronous on `stream`;
- * calls that share a workspace must not overlap.
+ * (size from the *_workspace queries); the library allocates no memory and
+ * keeps no state.  Calls are asynchronous on `stream`; calls that share a
+ * workspace must not overlap.
  */
 #ifndef EEMD_SPECTRA_H
 #define EEMD_SPECTRA_H
@@ -35,9 +38,16 @@ extern "C" {
 #define EEMD_SP_E_BADARG -1
 #define EEMD_SP_E_NOMEM -2   /* the workspace is smaller than the query returned */
 #define EEMD_SP_E_CUDA -5
-#define EEMD_SP_E_CUFFT -6   /* a cuFFT plan could not be made or executed */
 
 int32_t eemd_sp_version(void);
+
+/* Workspace bytes for eemd_sp_fft on M rows of N points. */
+int32_t eemd_sp_fft_workspace(int32_t M, int64_t N, size_t* bytes);
+
+/* out[m][k] = sum_n in[m][n] exp(sign 2 pi i n k / N) for every row (complex,
+ * interleaved re/im float64; sign -1 or +1; N >= 1; out may equal in). */
+int32_t eemd_sp_fft(const double* in, double* out, int32_t M, int64_t N, int32_t sign, void* ws, size_t ws_bytes,
+                    void* stream);
 
 /* Workspace bytes for eemd_sp_hilbert_if on M rows of N samples. */
 int32_t eemd_sp_hilbert_workspace(int32_t M, int64_t N, size_t* bytes);

@@ -75,3 +75,19 @@ def test_spectra_of_imfs_48k_against_the_oracle():
         assert np.max(np.abs(w[r] - ow)[m]) <= 1e-6 * sr
         _, _, oZ = SP.stft(X[r], sr, 4096)
         assert np.max(np.abs(Z[r] - oZ)) <= 1e-11 * np.max(np.abs(oZ))
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 5, 8, 30, 37, 100, 1001, 2048, 4097, 48000, 65536])
+def test_own_fft_against_numpy(N):
+    """eemd_sp_fft (Stockham radix 4/2/3/5/odd primes <= 31, Bluestein for
+    larger primes: 37, 4097 = 17 x 241) against numpy.fft on 3 rows, both signs."""
+    from eemd4cuda_b200 import _sp
+    rng = np.random.default_rng(N)
+    x = rng.standard_normal((3, N)) + 1j * rng.standard_normal((3, N))
+    z = torch.from_numpy(x).cuda()
+    f = _sp.fft_device(z, -1).cpu().numpy()
+    ref = np.fft.fft(x, axis=1)
+    assert np.max(np.abs(f - ref)) <= 1e-13 * max(1.0, np.max(np.abs(ref)))
+    b = _sp.fft_device(z, +1).cpu().numpy()
+    refb = np.fft.ifft(x, axis=1) * N
+    assert np.max(np.abs(b - refb)) <= 1e-13 * max(1.0, np.max(np.abs(refb)))
