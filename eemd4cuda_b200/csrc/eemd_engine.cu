@@ -997,11 +997,6 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
     const T* R0 = static_cast<const T*>(sl.M);
     const T* R1 = R0 + (int64_t)C.kcap * RS;
     const int kbase0 = S.pref[S.kpar][0][seg], kbase1 = S.pref[S.kpar][1][seg];
-    // the step's envelope constants, read from shared memory once per sweep
-    const bool both_splines = S.P[0] >= 2 && S.P[1] >= 2;
-    const int mir0 = S.mir[0], mir1 = S.mir[1];
-    const int tf0 = S.tfirst[0], tf1 = S.tfirst[1], tl0 = S.tlast[0], tl1 = S.tlast[1];
-    const int p2m0 = S.p2[0] - 1, p2m1 = S.p2[1] - 1;
     const int nt = (s1 - s0 + WT - 1) / WT;
     const int ta = wid * nt / NWARP, tb = (wid + 1) * nt / NWARP;
     const int r0 = s0 + ta * WT, r1 = min(s1, s0 + tb * WT);  // the warp's range [r0, r1)
@@ -1097,14 +1092,14 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
             }
             // interior tile: every sample's interval is (knots before it) + mir - 1, no clipping
             const int ta0 = t0 + j0, ta1 = t0 + j0 + nv - 1;
-            bool ok = both_splines;
+            bool ok = S.P[0] >= 2 && S.P[1] >= 2;
 #pragma unroll
             for (int env = 0; env < 2; ++env) {
                 const int kb = env ? kb1 : kb0;
                 const int kc = __popc(env ? kmn : kmx);
-                const int mir = env ? mir1 : mir0;
-                ok = ok && (!mir || ((env ? tf1 : tf0) < ta0 && (env ? tl1 : tl0) >= ta1));
-                ok = ok && (kb + mir >= 1) && (kb + kc + mir <= (env ? p2m1 : p2m0));
+                const int mir = S.mir[env];
+                ok = ok && (!mir || (S.tfirst[env] < ta0 && S.tlast[env] >= ta1));
+                ok = ok && (kb + mir >= 1) && (kb + kc + mir <= S.p2[env] - 1);
             }
             const bool fast = __all_sync(FULL, ok || nv == 0);
             T tnum = (T)0, tden = (T)0;  // fast mode: this tile's SD partial sums
@@ -1131,7 +1126,7 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
                 c0.t0 = c0.t1 = 0;
                 c0.y0 = c0.c1 = c0.c2 = c0.c3 = c0.y1 = c0.m1 = (T)0;
                 n0 = c1 = n1 = c0;
-                int k0 = kb0 + mir0 - 1, k1 = kb1 + mir1 - 1;
+                int k0 = kb0 + S.mir[0] - 1, k1 = kb1 + S.mir[1] - 1;
                 if (nv > 0) {
                     // the interior test above keeps every index of the run in [0, p2 - 2]
                     EEMD_CHECK_IV(k0, S.p2[0] - 2 - (int)__popc(kmx));

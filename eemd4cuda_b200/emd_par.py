@@ -195,10 +195,20 @@ def reference_noise(x: np.ndarray, E: int, eps: float, seed: int, stream: str) -
     raise ValueError("unknown noise stream %r" % (stream,))
 
 
+_TOTAL_MEM = {}
+
+
 def _auto_batch(torch, p, N, E, bytes_per_el):
-    """Trials resident at once: 70 % of free device memory (emd_par.py:214-223)."""
-    free, _ = torch.cuda.mem_get_info()
+    """Trials resident at once: 70 % of free device memory (emd_par.py:214-223).
+    The free-memory query (a driver round trip) is skipped when the whole
+    ensemble's workspace is under a tenth of the device's memory."""
     per_trial = L.workspace_size(p, [N], 1, False)
+    dev = torch.cuda.current_device()
+    if dev not in _TOTAL_MEM:
+        _TOTAL_MEM[dev] = torch.cuda.get_device_properties(dev).total_memory
+    if per_trial * E < _TOTAL_MEM[dev] // 10:
+        return E
+    free, _ = torch.cuda.mem_get_info()
     b = max(1, int(free * 0.7 // max(per_trial, 1)))
     return min(E, b)
 
