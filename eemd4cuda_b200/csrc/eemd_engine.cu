@@ -997,9 +997,13 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
     const T* R0 = static_cast<const T*>(sl.M);
     const T* R1 = R0 + (int64_t)C.kcap * RS;
     const int kbase0 = S.pref[S.kpar][0][seg], kbase1 = S.pref[S.kpar][1][seg];
-    const int nt = (s1 - s0 + WT - 1) / WT;
-    const int ta = wid * nt / NWARP, tb = (wid + 1) * nt / NWARP;
-    const int r0 = s0 + ta * WT, r1 = min(s1, s0 + tb * WT);  // the warp's range [r0, r1)
+    // the warp's range [r0, r1): an equal share of the segment in whole runs
+    // (shares in whole tiles left the last tiles' warps up to a tile behind),
+    // cut into tiles of WT samples from r0 (the last one partial)
+    const int nrun = (s1 - s0 + RUN - 1) / RUN;
+    const int r0 = min(s1, s0 + (int)((int64_t)wid * nrun / NWARP) * RUN);
+    const int r1 = min(s1, s0 + (int)((int64_t)(wid + 1) * nrun / NWARP) * RUN);
+    const int ta = 0, tb = (r1 - r0 + WT - 1) / WT;
 
     unsigned char* wb = smem + (size_t)wid * G::WARP_BYTES;
     T* const tbuf = reinterpret_cast<T*>(wb);                      // [2 buf][2 stream][TB]
@@ -1028,7 +1032,7 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
     // NBUF - 1 tiles are in flight while one is processed
     auto bufi = [&](int j) { return (j - ta) % G::NBUF; };
     auto prefetch = [&](int j) {
-        const int t0 = s0 + j * WT, t1 = min(s1, t0 + WT), bi = bufi(j);
+        const int t0 = r0 + j * WT, t1 = min(r1, t0 + WT), bi = bufi(j);
         if (needs_h) tile_copy<T>(tbuf + (bi * 2) * G::TB, io.hsrc + t0, t1 - t0, lane);
         if (USES_R) tile_copy<T>(tbuf + (bi * 2 + 1) * G::TB, io.rcur + t0, t1 - t0, lane);
         if (SIFTING && lane * RUN < t1 - t0) cp_async16(rib + bi * 32 + lane, ri_cur + t0 / RUN + lane);
@@ -1054,7 +1058,7 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
     }
 
     for (int j = ta; j < tb; ++j) {
-        const int t0 = s0 + j * WT, t1 = min(s1, t0 + WT), tl = t1 - t0;
+        const int t0 = r0 + j * WT, t1 = min(r1, t0 + WT), tl = t1 - t0;
         const int j0 = lane * RUN;
         const int nv = max(0, min(RUN, tl - j0));  // valid samples of this lane's run
         const int last_lane = (tl - 1) / RUN;
