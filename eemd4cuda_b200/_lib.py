@@ -34,7 +34,7 @@ EEMD_NOISE_PHILOX = 1
 EEMD_NOISE_INJECTED = 2
 EEMD_NOISE_PREPERTURBED = 3
 EEMD_NOISE_SCALED = 4
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 # every symbol include/eemd_b200.h declares
 EXPORTS = ("eemd_default_params", "eemd_version", "eemd_strerror",
@@ -65,6 +65,8 @@ class EemdParams(ctypes.Structure):
         ("watchdog", c_int64),
         ("cluster_size", c_int32),
         ("reserved", c_int32),
+        ("cta_warps", c_int32),
+        ("reserved2", c_int32),
     ]
 
 

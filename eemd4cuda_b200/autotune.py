@@ -1,19 +1,19 @@
-"""Threads per trial, tuned per signal-length bucket and task count.
+"""Threads per trial and block size, tuned per signal-length bucket and task count.
 
 The engine spreads one (signal, trial) task over a thread-block cluster of C
-CTAs of 128 threads (C x 128 threads per trial).  The best C depends on the
-signal length (how much work one CTA's segment holds) and on how many tasks
-share the launch (how many of the B200's 148 x 4 CTA slots each task can
-have).  `tune()` measures the persistent kernel for every (length bucket,
-task count, C) on synthetic signals of the 48 kHz benchmark kind and writes
-the fastest C per (bucket, task count) to a JSON table
-(eemd4cuda_b200/tuning/b200_<dtype>.json, committed with the package);
-`cluster_size()` looks a launch up in it, and the Python entry points
-(`emd_par.decompose`, `decompose_many`) pass the result to the engine when
-the caller leaves `EngineConfig.cluster_size` at 0.  Without a table entry
-the engine's own rule applies (eemd_engine.cu autotune_csize).  The CTA size
-(4 warps) and the fast solve's rows per lane are build-time constants,
-chosen by measurement; this table covers the launch-time choice.
+CTAs of W warps (C x W x 32 threads per trial; W = 4 or 5, four or three
+CTAs per SM).  The best (C, W) depends on the signal length (how much work
+one CTA's segment holds) and on how many tasks share the launch (how many of
+the B200's CTA slots each task can have).  `tune()` measures the persistent
+kernel for every (length bucket, task count, W, C) on synthetic signals of
+the 48 kHz benchmark kind and writes the fastest (C, W) per (bucket, task
+count) to a JSON table (eemd4cuda_b200/tuning/b200_<dtype>.json, committed
+with the package); `launch_shape()` looks a launch up in it, and the Python
+entry points (`emd_par.decompose`, `decompose_many`) pass the result to the
+engine when the caller leaves `EngineConfig.cluster_size` and `cta_warps` at
+0.  Without a table entry the engine's own rule applies (eemd_engine.cu
+autotune_csize, 4-warp CTAs).  The fast solve's rows per lane is a
+build-time constant chosen by measurement.
 
     python -m eemd4cuda_b200.autotune --dtype f32 [--quick]
 """
@@ -31,7 +31,8 @@ import numpy as np
 TABLE_DIR = Path(__file__).resolve().parent / "tuning"
 BUCKETS = (4096, 16384, 65536, 262144, 1 << 20, 1 << 22)
 TASKS = (1, 8, 32, 64, 100, 256, 1024, 4096)
-CANDIDATES = (1, 2, 3, 4, 5, 6, 8, 12, 16)
+CANDIDATES = (1, 2, 3, 4, 5, 6, 8, 12, 16)   # CTAs per task
+WARPS = (4, 5)                                # warps per CTA
 MAX_SAMPLES = 1 << 29  # tasks x length per measurement (workspace and time bound)
 
 
@@ -45,29 +46,36 @@ def _table(dtype: str):
     if not p.exists():
         return None
     d = json.loads(p.read_text())
-    return [(int(e["n"]), int(e["tasks"]), int(e["cluster_size"])) for e in d["entries"]]
+    return [(int(e["n"]), int(e["tasks"]), int(e["cluster_size"]), int(e.get("cta_warps", 4)))
+            for e in d["entries"]]
 
 
-def cluster_size(n_min: int, n_tasks: int, dtype: str) -> int:
-    """Tuned CTAs per task for a launch whose shortest signal has n_min samples
-    and which holds n_tasks tasks (nearest entry in log length, then in log
-    task count), or 0 when the table has no entry for that storage type."""
+def launch_shape(n_min: int, n_tasks: int, dtype: str) -> tuple:
+    """Tuned (CTAs per task, warps per CTA) for a launch whose shortest signal
+    has n_min samples and which holds n_tasks tasks (nearest entry in log
+    length, then in log task count), or (0, 0) when the table has no entry
+    for that storage type."""
     tab = _table(dtype)
     if not tab:
-        return 0
-    lengths = sorted({n for n, _, _ in tab})
+        return 0, 0
+    lengths = sorted({n for n, _, _, _ in tab})
     bn = min(lengths, key=lambda n: abs(math.log(n) - math.log(max(n_min, 1))))
-    rows = [(t, c) for n, t, c in tab if n == bn]
-    t, c = min(rows, key=lambda r: abs(math.log(r[0]) - math.log(max(n_tasks, 1))))
+    rows = [(t, c, w) for n, t, c, w in tab if n == bn]
+    t, c, w = min(rows, key=lambda r: abs(math.log(r[0]) - math.log(max(n_tasks, 1))))
     # a cluster needs at least 2048 samples per CTA (the engine's own bound)
     while c > 1 and n_min // c < 2048:
         c -= 1
-    return c
+    return c, w
 
 
-def _measure(n: int, tasks: int, dtype: str, c: int, reps: int) -> float:
+def cluster_size(n_min: int, n_tasks: int, dtype: str) -> int:
+    """The CTAs-per-task half of launch_shape()."""
+    return launch_shape(n_min, n_tasks, dtype)[0]
+
+
+def _measure(n: int, tasks: int, dtype: str, c: int, reps: int, nw: int = 4) -> float:
     """ms of the persistent kernel for `tasks` trials of one n-sample signal
-    (2 IMFs x 5 fixed sifts, Philox noise) with clusters of c CTAs."""
+    (2 IMFs x 5 fixed sifts, Philox noise) with clusters of c CTAs of nw warps."""
     import torch
 
     from . import _lib as L
@@ -77,7 +85,7 @@ def _measure(n: int, tasks: int, dtype: str, c: int, reps: int) -> float:
     dt = np.float32 if dtype == "f32" else np.float64
     x = signals.harmonic_clicks(n, seed=1).astype(dt)
     p = M.make_params(dtype=dt, noise_mode=L.EEMD_NOISE_PHILOX, eps=0.2, seed=1, tau=0.0, max_sifts=5,
-                      max_imf=2, config=M.EngineConfig(cluster_size=c))
+                      max_imf=2, config=M.EngineConfig(cluster_size=c, cta_warps=nw))
     dev = torch.device("cuda", torch.cuda.current_device())
     xd = torch.from_numpy(x).to(dev)
     ws = torch.empty((L.workspace_size(p, [n], tasks, False),), dtype=torch.uint8, device=dev)
@@ -101,19 +109,21 @@ def tune(dtype: str = "f32", quick: bool = False, reps: int = 2) -> dict:
             if n * tasks > MAX_SAMPLES or (dtype == "f64" and n * tasks > MAX_SAMPLES // 2):
                 continue
             times = {}
-            for c in CANDIDATES:
-                if n // c < 2048 and c > 1:
-                    continue
-                try:
-                    times[c] = _measure(n, tasks, dtype, c, reps)
-                except Exception as e:  # a cluster size the device cannot launch
-                    times[c] = None
-                    print(f"n={n} tasks={tasks} C={c}: {e}", flush=True)
-                torch.cuda.empty_cache()
-            ok = {c: t for c, t in times.items() if t is not None}
-            best = min(ok, key=ok.get)
-            entries.append({"n": n, "tasks": tasks, "cluster_size": best,
-                            "ms": {str(c): (round(t, 4) if t is not None else None) for c, t in times.items()}})
+            for nw in WARPS:
+                for c in CANDIDATES:
+                    if n // c < 2048 and c > 1:
+                        continue
+                    try:
+                        times[(nw, c)] = _measure(n, tasks, dtype, c, reps, nw)
+                    except Exception as e:  # a cluster size the device cannot launch
+                        times[(nw, c)] = None
+                        print(f"n={n} tasks={tasks} W={nw} C={c}: {e}", flush=True)
+                    torch.cuda.empty_cache()
+            ok = {k: t for k, t in times.items() if t is not None}
+            bw, bc = min(ok, key=ok.get)
+            entries.append({"n": n, "tasks": tasks, "cluster_size": bc, "cta_warps": bw,
+                            "ms": {f"{w}x{c}": (round(t, 4) if t is not None else None)
+                                   for (w, c), t in times.items()}})
             print(json.dumps(entries[-1]), flush=True)
     return {"device": torch.cuda.get_device_name(), "dtype": dtype,
             "workload": "harmonic + pink noise + clicks (48 kHz kind), Philox noise 0.2 std, 2 IMFs x 5 fixed sifts",

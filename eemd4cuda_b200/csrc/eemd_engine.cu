@@ -205,12 +205,11 @@ __global__ void __launch_bounds__(1024) k_sigma(const SignalDesc* sdesc, const v
 // ---------------------------------------------------------------------------
 // per-CTA task context (shared memory)
 // ---------------------------------------------------------------------------
-constexpr int NWARP = THREADS / 32;
-constexpr int MAXSEG = MAXC * NWARP;  // knot segments per task: one per warp of up to MAXC CTAs
+constexpr int MAXSEG = MAXC * MAXNW;  // knot segments per task: one per warp of up to MAXC CTAs
 
 struct Xchg {              // one CTA's published segment results (DSMEM-visible)
     double num, den;       // SD partial sums of the segment
-    int cnt[2][NWARP];     // new knots (maxima, minima) found by each warp
+    int cnt[2][MAXNW];     // new knots (maxima, minima) found by each warp
     int err;               // this CTA raised an error during the step: the task stops
 };
 
@@ -309,9 +308,9 @@ __host__ __device__ inline size_t wsolve_bytes(size_t bt, bool exact) {
 }
 
 // dynamic shared memory of k_emd: the sweep's and the solve's per-warp areas overlay
-__host__ __device__ inline size_t smem_bytes(int bt, bool exact) {
-    const size_t sweep = NWARP * (bt == 8 ? Geo<double>::WARP_BYTES : Geo<float>::WARP_BYTES);
-    const size_t solve = NWARP * wsolve_bytes((size_t)bt, exact);
+__host__ __device__ inline size_t smem_bytes(int bt, bool exact, int nw) {
+    const size_t sweep = nw * (bt == 8 ? Geo<double>::WARP_BYTES : Geo<float>::WARP_BYTES);
+    const size_t solve = nw * wsolve_bytes((size_t)bt, exact);
     return sweep > solve ? sweep : solve;
 }
 
@@ -329,7 +328,7 @@ struct Slot {
 };
 
 __device__ __forceinline__ int64_t knot_index(const Ctx& C, int par, int env, int seg, int i) {
-    return ((int64_t)((par * 2 + env) * C.csize * NWARP + seg)) * C.segcap + i;
+    return ((int64_t)((par * 2 + env) * C.csize * C.nw + seg)) * C.segcap + i;
 }
 
 // segment holding real knot i: largest r in [lo, hi) with pref[r] <= i
@@ -344,8 +343,8 @@ __device__ __forceinline__ int seg_of(const int* pref, int lo, int hi, int i) {
 // element offset of real knot i in the current knot lists
 __device__ __forceinline__ int64_t real_off(const Ctx& C, const TaskSm& S, int env, int i) {
     const int* pr = S.pref[S.kpar][env];
-    const int a = S.rank * NWARP, b = a + NWARP;  // most lookups fall in the CTA's own segments
-    const int r = (i >= pr[a] && i < pr[b]) ? seg_of(pr, a, b, i) : seg_of(pr, 0, S.csize * NWARP, i);
+    const int a = S.rank * C.nw, b = a + C.nw;  // most lookups fall in the CTA's own segments
+    const int r = (i >= pr[a] && i < pr[b]) ? seg_of(pr, a, b, i) : seg_of(pr, 0, S.csize * C.nw, i);
     return knot_index(C, S.kpar, env, r, i - pr[r]);
 }
 
@@ -364,7 +363,7 @@ template <typename T, bool EXACT>
 __device__ __forceinline__ void stage_range(const Ctx& C, const Slot& sl, TaskSm& S, int env, int rlo,
                                             int kcount, int* skt, T* sky, int lane) {
     const int* pr = S.pref[S.kpar][env];
-    const int nseg = S.csize * NWARP;
+    const int nseg = S.csize * C.nw;
     const int mir = S.mir[env], P = S.P[env];
     int r = -1;
     for (int k = lane; k < kcount; k += 32) {
@@ -577,7 +576,7 @@ __device__ __forceinline__ void window_fast_back(const int* skt, const T* sky, c
 #undef SKT
 #undef SSL
 
-template <typename T, bool EXACT>
+template <typename T, bool EXACT, int NW>
 __device__ void solve_task(const Ctx& C, const Slot& sl, TaskSm& S, unsigned char* smem) {
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
 #ifdef EEMD_TRACE
@@ -622,8 +621,8 @@ __device__ void solve_task(const Ctx& C, const Slot& sl, TaskSm& S, unsigned cha
     const int nw0 = (n0 + Bw - 1) / Bw, nw1 = (n1 + Bw - 1) / Bw;
     const int nwt = nw0 + nw1;
     const int ca = (int)((int64_t)S.rank * nwt / S.csize), cb = (int)((int64_t)(S.rank + 1) * nwt / S.csize);
-    const int wa = ca + (int)((int64_t)wid * (cb - ca) / NWARP);
-    const int wb = ca + (int)((int64_t)(wid + 1) * (cb - ca) / NWARP);
+    const int wa = ca + (int)((int64_t)wid * (cb - ca) / NW);
+    const int wb = ca + (int)((int64_t)(wid + 1) * (cb - ca) / NW);
     constexpr int CAP = stage_cap(EXACT);
     unsigned char* ws = smem + (size_t)wid * wsolve_bytes(sizeof(T), EXACT);
     double* ssl = reinterpret_cast<double*>(ws);
@@ -710,33 +709,6 @@ __device__ __forceinline__ double trial_input(const Ctx& C, const TaskDesc& d, i
             return rnd<T>(xv + C.sigma[d.signal] * philox_normal(C.seed, d.signal, d.trial, t));
         default: return xv;  // NONE, PREPERTURBED
     }
-}
-
-// Block-wide exclusive scan of two per-thread counts (one __syncthreads).
-// wtot: shared [2*NWARP], not reused before the next __syncthreads.
-__device__ __forceinline__ void block_scan2(int a, int b, int& ea, int& eb, int& ta, int& tb, int* wtot) {
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    int ia = a, ib = b;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int xa = __shfl_up_sync(0xffffffffu, ia, o);
-        const int xb = __shfl_up_sync(0xffffffffu, ib, o);
-        if (lane >= o) { ia += xa; ib += xb; }
-    }
-    if (lane == 31) { wtot[wid] = ia; wtot[NWARP + wid] = ib; }
-    __syncthreads();
-    int ba = 0, bb = 0;
-    ta = 0;
-    tb = 0;
-#pragma unroll
-    for (int w = 0; w < NWARP; ++w) {
-        const int va = wtot[w], vb = wtot[NWARP + w];
-        if (w < wid) { ba += va; bb += vb; }
-        ta += va;
-        tb += vb;
-    }
-    ea = ba + ia - a;
-    eb = bb + ib - b;
 }
 
 // One interval of an envelope (fast: monomial; exact: the two end knots).
@@ -958,14 +930,14 @@ __device__ T outside_g(const Ctx& C, const TaskSm& S, const TaskDesc& d, const S
 //     samples, knots and this step's run records are written.
 // Every step reads one set of buffers and writes another (ping-pong), so the
 // warps of a step never see each other's writes.
-template <typename T, bool EXACT, int MODE>
+template <typename T, bool EXACT, int MODE, int NW>
 __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned char* smem) {
     using G = Geo<T>;
     constexpr int RUN = G::RUN, WT = G::WT, RS = G::RS;
     constexpr unsigned FULL = 0xffffffffu;
     constexpr bool SIFTING = (MODE == TM_SIFT || MODE == TM_LAST);
     constexpr bool USES_R = (MODE == TM_LAST || MODE == TM_TRANS);
-    __shared__ double2 s_red[NWARP];
+    __shared__ double2 s_red[NW];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int n = S.n, s0 = S.s0, s1 = S.s1, rank = S.rank;
     const bool needs_h = SIFTING || (MODE == TM_TRANS && !S.imf_from_resid);
@@ -991,7 +963,7 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
     const int4* ri_cur = sl.ri + (int64_t)S.kpar * C.slot_runs;
     int4* ri_nxt = sl.ri + (int64_t)(S.kpar ^ 1) * C.slot_runs;
     const int np = S.kpar ^ 1;
-    const int seg = rank * NWARP + wid;
+    const int seg = rank * NW + wid;
     const int64_t pmx = knot_index(C, np, 0, seg, 0);
     const int64_t pmn = knot_index(C, np, 1, seg, 0);
     const T* R0 = static_cast<const T*>(sl.M);
@@ -1001,8 +973,8 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
     // (shares in whole tiles left the last tiles' warps up to a tile behind),
     // cut into tiles of WT samples from r0 (the last one partial)
     const int nrun = (s1 - s0 + RUN - 1) / RUN;
-    const int r0 = min(s1, s0 + (int)((int64_t)wid * nrun / NWARP) * RUN);
-    const int r1 = min(s1, s0 + (int)((int64_t)(wid + 1) * nrun / NWARP) * RUN);
+    const int r0 = min(s1, s0 + (int)((int64_t)wid * nrun / NW) * RUN);
+    const int r1 = min(s1, s0 + (int)((int64_t)(wid + 1) * nrun / NW) * RUN);
     const int ta = 0, tb = (r1 - r0 + WT - 1) / WT;
 
     unsigned char* wb = smem + (size_t)wid * G::WARP_BYTES;
@@ -1349,7 +1321,7 @@ __device__ void sweep(const Ctx& C, const Slot& sl, TaskSm& S, Xchg* X, unsigned
 #endif
 #undef SUB
     // ---------------- publish the segment's SD partials ----------------
-    const double2 rs = block_sum2<THREADS>(make_double2(num, den), s_red);
+    const double2 rs = block_sum2<32 * NW>(make_double2(num, den), s_red);
     if (tid == 0) {
         X[q].num = rs.x;
         X[q].den = rs.y;
@@ -1404,19 +1376,20 @@ __device__ __forceinline__ void imf_level(const Ctx& C, TaskSm& S, int cmax, int
 // Warp 0 gathers the knot counts of every (CTA, warp) segment through
 // distributed shared memory and writes their prefixes for the new lists;
 // thread 0 then takes the step decision, identical in every CTA.
+template <int NW>
 __device__ void decide(const Ctx& C, TaskSm& S, Xchg* X, cg::cluster_group& cl) {
     if (threadIdx.x < 32) {
         const int lane = threadIdx.x;
         const int q = S.step & 1;
-        const int nseg = S.csize * NWARP;
+        const int nseg = S.csize * NW;
         int c[2][2] = {{0, 0}, {0, 0}};  // [env][segment 2*lane + k]
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
             const int sg = 2 * lane + k;
             if (sg < nseg) {
-                const Xchg* xr = cl.map_shared_rank(&X[q], sg / NWARP);
-                c[0][k] = xr->cnt[0][sg % NWARP];
-                c[1][k] = xr->cnt[1][sg % NWARP];
+                const Xchg* xr = cl.map_shared_rank(&X[q], sg / NW);
+                c[0][k] = xr->cnt[0][sg % NW];
+                c[1][k] = xr->cnt[1][sg % NW];
             }
         }
         int tot[2];
@@ -1533,12 +1506,8 @@ __device__ void step_setup(const Ctx& C, const Slot& sl, TaskSm& S) {
 // ---------------------------------------------------------------------------
 // k_emd: the persistent cluster kernel
 // ---------------------------------------------------------------------------
-#ifndef EEMD_MIN_CTAS_PER_SM
-#define EEMD_MIN_CTAS_PER_SM CTAS_PER_SM
-#endif
-
-template <typename T, bool EXACT>
-__global__ void __launch_bounds__(THREADS, EEMD_MIN_CTAS_PER_SM) k_emd(const __grid_constant__ Ctx C) {
+template <typename T, bool EXACT, int NW>
+__global__ void __launch_bounds__(32 * NW, ctas_per_sm(NW)) k_emd(const __grid_constant__ Ctx C) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ TaskSm S;
     __shared__ Xchg X[2];
@@ -1628,21 +1597,21 @@ __global__ void __launch_bounds__(THREADS, EEMD_MIN_CTAS_PER_SM) k_emd(const __g
                     break;
                 }
                 EEMD_PHASE(0);
-                solve_task<T, EXACT>(C, sl, S, smem_raw);
+                solve_task<T, EXACT, NW>(C, sl, S, smem_raw);
                 EEMD_PHASE(1);
                 cl.sync();  // second derivatives of every segment visible
                 EEMD_PHASE(2);
             }
             switch (S.mode) {
-                case TM_SIFT: sweep<T, EXACT, TM_SIFT>(C, sl, S, X, smem_raw); break;
-                case TM_LAST: sweep<T, EXACT, TM_LAST>(C, sl, S, X, smem_raw); break;
-                case TM_TRANS: sweep<T, EXACT, TM_TRANS>(C, sl, S, X, smem_raw); break;
-                default: sweep<T, EXACT, TM_INIT>(C, sl, S, X, smem_raw); break;
+                case TM_SIFT: sweep<T, EXACT, TM_SIFT, NW>(C, sl, S, X, smem_raw); break;
+                case TM_LAST: sweep<T, EXACT, TM_LAST, NW>(C, sl, S, X, smem_raw); break;
+                case TM_TRANS: sweep<T, EXACT, TM_TRANS, NW>(C, sl, S, X, smem_raw); break;
+                default: sweep<T, EXACT, TM_INIT, NW>(C, sl, S, X, smem_raw); break;
             }
             EEMD_PHASE(3);
             cl.sync();  // segment results published
             EEMD_PHASE(4);
-            decide(C, S, X, cl);
+            decide<NW>(C, S, X, cl);
             EEMD_PHASE(5);
         }
         if (S.rcur) {
@@ -1650,7 +1619,7 @@ __global__ void __launch_bounds__(THREADS, EEMD_MIN_CTAS_PER_SM) k_emd(const __g
             const TaskDesc d = C.td[S.task];
             T* r0 = static_cast<T*>(C.resid) + d.s_off;
             const T* r1 = static_cast<const T*>(sl.r1);
-            for (int t = S.s0 + tid; t < S.s1; t += THREADS) r0[t] = r1[t];
+            for (int t = S.s0 + tid; t < S.s1; t += 32 * NW) r0[t] = r1[t];
         }
         if (rank == 0 && tid == 0) {
             TaskOut o;
@@ -1752,14 +1721,13 @@ using namespace eemd;
 namespace {
 
 constexpr int ASSUMED_SMS = 148;        // B200
-constexpr int ASSUMED_CTAS_PER_SM = CTAS_PER_SM;  // resident k_emd CTAs per SM the grid is sized for
 
 struct Layout {
     std::vector<TaskDesc> td;
     std::vector<SignalDesc> sd;
     std::vector<int32_t> order;
     int64_t NS = 0, NIMF = 0, slot_knots = 0, slot_M = 0, slot_n = 0, slot_runs = 0;
-    int B = 0, S = 0, csize = 1, slots = 1, segcap = 0, kcap = 0, scr_rows = 0;
+    int B = 0, S = 0, csize = 1, slots = 1, segcap = 0, kcap = 0, scr_rows = 0, nw = NW_DEFAULT;
     size_t o_hdr, o_td, o_order, o_tout, o_sd, o_sigma, o_resid, o_imfs, o_kt, o_ky, o_M, o_w1, o_r1, o_ri,
         o_scr;
     size_t total = 0;
@@ -1769,10 +1737,16 @@ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 // Clusters of c CTAs of the k_emd instance for (dtype, exact) that the
 // current device can hold at once (0 if the query fails, e.g. no device).
-int active_clusters(int dtype, bool exact, int c) {
-    const void* fn = (dtype == EEMD_F32) ? (const void*)k_emd<float, false>
-                                         : (exact ? (const void*)k_emd<double, true> : (const void*)k_emd<double, false>);
-    const size_t smem = smem_bytes(dtype == EEMD_F32 ? 4 : 8, exact);
+// the k_emd instance of (storage type, exact, warps per CTA)
+const void* emd_fn(int dtype, bool exact, int nw) {
+    if (dtype == EEMD_F32) return nw == 5 ? (const void*)k_emd<float, false, 5> : (const void*)k_emd<float, false, 4>;
+    if (exact) return (const void*)k_emd<double, true, 4>;
+    return nw == 5 ? (const void*)k_emd<double, false, 5> : (const void*)k_emd<double, false, 4>;
+}
+
+int active_clusters(int dtype, bool exact, int c, int nw) {
+    const void* fn = emd_fn(dtype, exact, nw);
+    const size_t smem = smem_bytes(dtype == EEMD_F32 ? 4 : 8, exact, nw);
     int n = 0;
     bool ok = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess;
     if (ok && c > 8) ok = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess;
@@ -1780,7 +1754,7 @@ int active_clusters(int dtype, bool exact, int c) {
         cudaLaunchConfig_t cfg;
         memset(&cfg, 0, sizeof(cfg));
         cfg.gridDim = dim3((unsigned)c, 1, 1);
-        cfg.blockDim = dim3(THREADS, 1, 1);
+        cfg.blockDim = dim3((unsigned)(32 * nw), 1, 1);
         cfg.dynamicSmemBytes = smem;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1800,13 +1774,13 @@ int active_clusters(int dtype, bool exact, int c) {
 
 // The cluster spreads one task over several SMs when there are fewer tasks
 // than CTA slots.
-int autotune_csize(int64_t n_tasks, int64_t nmin, int dtype, bool exact) {
+int autotune_csize(int64_t n_tasks, int64_t nmin, int dtype, bool exact, int nw) {
     // leave a fifth of the CTA slots free: clusters must fit inside a GPC,
     // and the last clusters to be placed would otherwise wait for a second
     // wave.  Signals of a million samples or more take every slot: each CTA
     // then sweeps long ranges, and measured on 64 trials of 2^22 samples 8
     // CTAs per signal (512 CTAs) run 10 % faster than 7.
-    const int64_t slots = (int64_t)ASSUMED_SMS * ASSUMED_CTAS_PER_SM;
+    const int64_t slots = (int64_t)ASSUMED_SMS * ctas_per_sm(nw);
     const int64_t budget = nmin >= (1 << 20) ? slots : slots * 4 / 5;
     int c = (int)std::max<int64_t>(1, std::min<int64_t>(8, budget / std::max<int64_t>(n_tasks, 1)));
     // more tasks than slots: pairs of CTAs halve each task's time and with it
@@ -1819,7 +1793,7 @@ int autotune_csize(int64_t n_tasks, int64_t nmin, int dtype, bool exact) {
     // wave would double the launch)
     if (c == 8 && nmin >= (1 << 20)) {
         for (int c2 = (int)std::min<int64_t>(MAXC, slots / std::max<int64_t>(n_tasks, 1)); c2 > 8; --c2) {
-            if (active_clusters(dtype, exact, c2) >= n_tasks) {
+            if (active_clusters(dtype, exact, c2, nw) >= n_tasks) {
                 c = c2;
                 break;
             }
@@ -1843,6 +1817,8 @@ int check_params(const eemd_params* p) {
     if (p->knots_per_block < 0 || p->knots_per_block > 4096 || p->halo < 0 || p->halo > 256)
         return EEMD_E_BADARG;
     if (p->cluster_size < 0 || p->cluster_size > MAXC) return EEMD_E_BADARG;
+    if (p->cta_warps != 0 && p->cta_warps != 4 && p->cta_warps != 5) return EEMD_E_BADARG;
+    if (p->exact && p->cta_warps == 5) return EEMD_E_NOTSUP;  // exact mode runs 4-warp CTAs
     return EEMD_OK;
 }
 
@@ -1859,7 +1835,8 @@ int make_layout(const eemd_params* p, const int64_t* lengths, int n_signals, int
         nmax = std::max(nmax, lengths[s]);
         nmin = std::min(nmin, lengths[s]);
     }
-    L.csize = p->cluster_size ? p->cluster_size : autotune_csize(n_tasks, nmin, p->dtype, p->exact != 0);
+    L.nw = p->cta_warps ? p->cta_warps : NW_DEFAULT;
+    L.csize = p->cluster_size ? p->cluster_size : autotune_csize(n_tasks, nmin, p->dtype, p->exact != 0, L.nw);
     // decay halo of the seam windows: the truncation error falls like
     // (2 - sqrt 3)^S; 16 rows put it far below float32 rounding
     L.S = p->halo ? p->halo : (p->exact ? 32 : (p->dtype == EEMD_F32 ? 16 : 24));
@@ -1909,7 +1886,7 @@ int make_layout(const eemd_params* p, const int64_t* lengths, int n_signals, int
     const int run = (p->dtype == EEMD_F64) ? Geo<double>::RUN : Geo<float>::RUN;
     const int wt = 32 * run;
     // knots of one kind in one warp's range: at most half its samples (+ends)
-    const int64_t tiles_per_warp = ((segmax + wt - 1) / wt + NWARP - 1) / NWARP;
+    const int64_t tiles_per_warp = ((segmax + wt - 1) / wt + L.nw - 1) / L.nw;
     L.segcap = (int)(tiles_per_warp * wt / 2 + 2);
 #ifdef EEMD_CHECKED
     // test hook of the checked build only: params.reserved > 0 shrinks the knot
@@ -1921,8 +1898,8 @@ int make_layout(const eemd_params* p, const int64_t* lengths, int n_signals, int
     L.slot_n = (nmax + 3) / 4 * 4;
     L.slot_runs = (nmax + run - 1) / run + 1;
     L.slots = (int)std::max<int64_t>(
-        1, std::min<int64_t>(n_tasks, (int64_t)ASSUMED_SMS * ASSUMED_CTAS_PER_SM / L.csize));
-    L.slot_knots = (int64_t)2 * 2 * L.csize * NWARP * L.segcap;
+        1, std::min<int64_t>(n_tasks, (int64_t)ASSUMED_SMS * ctas_per_sm(L.nw) / L.csize));
+    L.slot_knots = (int64_t)2 * 2 * L.csize * L.nw * L.segcap;
     L.slot_M = (int64_t)2 * L.kcap * rs;
     L.scr_rows = p->exact ? (L.B + L.S) : 0;
     L.NS = so;
@@ -1948,7 +1925,7 @@ int make_layout(const eemd_params* p, const int64_t* lengths, int n_signals, int
     L.o_w1 = take(bt * L.slot_n * L.slots);
     L.o_r1 = take(bt * L.slot_n * L.slots);
     L.o_ri = take(16 * 2 * L.slot_runs * L.slots);
-    L.o_scr = take(sizeof(double2) * (size_t)L.scr_rows * L.slots * L.csize * THREADS);
+    L.o_scr = take(sizeof(double2) * (size_t)L.scr_rows * L.slots * L.csize * 32 * L.nw);
     L.total = off;
     return EEMD_OK;
 }
@@ -1992,19 +1969,19 @@ struct Tracer {
     }
 };
 
-template <typename T, bool EXACT>
+template <typename T, bool EXACT, int NW>
 int launch_emd(const Ctx& C, const Layout& L, cudaStream_t st, Tracer& tr) {
-    const size_t smem = smem_bytes((int)sizeof(T), EXACT);
-    if (cudaFuncSetAttribute(k_emd<T, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+    const size_t smem = smem_bytes((int)sizeof(T), EXACT, NW);
+    if (cudaFuncSetAttribute(k_emd<T, EXACT, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return EEMD_E_CUDA;
     if (L.csize > 8 &&
-        cudaFuncSetAttribute(k_emd<T, EXACT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+        cudaFuncSetAttribute(k_emd<T, EXACT, NW>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
         return EEMD_E_CUDA;
     cudaLaunchConfig_t cfg;
     memset(&cfg, 0, sizeof(cfg));
     cfg.gridDim = dim3((unsigned)(L.slots * L.csize), 1, 1);
-    cfg.blockDim = dim3(THREADS, 1, 1);
+    cfg.blockDim = dim3(32 * NW, 1, 1);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
@@ -2015,7 +1992,7 @@ int launch_emd(const Ctx& C, const Layout& L, cudaStream_t st, Tracer& tr) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     tr.begin(EEMD_K_EMD);
-    const cudaError_t e = cudaLaunchKernelEx(&cfg, k_emd<T, EXACT>, C);
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, k_emd<T, EXACT, NW>, C);
     tr.end();
     return e == cudaSuccess ? EEMD_OK : EEMD_E_CUDA;
 }
@@ -2032,9 +2009,12 @@ int run_typed(const eemd_params* p, const Layout& L, Ctx& C, double* imf_sum, in
     }
     int rc;
     if constexpr (sizeof(T) == 8) {
-        rc = p->exact ? launch_emd<T, true>(C, L, st, tr) : launch_emd<T, false>(C, L, st, tr);
+        if (p->exact)
+            rc = launch_emd<T, true, 4>(C, L, st, tr);  // exact mode: float64, 4-warp CTAs
+        else
+            rc = L.nw == 5 ? launch_emd<T, false, 5>(C, L, st, tr) : launch_emd<T, false, 4>(C, L, st, tr);
     } else {
-        rc = launch_emd<T, false>(C, L, st, tr);  // exact mode is float64 only
+        rc = L.nw == 5 ? launch_emd<T, false, 5>(C, L, st, tr) : launch_emd<T, false, 4>(C, L, st, tr);
     }
     if (rc) return rc;
     if (imf_sum || mode_count) {
@@ -2179,6 +2159,7 @@ int32_t eemd_run_traced(const eemd_params* p, const void* x, const int64_t* leng
     C.B = L.B;
     C.S = L.S;
     C.scr_rows = L.scr_rows;
+    C.nw = L.nw;
     C.tau = p->tau;
     C.noise_scale = p->eps;
     C.seed = p->seed;

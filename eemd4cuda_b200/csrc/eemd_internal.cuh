@@ -31,15 +31,12 @@
 
 namespace eemd {
 
-#ifndef EEMD_CTA_WARPS
-#define EEMD_CTA_WARPS 4
-#endif
-constexpr int THREADS = 32 * EEMD_CTA_WARPS;  // threads per CTA of k_emd
-// resident CTAs per SM the kernel is compiled (launch bounds) and the grid sized for
-#ifndef EEMD_CTAS_PER_SM
-#define EEMD_CTAS_PER_SM (16 / EEMD_CTA_WARPS)  // 16 warps of 128 registers fill an SM
-#endif
-constexpr int CTAS_PER_SM = EEMD_CTAS_PER_SM;
+// warps per CTA of k_emd: 4 (the default) or 5, chosen per launch (the
+// autotune table's choice per length bucket); CTAs of 128 registers per
+// thread fill an SM at 16 warps: 4 CTAs of 4 warps, 3 of 5
+constexpr int NW_DEFAULT = 4;
+constexpr int MAXNW = 5;
+__host__ __device__ constexpr int ctas_per_sm(int nw) { return 16 / nw; }
 // largest cluster: portable clusters reach 8 CTAs; 9 to 16 are non-portable
 // and are taken only when the device reports that all of them fit at once
 constexpr int MAXC = 16;
@@ -136,6 +133,7 @@ struct Ctx {
     int32_t n_tasks, n_signals, trial_count, csize;
     int32_t max_sifts, max_imf, min_extrema, end_mode, rules, noise_mode;
     int32_t B, S, scr_rows;
+    int32_t nw;                   // warps per CTA of this launch
     double tau;
     double noise_scale;           // EEMD_NOISE_SCALED: the factor on noise[task][n]
     uint64_t seed;

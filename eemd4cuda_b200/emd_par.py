@@ -91,12 +91,14 @@ class EngineConfig:
     watchdog: negative -k is the test mode (each task first polls a flag that
         nothing sets k times, then the run fails with EEMD_E_TIMEOUT); 0 or
         positive has no effect.
-    cluster_size: CTAs sharing one signal (1..16; 9..16 are non-portable cluster sizes)."""
+    cluster_size: CTAs sharing one signal (1..16; 9..16 are non-portable cluster sizes).
+    cta_warps: warps per CTA (4 or 5; 0 = the autotune table's choice, else 4)."""
     tile: int = 0
     knots_per_block: int = 0
     halo: int = 0
     watchdog: int = 0
     cluster_size: int = 0
+    cta_warps: int = 0
 
 
 _RULES = {"ref": L.EEMD_RULES_REF, "numba": L.EEMD_RULES_NUMBA}
@@ -153,24 +155,26 @@ def make_params(*, dtype=np.float64, noise_mode=L.EEMD_NOISE_NONE, eps=0.2, seed
     p.halo = int(cfg.halo)
     p.watchdog = int(cfg.watchdog)
     p.cluster_size = int(cfg.cluster_size)
+    p.cta_warps = int(cfg.cta_warps)
     return p
 
 
 def tuned(p: L.EemdParams, lengths, trial_count: int) -> L.EemdParams:
-    """The parameters of one launch with the threads per trial (CTAs per task)
-    from the autotune table (eemd4cuda_b200/tuning/) when the caller left
-    cluster_size at 0; otherwise, or without a table entry, p unchanged (the
-    engine then applies its own rule)."""
+    """The parameters of one launch with the threads per trial (CTAs per task
+    and warps per CTA) from the autotune table (eemd4cuda_b200/tuning/) when
+    the caller left cluster_size and cta_warps at 0; otherwise, or without a
+    table entry, p unchanged (the engine then applies its own rule)."""
     from . import autotune
 
-    if p.cluster_size:
+    if p.cluster_size or p.cta_warps:
         return p
-    c = autotune.cluster_size(min(int(n) for n in lengths), len(lengths) * int(trial_count),
-                              "f32" if p.dtype == L.EEMD_F32 else "f64")
+    c, nw = autotune.launch_shape(min(int(n) for n in lengths), len(lengths) * int(trial_count),
+                                  "f32" if p.dtype == L.EEMD_F32 else "f64")
     if not c:
         return p
     q = L.EemdParams.from_buffer_copy(p)
     q.cluster_size = c
+    q.cta_warps = nw if (nw and not p.exact) else 0
     return q
 
 

@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define EEMD_ABI_VERSION 1
+#define EEMD_ABI_VERSION 2
 
 /* status codes (0 = success, negative = error) */
 #define EEMD_OK                 0
@@ -105,6 +105,9 @@ typedef struct eemd_params {
                                  lists at k knots of one kind per warp segment, so that
                                  the EEMD_E_KNOT_OVERFLOW path can be exercised; the
                                  release build ignores it */
+    int32_t  cta_warps;       /* warps per CTA of the persistent kernel: 0 = 4, 4 or 5 (5: three
+                                 CTAs per SM instead of four; float64 exact mode runs 4) */
+    int32_t  reserved2;       /* 0 */
 } eemd_params;
 
 /* Fill p with the defaults of emd_par.decompose (emd_par.py:260-262):

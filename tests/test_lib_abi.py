@@ -65,7 +65,8 @@ def test_version_and_strerror():
 
 
 def test_struct_layout():
-    assert ctypes.sizeof(L.EemdParams) == 88
+    assert ctypes.sizeof(L.EemdParams) == 96
+    assert L.EemdParams.cta_warps.offset == 88
     assert L.EemdParams.watchdog.offset == 72
     p = L.default_params()
     assert p.dtype == L.EEMD_F64 and p.max_sifts == 50 and p.min_extrema == 4
