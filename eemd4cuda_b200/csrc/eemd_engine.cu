@@ -1382,10 +1382,15 @@ __device__ void decide(const Ctx& C, TaskSm& S, Xchg* X, cg::cluster_group& cl) 
         const int lane = threadIdx.x;
         const int q = S.step & 1;
         const int nseg = S.csize * NW;
-        int c[2][2] = {{0, 0}, {0, 0}};  // [env][segment 2*lane + k]
+        // segments SPL*lane .. SPL*lane + SPL-1 per lane (SPL = 3 covers the
+        // 16 x 5 = 80 segments of the largest cluster of 5-warp CTAs)
+        constexpr int SPL = (MAXSEG + 31) / 32;
+        static_assert(SPL * 32 >= MAXSEG, "segments per lane");
+        int c[2][SPL];  // [env][segment SPL*lane + k]
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const int sg = 2 * lane + k;
+        for (int k = 0; k < SPL; ++k) {
+            const int sg = SPL * lane + k;
+            c[0][k] = c[1][k] = 0;
             if (sg < nseg) {
                 const Xchg* xr = cl.map_shared_rank(&X[q], sg / NW);
                 c[0][k] = xr->cnt[0][sg % NW];
@@ -1395,7 +1400,9 @@ __device__ void decide(const Ctx& C, TaskSm& S, Xchg* X, cg::cluster_group& cl) 
         int tot[2];
 #pragma unroll
         for (int env = 0; env < 2; ++env) {
-            const int v = c[env][0] + c[env][1];
+            int v = 0;
+#pragma unroll
+            for (int k = 0; k < SPL; ++k) v += c[env][k];
             int inc = v;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -1404,9 +1411,12 @@ __device__ void decide(const Ctx& C, TaskSm& S, Xchg* X, cg::cluster_group& cl) 
             }
             tot[env] = __shfl_sync(0xffffffffu, inc, 31);
             int* pr = S.pref[S.kpar ^ 1][env];
-            const int e = inc - v;
-            if (2 * lane < nseg) pr[2 * lane] = e;
-            if (2 * lane + 1 < nseg) pr[2 * lane + 1] = e + c[env][0];
+            int e = inc - v;
+#pragma unroll
+            for (int k = 0; k < SPL; ++k) {
+                if (SPL * lane + k < nseg) pr[SPL * lane + k] = e;
+                e += c[env][k];
+            }
             if (lane == 0) pr[nseg] = tot[env];
         }
         if (lane == 0) {

@@ -330,3 +330,20 @@ def test_knot_capacity_overflow_is_reported_and_context_survives():
         outs.append((imfs.cpu().numpy(), int(nmode.item())))
     assert outs[0][1] == outs[1][1] == 8
     assert np.array_equal(outs[0][0], outs[1][0])
+
+
+@pytest.mark.parametrize("cta_warps,cluster", [(5, 4), (5, 13), (5, 16), (4, 16)])
+def test_launch_shapes_give_identical_results(cta_warps, cluster):
+    """Every launch shape the autotune table may choose -- 4- or 5-warp CTAs,
+    up to 16 CTAs per task (80 knot segments) -- gives the same IMFs bit for
+    bit as 4-warp CTAs in clusters of 4 (fixed sift counts, so no decision
+    depends on how the SD sums are grouped)."""
+    x = signals.harmonic_clicks(65536, seed=3)
+    kw = dict(tau=0.0, max_sifts=5, max_imf=3, exact=False, noise_mode=L.EEMD_NOISE_PHILOX, eps=0.2, seed=4,
+              lengths=[len(x)], trial_count=2)
+    base = raw_run(None, x=x, config=M.EngineConfig(cta_warps=4, cluster_size=4), **kw)
+    other = raw_run(None, x=x, config=M.EngineConfig(cta_warps=cta_warps, cluster_size=cluster), **kw)
+    assert other["nmode"].tolist() == base["nmode"].tolist()
+    assert np.array_equal(other["knot_log"], base["knot_log"])
+    for a, b in zip(other["imfs"], base["imfs"]):
+        assert np.array_equal(a, b)
