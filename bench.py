@@ -379,10 +379,13 @@ def measured_peak_hbm():
 # of the same signal and are scaled per (signal, trial) task, since every task
 # streams its own buffers.
 EMD_TRAFFIC = {
-    "harmonic48k": {"bytes_per_launch": 6730622000, "engine_sha256": None,
-                    "capture": "one k_emd launch of the 100-trial 48 kHz workload"},
-    "amfm4m": {"bytes_per_task": 5606744640.0, "engine_sha256": None,
-               "capture": "one k_emd launch of 4 trials of the 2^22-sample signal, per task"},
+    "harmonic48k": {"bytes_per_launch": 6861367000,
+                    "engine_sha256": "7754f01fd896a1987064dee2d8a6248e61ca6833687fc52b45c2910270572110",
+                    "capture": "one k_emd launch of the 100-trial 48 kHz workload (clusters of 4 five-warp CTAs)"},
+    "amfm4m": {"bytes_per_task": 5611588672.0,
+               "engine_sha256": "7754f01fd896a1987064dee2d8a6248e61ca6833687fc52b45c2910270572110",
+               "capture": "one k_emd launch of 4 trials of the 2^22-sample signal (clusters of 16 five-warp "
+                          "CTAs), per task"},
 }
 
 
@@ -1208,6 +1211,34 @@ def run_ceemdan(args):
 # ---------------------------------------------------------------------------
 # the IMF spectra stage (spectra.py:18-58 semantics) on the device
 # ---------------------------------------------------------------------------
+def fft_passes(n: int) -> int:
+    """Kernel launches of one FFT of length n in libeemd_spectra.so: one
+    Stockham pass per radix (4s, then 2s, then odd primes up to 31), or for a
+    length with a larger prime factor Bluestein's 2 + 3 power-of-two
+    transforms + 2."""
+    def radices(m):
+        k = 0
+        for q in (4, 2, *range(3, 32, 2)):
+            while m % q == 0:
+                m //= q
+                k += 1
+        return k, m == 1
+    k, ok = radices(n)
+    if ok:
+        return max(k, 1)
+    L = 1
+    while L < 2 * n - 1:
+        L <<= 1
+    return 4 + 3 * radices(L)[0]
+
+
+def spectra_launches(n: int, nperseg: int) -> int:
+    """Launches of the spectra step: two STFT calls (k_frames, the frame FFT,
+    k_stft_out) and one Hilbert call (k_promote, FFT, k_analytic, inverse FFT,
+    k_if_amp)."""
+    return 2 * (2 + fft_passes(nperseg)) + 3 + 2 * fft_passes(n)
+
+
 def run_spectra(args):
     """One step: the Tier-2 spectra of the bench workload's decomposition --
     STFT (nperseg 4096, 50 % overlap) of x and of its 8 ensemble-mean IMFs and
@@ -1297,8 +1328,9 @@ def run_spectra(args):
         "e2e": {"value": round(rows * N / (e2e / 1e3) / 1e6, 3), "unit": "Msamples/s", "ms_per_step": round(e2e, 3),
                 "h2d_bytes_per_step": rows * N * 8 + r.n_modes * N * 8,
                 "d2h_bytes_per_step": rows * F * T * 16 + 2 * r.n_modes * N * 8},
-        "gpu_launches": 6 * args.steps,  # k_frames + k_stft_out per STFT call, k_analytic + k_if_amp (cuFFT not counted)
-        "roofline": {"bound": "hbm", "kernel": "hilbert stage (cuFFT D2Z, k_analytic, Z2Z, k_if_amp)",
+        "gpu_launches": spectra_launches(N, nper) * args.steps,
+        "roofline": {"bound": "hbm", "kernel": "hilbert stage (k_promote, FFT passes, k_analytic, inverse FFT "
+                                               "passes, k_if_amp)",
                      "achieved": round(gbs, 2), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": round(gbs / peak, 4), "traffic": None, "algorithmic_bytes": h_bytes,
                      "ms": round(h_ms, 4)},

@@ -5,8 +5,9 @@ stft_block and hilbert_if take one signal (1-D) or a batch of rows (2-D,
 [M, N]) as host arrays and return host arrays, like the reference; the
 *_device variants take and return float64 torch tensors resident on the GPU,
 so the IMFs of eemd_finalize can be analysed without leaving the device.
-All arithmetic runs in libeemd_spectra.so (cuFFT for the transforms, this
-package's kernels between them); if_stats is the reference's host reduction.
+All arithmetic runs in libeemd_spectra.so (its own Stockham / Bluestein FFT
+kernels and the kernels between the transforms; no FFT library); if_stats is
+the reference's host reduction.
 """
 from __future__ import annotations
 

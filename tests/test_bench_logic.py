@@ -36,3 +36,13 @@ def test_measured_traffic_per_workload():
     assert bench.measured_traffic("plain8k", 1) == (None, None)
     # the flag follows the engine source the capture ran
     assert len(bench.engine_source_sha256()) == 64
+
+
+def test_spectra_launch_count():
+    """The spectra line's launch count follows the FFT plan of libeemd_spectra.so:
+    48000 = 4^3 * 2 * 3 * 5^3 (8 passes), 4096 = 4^6 (6), 4099 (prime) through
+    Bluestein's 16384-point transforms (4 + 3 * 7)."""
+    assert bench.fft_passes(48000) == 8
+    assert bench.fft_passes(4096) == 6
+    assert bench.fft_passes(4099) == 4 + 3 * 7
+    assert bench.spectra_launches(48000, 4096) == 2 * (2 + 6) + 3 + 2 * 8
