@@ -1081,12 +1081,14 @@ def run_surrogate(args):
                      "peak": hbm_peak, "peak_kind": hbm_kind, "unit": "GB/s", "frac": round(emd_gbs / hbm_peak, 4),
                      "traffic": None, "algorithmic_bytes_per_launch": round(emd_bytes),
                      "avg_launch_ms": round(emd_ev["ms"], 4)},
-        "roofline_tensor": {"bound": "tensor", "kernel": "k_conv_tma", "achieved": round(tflops, 2), "peak": peak,
+        "roofline_tensor": {"bound": "tensor", "kernel": CONV_KERNEL_NAMES.get(net.conv_kernel, "conv"),
+                     "achieved": round(tflops, 2), "peak": peak,
                      "peak_kind": peak_kind, "unit": "TFLOP/s", "frac": round(tflops * 1e12 / (peak * 1e12), 4),
                      "traffic": None, "algorithmic_flops_per_launch": round(flops / n_conv),
                      "avg_launch_ms": round(net_ms / n_conv, 5)},
         # one 64-channel layer does 96 FLOP per byte, below the ridge: the layer's own bound is HBM
-        "roofline_hbm": {"bound": "hbm", "kernel": "k_conv_tma", "achieved": round(net_bytes / (net_ms / 1e3) / 1e9, 2),
+        "roofline_hbm": {"bound": "hbm", "kernel": CONV_KERNEL_NAMES.get(net.conv_kernel, "conv"),
+                         "achieved": round(net_bytes / (net_ms / 1e3) / 1e9, 2),
                          "peak": hbm_peak, "peak_kind": hbm_kind, "unit": "GB/s",
                          "frac": round(net_bytes / (net_ms / 1e3) / 1e9 / hbm_peak, 4),
                          "algorithmic_bytes_per_pass": net_bytes},
@@ -1211,11 +1213,16 @@ def run_ceemdan(args):
 # ---------------------------------------------------------------------------
 # the IMF spectra stage (spectra.py:18-58 semantics) on the device
 # ---------------------------------------------------------------------------
+SMEM_FFT_MAX = 4096  # longest row libeemd_spectra.so transforms in one shared-memory launch
+# eemd_sg_conv's tensor_cores argument -> the kernel it runs
+CONV_KERNEL_NAMES = {1: "k_conv_tc", 2: "k_conv_tc2", 3: "k_conv_tma", 4: "k_conv_ws"}
+
+
 def fft_passes(n: int) -> int:
     """Kernel launches of one FFT of length n in libeemd_spectra.so: one
-    Stockham pass per radix (4s, then 2s, then odd primes up to 31), or for a
-    length with a larger prime factor Bluestein's 2 + 3 power-of-two
-    transforms + 2."""
+    launch for a length up to 4096 whose factors are 4, 2 and odd primes up
+    to 31, else one Stockham pass per such factor, or for a length with a
+    larger prime factor Bluestein's 2 + 3 power-of-two transforms + 2."""
     def radices(m):
         k = 0
         for q in (4, 2, *range(3, 32, 2)):
@@ -1223,20 +1230,25 @@ def fft_passes(n: int) -> int:
                 m //= q
                 k += 1
         return k, m == 1
-    k, ok = radices(n)
-    if ok:
-        return max(k, 1)
+
+    def direct(m):
+        k = radices(m)[0]
+        return 1 if m <= SMEM_FFT_MAX else max(k, 1)
+    if radices(n)[1]:
+        return direct(n)
     L = 1
     while L < 2 * n - 1:
         L <<= 1
-    return 4 + 3 * radices(L)[0]
+    return 4 + 3 * direct(L)
 
 
 def spectra_launches(n: int, nperseg: int) -> int:
-    """Launches of the spectra step: two STFT calls (k_frames, the frame FFT,
-    k_stft_out) and one Hilbert call (k_promote, FFT, k_analytic, inverse FFT,
-    k_if_amp)."""
-    return 2 * (2 + fft_passes(nperseg)) + 3 + 2 * fft_passes(n)
+    """Launches of the spectra step: two STFT calls (one launch each when the
+    frame transform fits one shared-memory launch, else k_frames, the frame
+    FFT and k_stft_out) and one Hilbert call (k_promote, FFT, k_analytic,
+    inverse FFT, k_if_amp)."""
+    stft = 1 if fft_passes(nperseg) == 1 and nperseg <= SMEM_FFT_MAX else 2 + fft_passes(nperseg)
+    return 2 * stft + 3 + 2 * fft_passes(n)
 
 
 def run_spectra(args):

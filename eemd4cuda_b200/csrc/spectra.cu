@@ -200,6 +200,76 @@ __device__ __forceinline__ void dft_small(double2 (&a)[R], int sign) {
     }
 }
 
+// butterfly j of a Stockham pass of radix R over one row of N (nb = N / R):
+// reads x[j + q nb], twiddles by w^(q k) of the sub-transform length Ns R
+// (k = j mod Ns), takes the radix-R DFT and writes y[(j / Ns) Ns R + k + q Ns]
+// twiddles formed on the fly
+struct TwDirect {
+    __device__ __forceinline__ double2 operator()(int64_t num, int64_t den, int sign) const {
+        return twiddle(num, den, sign);
+    }
+};
+
+// twiddles looked up in a table of exp(2 pi i m / n), m < n, made with the
+// same sincospi arguments (m / n and r / den are the same correctly rounded
+// quotient when r = m den / n), so the values are twiddle()'s bit for bit
+struct TwTable {
+    const double2* tab;
+    int64_t n;
+    __device__ __forceinline__ double2 operator()(int64_t num, int64_t den, int sign) const {
+        int64_t r = num % den;
+        if (r < 0) r += den;
+        const double2 v = tab[r * (n / den)];
+        return make_double2(v.x, sign < 0 ? -v.y : v.y);
+    }
+};
+
+template <int R, typename TW = TwDirect>
+__device__ __forceinline__ void bfly(const double2* x, double2* y, int64_t j, int64_t nb, int64_t Ns, int sign,
+                                     const TW& tw = TW()) {
+    const int64_t k = j % Ns;
+    double2 a[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) a[q] = x[j + q * nb];
+    if (Ns > 1) {
+#pragma unroll
+        for (int q = 1; q < R; ++q) a[q] = cmul(a[q], tw((int64_t)q * k, Ns * R, sign));
+    }
+    dft_small<R>(a, sign);
+    const int64_t base = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int q = 0; q < R; ++q) y[base + q * Ns] = a[q];
+}
+
+// the same butterfly for an odd prime radix r <= 31 (a direct DFT of the r points)
+__device__ __forceinline__ void bfly_prime(const double2* x, double2* y, int64_t j, int64_t nb, int64_t Ns, int r,
+                                           int sign) {
+    const int64_t k = j % Ns;
+    double2 a[31];
+    for (int q = 0; q < r; ++q) {
+        a[q] = x[j + q * nb];
+        if (q > 0 && Ns > 1) a[q] = cmul(a[q], twiddle((int64_t)q * k, Ns * r, sign));
+    }
+    const int64_t base = (j / Ns) * Ns * r + k;
+    for (int q = 0; q < r; ++q) {
+        double2 s = a[0];
+        for (int p = 1; p < r; ++p) s = cadd(s, cmul(a[p], twiddle((int64_t)p * q, r, sign)));
+        y[base + q * Ns] = s;
+    }
+}
+
+template <typename TW>
+__device__ __forceinline__ void bfly_any(const double2* x, double2* y, int64_t j, int64_t nb, int64_t Ns, int r,
+                                         int sign, const TW& tw) {
+    switch (r) {
+        case 2: bfly<2>(x, y, j, nb, Ns, sign, tw); break;
+        case 3: bfly<3>(x, y, j, nb, Ns, sign, tw); break;
+        case 4: bfly<4>(x, y, j, nb, Ns, sign, tw); break;
+        case 5: bfly<5>(x, y, j, nb, Ns, sign, tw); break;
+        default: bfly_prime(x, y, j, nb, Ns, r, sign); break;
+    }
+}
+
 // one Stockham pass of radix R over M rows of N: in -> out (distinct buffers)
 template <int R>
 __global__ void k_fft_pass(const double2* __restrict__ in, double2* __restrict__ out, int M, int64_t N, int64_t Ns,
@@ -209,24 +279,10 @@ __global__ void k_fft_pass(const double2* __restrict__ in, double2* __restrict__
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t m = i / nb, j = i % nb;
-        const double2* x = in + m * N;
-        double2* y = out + m * N;
-        const int64_t k = j % Ns;
-        double2 a[R];
-#pragma unroll
-        for (int q = 0; q < R; ++q) a[q] = x[j + q * nb];
-        if (Ns > 1) {
-#pragma unroll
-            for (int q = 1; q < R; ++q) a[q] = cmul(a[q], twiddle((int64_t)q * k, Ns * R, sign));
-        }
-        dft_small<R>(a, sign);
-        const int64_t base = (j / Ns) * Ns * R + k;
-#pragma unroll
-        for (int q = 0; q < R; ++q) y[base + q * Ns] = a[q];
+        bfly<R>(in + m * N, out + m * N, j, nb, Ns, sign);
     }
 }
 
-// the same pass for an odd prime radix r <= 31 (a direct DFT of the r points)
 __global__ void k_fft_pass_prime(const double2* __restrict__ in, double2* __restrict__ out, int M, int64_t N,
                                  int64_t Ns, int r, int sign) {
     const int64_t nb = N / r;
@@ -234,20 +290,100 @@ __global__ void k_fft_pass_prime(const double2* __restrict__ in, double2* __rest
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t m = i / nb, j = i % nb;
-        const double2* x = in + m * N;
-        double2* y = out + m * N;
-        const int64_t k = j % Ns;
-        double2 a[31];
-        for (int q = 0; q < r; ++q) {
-            a[q] = x[j + q * nb];
-            if (q > 0 && Ns > 1) a[q] = cmul(a[q], twiddle((int64_t)q * k, Ns * r, sign));
+        bfly_prime(in + m * N, out + m * N, j, nb, Ns, r, sign);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// One row per CTA in shared memory: every pass of a direct plan (no
+// Bluestein) of length n <= SMEM_FFT_MAX in one launch, the two ping-pong
+// buffers and a table of the n twiddles exp(2 pi i m / n) in shared memory
+// (made once per CTA: n sincospi instead of (R - 1) n / R per pass).  The
+// butterflies are the global passes' own (bfly, bfly_prime) and the table
+// holds twiddle()'s values, so the results are the same bit for bit.
+// ---------------------------------------------------------------------------
+constexpr int SMEM_FFT_MAX = 4096;   // three arrays of n complex doubles: 192 KB
+constexpr int SMEM_FFT_THREADS = 512;
+constexpr int SMEM_FFT_MAXRAD = 16;  // factors of n <= 4096 (at most 12)
+
+struct SmemPlan {
+    int n, nrad;
+    int rad[SMEM_FFT_MAXRAD];
+};
+
+// tab[m] = exp(2 pi i m / n), m < n (twiddle()'s arithmetic)
+__device__ void smem_twiddles(double2* tab, int n) {
+    for (int m = threadIdx.x; m < n; m += blockDim.x) {
+        double sv, cv;
+        sincospi(2.0 * ((double)m / (double)n), &sv, &cv);
+        tab[m] = make_double2(cv, sv);
+    }
+}
+
+// the passes over a[0..n) (b: the other buffer, tab: the twiddle table);
+// returns the buffer holding the result
+__device__ double2* smem_stockham(double2* a, double2* b, const double2* tab, const SmemPlan& P, int sign) {
+    double2* cur = a;
+    double2* dst = b;
+    const TwTable tw{tab, P.n};
+    int Ns = 1;
+    for (int s = 0; s < P.nrad; ++s) {
+        const int r = P.rad[s], nb = P.n / r;
+        for (int j = threadIdx.x; j < nb; j += blockDim.x) bfly_any(cur, dst, j, nb, Ns, r, sign, tw);
+        __syncthreads();
+        Ns *= r;
+        double2* t = cur;
+        cur = dst;
+        dst = t;
+    }
+    return cur;
+}
+
+__global__ void __launch_bounds__(SMEM_FFT_THREADS) k_fft_smem(const double2* __restrict__ in, double2* out, int M,
+                                                               const __grid_constant__ SmemPlan P, int sign) {
+    extern __shared__ double2 sfft[];
+    double2* a = sfft;
+    double2* b = sfft + P.n;
+    double2* tab = sfft + 2 * P.n;
+    smem_twiddles(tab, P.n);
+    for (int m = blockIdx.x; m < M; m += gridDim.x) {
+        const double2* x = in + (int64_t)m * P.n;
+        for (int i = threadIdx.x; i < P.n; i += blockDim.x) a[i] = x[i];
+        __syncthreads();
+        const double2* r = smem_stockham(a, b, tab, P, sign);
+        double2* y = out + (int64_t)m * P.n;
+        for (int i = threadIdx.x; i < P.n; i += blockDim.x) y[i] = r[i];
+        __syncthreads();
+    }
+}
+
+// The whole STFT of one frame per CTA iteration: frame (m, j) windowed into
+// shared memory (k_frames' arithmetic), its transform, and bins f < F scaled
+// into Z[m][f][j] (k_stft_out's arithmetic).
+__global__ void __launch_bounds__(SMEM_FFT_THREADS) k_stft_smem(const double* __restrict__ x, double2* Z, int M,
+                                                                int64_t N, int step, int T, int F, double inv_wsum,
+                                                                const __grid_constant__ SmemPlan P) {
+    extern __shared__ double2 sfft[];
+    double2* a = sfft;
+    double2* b = sfft + P.n;
+    double2* tab = sfft + 2 * P.n;
+    smem_twiddles(tab, P.n);
+    const int nperseg = P.n, half = nperseg / 2;
+    for (int64_t mj = blockIdx.x; mj < (int64_t)M * T; mj += gridDim.x) {
+        const int j = (int)(mj % T);
+        const int64_t m = mj / T;
+        for (int n = threadIdx.x; n < nperseg; n += blockDim.x) {
+            const int64_t s = (int64_t)j * step + n - half;
+            const double w = 0.5 - 0.5 * cos(2.0 * PI * (double)n / (double)nperseg);
+            a[n] = make_double2((s >= 0 && s < N) ? x[m * N + s] * w : 0.0, 0.0);
         }
-        const int64_t base = (j / Ns) * Ns * r + k;
-        for (int q = 0; q < r; ++q) {
-            double2 s = a[0];
-            for (int p = 1; p < r; ++p) s = cadd(s, cmul(a[p], twiddle((int64_t)p * q, r, sign)));
-            y[base + q * Ns] = s;
+        __syncthreads();
+        const double2* r = smem_stockham(a, b, tab, P, -1);
+        for (int f = threadIdx.x; f < F; f += blockDim.x) {
+            const double2 v = r[f];
+            Z[(m * F + f) * T + j] = make_double2(v.x * inv_wsum, v.y * inv_wsum);
         }
+        __syncthreads();
     }
 }
 
@@ -330,6 +466,23 @@ FftPlan make_fft_plan(int64_t n) {
 // complex elements of scratch an FFT of M rows needs beyond its two ping-pong buffers
 int64_t fft_extra(const FftPlan& P, int M) { return P.L ? 2 * (int64_t)M * P.L + 2 * P.L : 0; }
 
+// the shared-memory plan of a length, or false when it runs as global passes
+bool smem_plan(int64_t len, const std::vector<int>& rad, SmemPlan& sp) {
+    if (len > SMEM_FFT_MAX || rad.empty() || rad.size() > (size_t)SMEM_FFT_MAXRAD) return false;
+    sp.n = (int)len;
+    sp.nrad = (int)rad.size();
+    for (size_t i = 0; i < rad.size(); ++i) sp.rad[i] = rad[i];
+    return true;
+}
+
+// shared memory of the one-row-per-CTA kernels (set once per kernel)
+bool smem_ready(const void* fn) {
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(3 * SMEM_FFT_MAX * sizeof(double2))) == cudaSuccess;
+}
+
+unsigned smem_grid(int64_t rows) { return (unsigned)(rows < 65535 ? rows : 65535); }
+
 // Stockham passes of length len over M rows: src -> (b1, b2 alternately); returns the result buffer
 double2* stockham(const double2* src, double2* b1, double2* b2, int M, int64_t len, const std::vector<int>& rad,
                   int sign, cudaStream_t st) {
@@ -338,6 +491,12 @@ double2* stockham(const double2* src, double2* b1, double2* b2, int M, int64_t l
     int64_t Ns = 1;
     if (rad.empty()) {  // length 1: the transform is the identity
         cudaMemcpyAsync(b1, src, sizeof(double2) * (size_t)M * (size_t)len, cudaMemcpyDeviceToDevice, st);
+        return b1;
+    }
+    SmemPlan sp;
+    static const bool smem_ok = smem_ready(reinterpret_cast<const void*>(k_fft_smem));
+    if (smem_ok && smem_plan(len, rad, sp)) {
+        k_fft_smem<<<smem_grid(M), SMEM_FFT_THREADS, 3 * sp.n * sizeof(double2), st>>>(src, b1, M, sp, sign);
         return b1;
     }
     for (int r : rad) {
@@ -513,6 +672,14 @@ int32_t eemd_sp_stft(const double* x, int32_t M, int64_t N, int32_t nperseg, int
     // the window's sum, added in index order (as the reference's window sum is formed)
     double wsum = 0.0;
     for (int n = 0; n < nperseg; ++n) wsum += 0.5 - 0.5 * cos(2.0 * PI * (double)n / (double)nperseg);
+    SmemPlan sp;
+    static const bool smem_ok = smem_ready(reinterpret_cast<const void*>(k_stft_smem));
+    if (smem_ok && !L.P.L && smem_plan(nperseg, L.P.radices, sp)) {
+        // one launch: frames, their transforms and the scaled bins
+        k_stft_smem<<<smem_grid((int64_t)M * T), SMEM_FFT_THREADS, 3 * sp.n * sizeof(double2), st>>>(
+            x, reinterpret_cast<double2*>(Z), M, N, nperseg - noverlap, T, F, 1.0 / wsum, sp);
+        return cudaGetLastError() == cudaSuccess ? EEMD_SP_OK : EEMD_SP_E_CUDA;
+    }
     k_frames<<<grid_for((int64_t)M * T * nperseg), 256, 0, st>>>(x, b.x, M, N, nperseg, nperseg - noverlap, T);
     double2* spec = fft_rows(b.x, b.y, b.z, b.extra, M * T, L.P, -1, st);
     k_stft_out<<<grid_for((int64_t)M * F * T), 256, 0, st>>>(spec, reinterpret_cast<double2*>(Z), M, F, T, nperseg,

@@ -7,9 +7,10 @@
 // with C = 16 (10 IMF channels, zero padded) or 64.
 //
 // Every convolution is an implicit GEMM on the 5th-generation tensor cores
-// (three forms: k_conv_tc, single-buffered with cp.async staging; k_conv_tc2,
-// double-buffered; k_conv_tma, double-buffered with bulk-tensor loads -- the
-// one the network uses):
+// (four forms: k_conv_tc, single-buffered with cp.async staging; k_conv_tc2,
+// double-buffered; k_conv_tma, double-buffered with bulk-tensor loads;
+// k_conv_ws, warp-specialised with swizzled operands and bulk-tensor loads
+// and stores):
 //     D[t][n] = sum_{tap, c} X[t + dir*(tap-1)*dil][c] * W[n][tap*Cin + c]
 // with M = 128 time samples per tile, N = the output channels and
 // K = 3*Cin.  The CTA stages the three shifted copies of its input tile
@@ -22,9 +23,10 @@
 // ReLU-derivative mask, bf16 store).  dir = +1 is the forward convolution;
 // dir = -1 with transposed weights is the gradient with respect to the input.
 //
-// The weight gradient, the loss, Adam and the packing kernels run on CUDA
-// cores.  A plain CUDA-core convolution with the same arguments is kept for
-// checking the tensor-core path on the GPU.
+// The weight gradient is an implicit GEMM over time on tcgen05 too
+// (k_wgrad_tc; k_wgrad is its CUDA-core form); the loss, Adam and the packing
+// kernels run on CUDA cores.  A plain CUDA-core convolution with the same
+// arguments is kept for checking the tensor-core path on the GPU.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
@@ -647,6 +649,269 @@ __global__ void __launch_bounds__(32 * EW) k_conv_tma(const __grid_constant__ CU
     }
 }
 
+// ---------------------------------------------------------------------------
+// Warp-specialised variant (tensor_cores = 4).  Every operand is in a
+// swizzled K-major layout whose rows are one tap's CIN channels: 64 channels
+// in the 128-byte swizzle (rows of 128 bytes, the 16-byte chunks of row r
+// permuted by XOR with r mod 8, 8-row groups 1024 bytes apart), 16 channels
+// in the 32-byte swizzle (rows of 32 bytes, chunk XOR (r / 4) mod 2, 8-row
+// groups 256 bytes apart).  A tap of the input tile is ONE bulk-tensor box
+// {CIN channels, 128 samples} written in that layout by the copy engine, so
+// a tile takes 3 copies instead of 3 * CIN / 8 narrow ones, and the weights
+// are re-laid into the same form in shared memory once per CTA.  The roles
+// run concurrently on their own mbarriers:
+//   copy warp  (lane 0): tile k into input stage k mod WS_STAGES once MMA
+//                        k - WS_STAGES has released it (empty[s]);
+//   MMA warp   (lane 0): waits full[s] and the accumulator's release
+//                        (acce[k & 1]), issues the 3 * CIN / 16 MMAs of tile k into
+//                        accumulator k & 1, commits to empty[s] and accf[k & 1];
+//   8 epilogue warps   : read their lane quadrant x half the columns of the
+//                        accumulator, release it, add bias / ReLU / mask,
+//                        write the bf16 tile into a swizzled staging buffer,
+//                        and one thread stores it with a bulk-tensor store
+//                        (rows past T are clipped by the tensor map).
+// The MMA's K order (tap-major, 16 channels per instruction) is the same as
+// the other forms', so the results are bit-identical to theirs.  Every wait
+// is bounded; a wait that gives up sets *err and every role leaves its loop.
+// No multicast.
+// ---------------------------------------------------------------------------
+constexpr int WS_STAGES = 3;                    // input tiles in flight
+constexpr int WS_EPI = 8;                       // epilogue warps
+constexpr int WS_THREADS = 32 * (WS_EPI + 2);   // + the copy warp and the MMA warp
+
+template <int CIN, int COUT>
+struct WsGeo {
+    static constexpr int ROWB = CIN * 2;                     // bytes of one operand row (one tap)
+    static constexpr int SBO = 8 * ROWB;                     // 8-row group stride
+    static constexpr uint64_t LAYOUT = CIN == 64 ? 2 : 6;    // descriptor swizzle: 128-byte / 32-byte
+    static constexpr int TAP_BYTES = TM * ROWB;              // 128 rows of one tap
+    static constexpr int A_BYTES = 3 * TAP_BYTES;            // one input stage
+    static constexpr int B_TAP = COUT * ROWB;                // one tap of the weights
+    static constexpr int B_BYTES = 3 * B_TAP;
+    static constexpr int O_BYTES = TM * COUT * 2;            // one output tile
+    static constexpr int SMEM = WS_STAGES * A_BYTES + B_BYTES + 2 * O_BYTES + 1024;  // + alignment slack
+    // 16-byte chunk c of operand row r in the swizzled layout
+    static __device__ __forceinline__ int chunk(int c, int r) { return CIN == 64 ? c ^ (r & 7) : c ^ ((r >> 2) & 1); }
+};
+
+// shared-memory descriptor of a K-major swizzled operand: 8-row groups sbo
+// bytes apart; the leading offset is unused for these layouts
+__device__ __forceinline__ uint64_t sw_desc(uint32_t addr, uint32_t sbo, uint64_t layout) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) |
+           (1ull << 46) | (layout << 61);
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// named barrier 1 over the epilogue warps, OR of v over their threads
+__device__ __forceinline__ bool epi_bar_or(bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, 1, %2, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v), "n"(32 * WS_EPI)
+        : "memory");
+    return r != 0;
+}
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(WS_THREADS, 1) k_conv_ws(const __grid_constant__ CUtensorMap tin,
+                                                            const __grid_constant__ CUtensorMap tout,
+                                                            const __nv_bfloat16* __restrict__ wpk,
+                                                            const float* __restrict__ bias, int B, int T, int dil,
+                                                            int dir, int relu,
+                                                            const __nv_bfloat16* __restrict__ mask, int* err,
+                                                            long long spin_limit) {
+    using G = WsGeo<CIN, COUT>;
+    constexpr int NS = WS_STAGES;
+    constexpr int KC = CIN / 8;            // 16-byte chunks per operand row
+    constexpr int ACOLS = COUT < 32 ? 32 : COUT;
+    constexpr int TCOLS = 2 * ACOLS;
+    constexpr int NC = COUT * 4 / WS_EPI;  // accumulator columns per epilogue warp
+    constexpr uint32_t IDESC = instr_desc(TM, COUT);
+    static_assert((CIN == 64 || CIN == 16) && (COUT == 64 || COUT == 16), "shape");
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[NS], empty[NS], accf[2], acce[2];
+    __shared__ uint32_t tmem_slot;
+    __shared__ volatile int abort_flag;
+    __shared__ float sbias[COUT];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t a_base = (raw + 1023u) & ~1023u;  // swizzled operands need 1024-byte alignment
+    unsigned char* const sm = smem_raw + (a_base - raw);
+    const uint32_t b_base = a_base + NS * G::A_BYTES;
+    const uint32_t o_base = b_base + G::B_BYTES;
+    unsigned char* const so = sm + NS * G::A_BYTES + G::B_BYTES;
+    for (int i = tid; i < COUT; i += WS_THREADS) sbias[i] = bias ? bias[i] : 0.f;
+    // weights: the packed K-major image (8-element chunks (n, k8) at k8*COUT*8 + (n/8)*64 + (n%8)*8)
+    // into swizzled rows: tap k8 / KC, row n, chunk k8 % KC
+    for (int i = tid; i < COUT * 3 * KC; i += WS_THREADS) {
+        const int n = i % COUT, k8 = i / COUT;
+        const int tap = k8 / KC, c8 = k8 % KC;
+        const uint4 v = *reinterpret_cast<const uint4*>(wpk + (size_t)k8 * COUT * 8 + (n >> 3) * 64 + (n & 7) * 8);
+        *reinterpret_cast<uint4*>(sm + NS * G::A_BYTES + tap * G::B_TAP + (n >> 3) * G::SBO + (n & 7) * G::ROWB +
+                                  (G::chunk(c8, n) << 4)) = v;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                         smem_u32(&tmem_slot)),
+                     "r"(TCOLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        for (int i = 0; i < NS; ++i) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&full[i])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&empty[i])));
+        }
+        for (int i = 0; i < 2; ++i) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&accf[i])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&acce[i])), "n"(WS_EPI));
+        }
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // the weights, for the MMA
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    const int tiles_per_b = (T + TM - 1) / TM;
+    const int n_tiles = B * tiles_per_b;
+    const int nk = blockIdx.x < n_tiles ? (n_tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+
+    if (warp == WS_EPI) {
+        // ---------------- copy warp ----------------
+        if (lane == 0) {
+            int k = 0;
+            for (; k < nk && !abort_flag; ++k) {
+                const int s = k % NS;
+                if (k >= NS && !wait_parity(&empty[s], (uint32_t)((k / NS) - 1) & 1u, spin_limit)) {
+                    raise(err, EEMD_SG_E_TIMEOUT);
+                    abort_flag = 1;
+                    break;
+                }
+                const int tile = blockIdx.x + k * gridDim.x;
+                const int b = tile / tiles_per_b, t0 = (tile % tiles_per_b) * TM;
+                const uint32_t dst = a_base + s * G::A_BYTES;
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(&full[s])),
+                             "n"(G::A_BYTES)
+                             : "memory");
+#pragma unroll
+                for (int tap = 0; tap < 3; ++tap)
+                    asm volatile(
+                        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], "
+                        "[%1, {%2, %3, %4}], [%5];\n" ::"r"(dst + tap * G::TAP_BYTES),
+                        "l"(reinterpret_cast<uint64_t>(&tin)), "r"(0), "r"(t0 + dir * (tap - 1) * dil), "r"(b),
+                        "r"(smem_u32(&full[s]))
+                        : "memory");
+            }
+            // copies still in flight (only when a role gave up) land before the CTA leaves
+            for (int j = k - 1; j >= 0 && j >= k - NS; --j) wait_parity(&full[j % NS], (uint32_t)(j / NS) & 1u, spin_limit);
+        }
+    } else if (warp == WS_EPI + 1) {
+        // ---------------- MMA warp ----------------
+        if (lane == 0) {
+            int k = 0;
+            for (; k < nk && !abort_flag; ++k) {
+                const int s = k % NS, a = k & 1;
+                if (!wait_parity(&full[s], (uint32_t)(k / NS) & 1u, spin_limit) ||
+                    (k >= 2 && !wait_parity(&acce[a], (uint32_t)((k >> 1) - 1) & 1u, spin_limit))) {
+                    raise(err, EEMD_SG_E_TIMEOUT);
+                    abort_flag = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                const uint32_t a_buf = a_base + s * G::A_BYTES;
+#pragma unroll
+                for (int s2 = 0; s2 < 3 * CIN / 16; ++s2) {
+                    const int tap = s2 / (CIN / 16), kk = s2 % (CIN / 16);
+                    const uint64_t da = sw_desc(a_buf + tap * G::TAP_BYTES + kk * 32, G::SBO, G::LAYOUT);
+                    const uint64_t db = sw_desc(b_base + tap * G::B_TAP + kk * 32, G::SBO, G::LAYOUT);
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem + a * ACOLS),
+                        "l"(da), "l"(db), "r"(IDESC), "r"(s2 > 0 ? 1u : 0u));
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                                 smem_u32(&empty[s]))
+                             : "memory");
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                                 smem_u32(&accf[a]))
+                             : "memory");
+            }
+            // the issued MMAs are complete before the tensor memory is freed
+            if (k > 0) wait_parity(&accf[(k - 1) & 1], (uint32_t)((k - 1) >> 1) & 1u, spin_limit);
+        }
+    } else {
+        // ---------------- epilogue warps ----------------
+        const int quad = warp & 3, cb = (warp >> 2) * NC;
+        const int r = 32 * quad + lane;  // tile row of this lane
+        for (int k = 0; k < nk; ++k) {
+            const int a = k & 1;
+            const int tile = blockIdx.x + k * gridDim.x;
+            const int b = tile / tiles_per_b, t0 = (tile % tiles_per_b) * TM;
+            const bool ok = __all_sync(0xffffffffu, wait_parity(&accf[a], (uint32_t)(k >> 1) & 1u, spin_limit));
+            if (ok) {
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                float v[NC];
+                tmem_ld_cols<NC>(tmem + a * ACOLS + ((uint32_t)(32 * quad) << 16) + (uint32_t)cb, v);
+                asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&acce[a]);
+                const int t = t0 + r;
+                const __nv_bfloat16* mk = (mask && t < T) ? mask + ((size_t)b * T + t) * COUT + cb : nullptr;
+                unsigned char* const ob = so + (k & 1) * G::O_BYTES;
+#pragma unroll
+                for (int j = 0; j < NC / 8; ++j) {
+                    __align__(16) __nv_bfloat16 h[8];
+                    uint4 mv = make_uint4(0, 0, 0, 0);
+                    if (mk) mv = *reinterpret_cast<const uint4*>(mk + 8 * j);
+                    const __nv_bfloat16* mh = reinterpret_cast<const __nv_bfloat16*>(&mv);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        float x = v[8 * j + i] + sbias[cb + 8 * j + i];
+                        if (relu) x = fmaxf(x, 0.f);
+                        if (mask && !(__bfloat162float(mh[i]) > 0.f)) x = 0.f;
+                        h[i] = __float2bfloat16(x);
+                    }
+                    const int c = (cb >> 3) + j;  // 16-byte chunk of the output row
+                    const int off = COUT == 64 ? r * 128 + ((c ^ (r & 7)) << 4) : r * (COUT * 2) + (c << 4);
+                    *reinterpret_cast<uint4*>(ob + off) = *reinterpret_cast<const uint4*>(h);
+                }
+                asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            }
+            // the stores issued so far (tile k-1's) have read their staging buffer
+            // before tile k+1 overwrites it
+            if (tid == 0) asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+            __syncwarp();
+            if (epi_bar_or(!ok)) {
+                if (tid == 0) raise(err, EEMD_SG_E_TIMEOUT);
+                abort_flag = 1;
+                break;
+            }
+            if (tid == 0) {
+                asm volatile(
+                    "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];\n" ::"l"(
+                        reinterpret_cast<uint64_t>(&tout)),
+                    "r"(0), "r"(t0), "r"(b), "r"(o_base + (k & 1) * G::O_BYTES)
+                    : "memory");
+                asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+            }
+        }
+        if (tid == 0) asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+    }
+    __syncwarp();
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
+    }
+}
+
 // CUDA-core convolution with the same arguments (reference for the tensor-core path)
 __global__ void k_conv_ref(const __nv_bfloat16* __restrict__ in, const __nv_bfloat16* __restrict__ wpk,
                            const float* __restrict__ bias, __nv_bfloat16* out, int B, int T, int cin, int cout,
@@ -1179,7 +1444,8 @@ using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, 
                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-int input_map(CUtensorMap* m, const void* in, int B, int T, int CIN) {
+// 3-D tensor map of a bf16 [B][T][C] array with the box {box_c, 128, 1}
+int tensor_map3(CUtensorMap* m, const void* p, int B, int T, int C, int box_c, CUtensorMapSwizzle swz) {
     static EncodeTiled encode = nullptr;
     if (!encode) {
         void* fn = nullptr;
@@ -1189,15 +1455,20 @@ int input_map(CUtensorMap* m, const void* in, int B, int T, int CIN) {
             return EEMD_SG_E_CUDA;
         encode = reinterpret_cast<EncodeTiled>(fn);
     }
-    if ((reinterpret_cast<uintptr_t>(in) & 15) != 0) return EEMD_SG_E_BADARG;  // a tensor map needs 16-byte alignment
-    const cuuint64_t dims[3] = {(cuuint64_t)CIN, (cuuint64_t)T, (cuuint64_t)B};
-    const cuuint64_t strides[2] = {(cuuint64_t)CIN * 2, (cuuint64_t)T * CIN * 2};
-    const cuuint32_t box[3] = {8, (cuuint32_t)TM, 1};
+    if ((reinterpret_cast<uintptr_t>(p) & 15) != 0) return EEMD_SG_E_BADARG;  // a tensor map needs 16-byte alignment
+    const cuuint64_t dims[3] = {(cuuint64_t)C, (cuuint64_t)T, (cuuint64_t)B};
+    const cuuint64_t strides[2] = {(cuuint64_t)C * 2, (cuuint64_t)T * C * 2};
+    const cuuint32_t box[3] = {(cuuint32_t)box_c, (cuuint32_t)TM, 1};
     const cuuint32_t estr[3] = {1, 1, 1};
-    const CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(in), dims, strides, box, estr,
-                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    const CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(p), dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? EEMD_SG_OK : EEMD_SG_E_CUDA;
+}
+
+// the input of k_conv_tma: boxes of 8 channels (one K-major no-swizzle chunk column)
+int input_map(CUtensorMap* m, const void* in, int B, int T, int CIN) {
+    return tensor_map3(m, in, B, T, CIN, 8, CU_TENSOR_MAP_SWIZZLE_NONE);
 }
 
 template <int CIN, int COUT>
@@ -1231,6 +1502,38 @@ int launch_tma(const void* in, const void* wpk, const float* bias, void* out, in
     k_conv_tma<CIN, COUT, EW><<<grid, 32 * EW, smem, st>>>(m, static_cast<const __nv_bfloat16*>(wpk), bias,
                                                    static_cast<__nv_bfloat16*>(out), B, T, dil, dir, relu,
                                                    static_cast<const __nv_bfloat16*>(mask), err, spin);
+    return cudaGetLastError() == cudaSuccess ? EEMD_SG_OK : EEMD_SG_E_CUDA;
+}
+
+// the warp-specialised kernel: one CTA per SM, the input through a swizzled
+// tensor map (128-byte for 64 channels, 32-byte for 16), the output through a
+// 128-byte-swizzled one (no swizzle for 16 output channels, rows of 32 bytes)
+template <int CIN, int COUT>
+int launch_ws(const void* in, const void* wpk, const float* bias, void* out, int B, int T, int dil, int dir,
+              int relu, const void* mask, int* err, long long spin, cudaStream_t st) {
+    using G = WsGeo<CIN, COUT>;
+    const auto misaligned = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15) != 0; };
+    if (misaligned(wpk) || misaligned(out) || (mask && misaligned(mask))) return EEMD_SG_E_BADARG;
+    if (cudaFuncSetAttribute(k_conv_ws<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM) !=
+        cudaSuccess)
+        return EEMD_SG_E_CUDA;
+    CUtensorMap mi, mo;
+    int rc = tensor_map3(&mi, in, B, T, CIN, CIN, CIN == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_32B);
+    if (rc) return rc;
+    rc = tensor_map3(&mo, out, B, T, COUT, COUT, COUT == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE);
+    if (rc) return rc;
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            return EEMD_SG_E_CUDA;
+    }
+    const int tiles = B * ((T + TM - 1) / TM);
+    const int grid = tiles < sms ? tiles : sms;
+    k_conv_ws<CIN, COUT><<<grid, WS_THREADS, G::SMEM, st>>>(mi, mo, static_cast<const __nv_bfloat16*>(wpk), bias,
+                                                           B, T, dil, dir, relu,
+                                                           static_cast<const __nv_bfloat16*>(mask), err, spin);
     return cudaGetLastError() == cudaSuccess ? EEMD_SG_OK : EEMD_SG_E_CUDA;
 }
 
@@ -1331,7 +1634,13 @@ int32_t eemd_sg_conv(const void* in, const void* wpk, const float* bias, void* o
         return cudaGetLastError() == cudaSuccess ? EEMD_SG_OK : EEMD_SG_E_CUDA;
     }
     const long long spin = spin_limit > 0 ? spin_limit : (1LL << 24);
-    if (tensor_cores == 3) {
+    if (tensor_cores == 4) {
+        if (cin == 64 && cout == 64) return launch_ws<64, 64>(in, wpk, bias, out, B, T, dil, dir, relu, mask, err, spin, st);
+        if (cin == 16 && cout == 64) return launch_ws<16, 64>(in, wpk, bias, out, B, T, dil, dir, relu, mask, err, spin, st);
+        if (cin == 64 && cout == 16) return launch_ws<64, 16>(in, wpk, bias, out, B, T, dil, dir, relu, mask, err, spin, st);
+        return EEMD_SG_E_BADARG;
+    }
+    if (tensor_cores >= 3) {
         if (cin == 64 && cout == 64)
             return launch_tma<64, 64>(in, wpk, bias, out, B, T, dil, dir, relu, mask, err, spin, st);
         if (cin == 16 && cout == 64)

@@ -38,8 +38,11 @@ int32_t eemd_sg_version(void);
  * (the ReLU derivative).  tensor_cores = 1 runs the tcgen05 implicit GEMM,
  * 2 its double-buffered form (the next tile's copies and the previous tile's
  * epilogue overlap the MMA), 3 the double-buffered form fed by bulk-tensor
- * (TMA) copies of a 3-D tensor map over x (x must be 16-byte aligned); all
- * three give the same results bit for bit.  0 runs a CUDA-core reference
+ * (TMA) copies of a 3-D tensor map over x (x must be 16-byte aligned), 4
+ * a warp-specialised form: a copy warp, an MMA warp and eight epilogue warps
+ * on their own barriers, swizzled operands (one bulk-tensor box per tap) and
+ * bulk-tensor stores of y (x, y, the packed weights and mask 16-byte
+ * aligned); all four give the same results bit for bit.  0 runs a CUDA-core reference
  * kernel with identical semantics.  *err (device,
  * may be null) receives EEMD_SG_E_TIMEOUT if a tensor-core wait gives up
  * after spin_limit polls (0: default). */

@@ -77,10 +77,12 @@ def test_spectra_of_imfs_48k_against_the_oracle():
         assert np.max(np.abs(Z[r] - oZ)) <= 1e-11 * np.max(np.abs(oZ))
 
 
-@pytest.mark.parametrize("N", [1, 2, 3, 5, 8, 30, 37, 100, 1001, 2048, 4097, 48000, 65536])
+@pytest.mark.parametrize("N", [1, 2, 3, 5, 8, 30, 37, 100, 1001, 2048, 4097, 6144, 7168, 48000, 65536])
 def test_own_fft_against_numpy(N):
     """eemd_sp_fft (Stockham radix 4/2/3/5/odd primes <= 31, Bluestein for
-    larger primes: 37, 4097 = 17 x 241) against numpy.fft on 3 rows, both signs."""
+    larger primes: 37, 4097 = 17 x 241) against numpy.fft on 3 rows, both signs;
+    lengths up to 4096 run as one shared-memory launch per row (37's Bluestein
+    transforms of 128 too), longer ones as global passes."""
     from eemd4cuda_b200 import _sp
     rng = np.random.default_rng(N)
     x = rng.standard_normal((3, N)) + 1j * rng.standard_normal((3, N))
@@ -91,3 +93,18 @@ def test_own_fft_against_numpy(N):
     b = _sp.fft_device(z, +1).cpu().numpy()
     refb = np.fft.ifft(x, axis=1) * N
     assert np.max(np.abs(b - refb)) <= 1e-13 * max(1.0, np.max(np.abs(refb)))
+
+
+@pytest.mark.parametrize("nper", [256, 1000, 4096, 8192])
+def test_stft_frame_lengths_against_oracle(nper):
+    """The STFT's one-launch shared-memory form (frames of up to 4096 samples
+    with radix 4/2/3/5 factors) and its global-pass form (8192) against the
+    oracle's restatement of the reference's scipy call."""
+    rng = np.random.default_rng(nper)
+    sr, N = 48000, 20000
+    X = rng.standard_normal((2, N))
+    f, t, Z = spectra.stft_block(X, sr, nperseg=nper)
+    for r in range(2):
+        of, ot, oZ = SP.stft(X[r], sr, nper)
+        assert np.allclose(f, of) and np.allclose(t, ot)
+        assert np.max(np.abs(Z[r] - oZ)) <= 1e-11 * np.max(np.abs(oZ))

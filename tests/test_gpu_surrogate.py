@@ -134,9 +134,11 @@ def test_loss_and_adam():
 @pytest.mark.parametrize("dil", [1, 13, 128])
 def test_double_buffered_kernels_equal_single_buffered(cin, cout, dil):
     """tensor_cores=2 (two input buffers and accumulators, epilogue of tile
-    k-1 overlapping MMA k) and 3 (the same fed by bulk-tensor copies) against
-    tensor_cores=1, forward and masked input gradient, with more tiles than
-    CTAs, a ragged last tile and halo rows outside the signal."""
+    k-1 overlapping MMA k), 3 (the same fed by bulk-tensor copies) and 4
+    (warp-specialised, swizzled operands, bulk-tensor stores) against
+    tensor_cores=1, forward and
+    masked input gradient, with more tiles than CTAs, a ragged last tile and
+    halo rows outside the signal."""
     rng = np.random.default_rng(100 + cin + cout + dil)
     B, T = 8, 10000
     x = rng.standard_normal((B, T, cin)).astype(np.float32)
@@ -146,23 +148,46 @@ def test_double_buffered_kernels_equal_single_buffered(cin, cout, dil):
     wp = packed(w, cout, cin)
     err = torch.zeros((1,), dtype=torch.int32, device="cuda")
     ys = []
-    for mode in (1, 2, 3):
+    for mode in (1, 2, 3, 4):
         y = torch.full((B, T, cout), 7.0, dtype=torch.bfloat16, device="cuda")
         _sg.conv(xd, wp, bd, y, B, T, cin, cout, dil, relu=True, tensor_cores=mode, err=err)
         ys.append(y)
     torch.cuda.synchronize()
     assert int(err.item()) == 0
-    assert torch.equal(ys[0], ys[1]) and torch.equal(ys[0], ys[2])
+    assert all(torch.equal(ys[0], y) for y in ys[1:])
     # masked input gradient
     dy = rng.standard_normal((B, T, cout)).astype(np.float32)
     mask = (rng.random((B, T, cin)) > 0.3).astype(np.float32)
     wpt = packed(w, cin, cout, transpose=True)
     gs = []
-    for mode in (1, 2, 3):
+    for mode in (1, 2, 3, 4):
         g = torch.full((B, T, cin), 7.0, dtype=torch.bfloat16, device="cuda")
         _sg.conv(bf16(dy).cuda(), wpt, None, g, B, T, cout, cin, dil, direction=-1, mask=bf16(mask).cuda(),
                  tensor_cores=mode, err=err)
         gs.append(g)
     torch.cuda.synchronize()
     assert int(err.item()) == 0
-    assert torch.equal(gs[0], gs[1]) and torch.equal(gs[0], gs[2])
+    assert all(torch.equal(gs[0], g) for g in gs[1:])
+
+
+@pytest.mark.parametrize("cin,cout", [(64, 64), (64, 16), (16, 64)])
+@pytest.mark.parametrize("dil", [1, 64])
+def test_warp_specialised_conv_over_many_tiles(cin, cout, dil):
+    """tensor_cores=4 over 16 x 65536 samples (55 or 56 tiles per CTA: every
+    input stage and accumulator reused many times) equals tensor_cores=3."""
+    rng = np.random.default_rng(500 + cin + cout + dil)
+    B, T = 16, 65536
+    xd = (torch.randn((B, T, cin), generator=torch.Generator().manual_seed(cin + cout + dil)) * 0.5).to(
+        torch.bfloat16).cuda()
+    w = (rng.standard_normal((cout, 3, cin)) / np.sqrt(3 * cin)).astype(np.float32)
+    bd = torch.from_numpy(rng.standard_normal(cout).astype(np.float32)).cuda()
+    wp = packed(w, cout, cin)
+    err = torch.zeros((1,), dtype=torch.int32, device="cuda")
+    ys = []
+    for mode in (3, 4):
+        y = torch.full((B, T, cout), 7.0, dtype=torch.bfloat16, device="cuda")
+        _sg.conv(xd, wp, bd, y, B, T, cin, cout, dil, relu=True, tensor_cores=mode, err=err)
+        ys.append(y)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    assert torch.equal(ys[0], ys[1])
