@@ -221,6 +221,18 @@ _STAGE = {}
 _STAGE_LOCK = threading.Lock()
 
 
+# results up to this size come back in pinned host tensors of their own from
+# torch's caching host allocator: the device-to-host copies land in memory
+# that is already paged in, and the returned arrays are views of it (they keep
+# the tensor, and so the block, alive); larger results go through the shared
+# staging buffers into fresh arrays
+PINNED_RESULT_BYTES = 64 << 20
+
+
+def _pinned(torch, shape, dtype):
+    return torch.empty(shape, dtype=dtype, pin_memory=True)
+
+
 def _staging(torch, slots, N):
     """Pinned host buffers for the outputs of one shape (the latest shape only is kept)."""
     key = (slots, N)
@@ -351,16 +363,29 @@ def _run_ensemble(x, *, E, eps, tau, max_sifts, max_imf, min_extrema, end, seed,
     n_modes_d = torch.empty((1,), dtype=torch.int32, device=dev)
     with nvtx.range("eemd.finalize"):
         L.finalize(p, xd, [N], imf_sum, mode_count, imf_mean, resid, n_modes_d)
-    # all outputs through pinned staging with one synchronisation
-    with _STAGE_LOCK, nvtx.range("eemd.download"):  # callers on several threads share the buffers
-        h_mean, h_resid, h_n = _staging(torch, slots, N)
-        h_mean.copy_(imf_mean, non_blocking=True)
-        h_resid.copy_(resid, non_blocking=True)
-        h_n.copy_(n_modes_d, non_blocking=True)
-        ch = cnt.cpu()  # synchronises the stream: every copy above has landed
-        n_modes = int(h_n[0])
-        imfs = fresh_copy(h_mean[:n_modes].numpy())
-        residual = h_resid.numpy().copy()
+    # all outputs through pinned memory with one synchronisation
+    if slots * N * 8 <= PINNED_RESULT_BYTES:
+        with nvtx.range("eemd.download"):
+            h_mean, h_resid = _pinned(torch, (slots, N), torch.float64), _pinned(torch, (N,), torch.float64)
+            h_n, ch = _pinned(torch, (1,), torch.int32), _pinned(torch, (3, E), torch.int32)
+            h_mean.copy_(imf_mean, non_blocking=True)
+            h_resid.copy_(resid, non_blocking=True)
+            h_n.copy_(n_modes_d, non_blocking=True)
+            ch.copy_(cnt, non_blocking=True)
+            torch.cuda.current_stream(dev).synchronize()
+            n_modes = int(h_n[0])
+            imfs = h_mean[:n_modes].numpy()
+            residual = h_resid.numpy()
+    else:
+        with _STAGE_LOCK, nvtx.range("eemd.download"):  # callers on several threads share the buffers
+            h_mean, h_resid, h_n = _staging(torch, slots, N)
+            h_mean.copy_(imf_mean, non_blocking=True)
+            h_resid.copy_(resid, non_blocking=True)
+            h_n.copy_(n_modes_d, non_blocking=True)
+            ch = cnt.cpu()  # synchronises the stream: every copy above has landed
+            n_modes = int(h_n[0])
+            imfs = fresh_copy(h_mean[:n_modes].numpy())
+            residual = h_resid.numpy().copy()
     per_trial_sifts, per_trial_modes, flags_all = ch[0].tolist(), ch[1].tolist(), ch[2].tolist()
     if ck is not None:
         ck.remove()
@@ -398,13 +423,23 @@ def _run_single(x, *, tau, max_sifts, max_imf, min_extrema, end, rules, exact, d
     t0 = time.time()
     L.run(p, xd, [N], 0, 1, ws, imfs=imfs, resid_out=resid, nsift=nsift, nmode=nmode,
           mode_sifts=msifts, flags=flags)
-    nm = int(nmode.item())
-    out = imfs[0, :nm].to(torch.float64).cpu().numpy()
-    res = resid[0].to(torch.float64).cpu().numpy()
-    per_mode = msifts[0, :nm].cpu().tolist()
-    stats = dict(method="gpu", backend="b200", E=1, n_modes=nm, total_sifts=int(nsift.item()),
-                 per_mode_sifts=per_mode, per_trial_total_sifts=np.array([int(nsift.item())]),
-                 max_imf_reached=bool(int(flags.item()) & 1 and max_imf == -1),
+    # every output into pinned memory, one synchronisation
+    h_imfs, h_res = _pinned(torch, (slots, N), torch.float64), _pinned(torch, (N,), torch.float64)
+    h_cnt = _pinned(torch, (3 + slots,), torch.int32)
+    h_imfs.copy_(imfs[0].to(torch.float64), non_blocking=True)
+    h_res.copy_(resid[0].to(torch.float64), non_blocking=True)
+    h_cnt[0:1].copy_(nsift, non_blocking=True)
+    h_cnt[1:2].copy_(nmode, non_blocking=True)
+    h_cnt[2:3].copy_(flags, non_blocking=True)
+    h_cnt[3:].copy_(msifts[0], non_blocking=True)
+    torch.cuda.current_stream(dev).synchronize()
+    c = h_cnt.tolist()
+    nm = int(c[1])
+    out = h_imfs[:nm].numpy()
+    res = h_res.numpy()
+    stats = dict(method="gpu", backend="b200", E=1, n_modes=nm, total_sifts=int(c[0]),
+                 per_mode_sifts=[int(v) for v in c[3:3 + nm]], per_trial_total_sifts=np.array([int(c[0])]),
+                 max_imf_reached=bool(int(c[2]) & 1 and max_imf == -1),
                  gpu_time_s=time.time() - t0, x=np.asarray(x, dtype=float))
     return out, res, stats
 

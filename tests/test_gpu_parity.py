@@ -347,3 +347,19 @@ def test_launch_shapes_give_identical_results(cta_warps, cluster):
     assert np.array_equal(other["knot_log"], base["knot_log"])
     for a, b in zip(other["imfs"], base["imfs"]):
         assert np.array_equal(a, b)
+
+
+def test_results_stay_valid_across_calls():
+    """decompose returns its IMFs and residual as views of pinned host memory
+    of that call: a later call (same shape, and a different one) leaves an
+    earlier result untouched, plain EMD and EEMD alike."""
+    x1 = signals.harmonic_clicks(12000, seed=5)
+    x2 = signals.harmonic_clicks(12000, seed=6)
+    for kw in (dict(E=1, tau=0.25, max_sifts=20), dict(E=4, tau=0.25, max_sifts=20, seed=3)):
+        r1 = M.decompose(x1, **kw)
+        keep = (r1.imfs.copy(), r1.residual.copy())
+        r2 = M.decompose(x2, **kw)
+        r3 = M.decompose(signals.plain_emd_8k(), **kw)
+        assert np.array_equal(r1.imfs, keep[0]) and np.array_equal(r1.residual, keep[1])
+        assert r2.imfs.shape[1] == 12000 and r3.imfs.shape[1] == 8192
+        assert np.allclose(r1.imfs.sum(axis=0) + r1.residual, x1, atol=1e-9)
