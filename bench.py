@@ -1218,37 +1218,61 @@ SMEM_FFT_MAX = 4096  # longest row libeemd_spectra.so transforms in one shared-m
 CONV_KERNEL_NAMES = {1: "k_conv_tc", 2: "k_conv_tc2", 3: "k_conv_tma", 4: "k_conv_ws"}
 
 
+def _fft_radices(m: int):
+    """(factors, fully factored) of m over 4, 2 and the odd primes up to 31."""
+    k = 0
+    for q in (4, 2, *range(3, 32, 2)):
+        while m % q == 0:
+            m //= q
+            k += 1
+    return k, m == 1
+
+
+def fft4_split(n: int):
+    """The four-step split (N1, N2) libeemd_spectra.so uses for a length above
+    4096: N1 the divisor nearest below sqrt(n) with both factors direct
+    lengths up to 4096; None when there is none."""
+    if n <= SMEM_FFT_MAX or n > SMEM_FFT_MAX * SMEM_FFT_MAX:
+        return None
+    n1 = 1
+    while (n1 + 1) * (n1 + 1) <= n:
+        n1 += 1
+    for d in range(n1, 1, -1):
+        if n % d:
+            continue
+        if n // d > SMEM_FFT_MAX:
+            break
+        if _fft_radices(d)[1] and _fft_radices(n // d)[1]:
+            return d, n // d
+    return None
+
+
 def fft_passes(n: int) -> int:
     """Kernel launches of one FFT of length n in libeemd_spectra.so: one
-    launch for a length up to 4096 whose factors are 4, 2 and odd primes up
-    to 31, else one Stockham pass per such factor, or for a length with a
-    larger prime factor Bluestein's 2 + 3 power-of-two transforms + 2."""
-    def radices(m):
-        k = 0
-        for q in (4, 2, *range(3, 32, 2)):
-            while m % q == 0:
-                m //= q
-                k += 1
-        return k, m == 1
-
-    def direct(m):
-        k = radices(m)[0]
-        return 1 if m <= SMEM_FFT_MAX else max(k, 1)
-    if radices(n)[1]:
-        return direct(n)
+    shared-memory launch up to 4096, two for the four-step split above it,
+    else one Stockham pass per factor (4s, 2s, odd primes up to 31); a length
+    with a larger prime factor runs Bluestein's 2 + 3 power-of-two transforms
+    + 2."""
+    k, direct = _fft_radices(n)
+    if direct:
+        if n <= SMEM_FFT_MAX:
+            return 1
+        return 2 if fft4_split(n) else max(k, 1)
     L = 1
     while L < 2 * n - 1:
         L <<= 1
-    return 4 + 3 * direct(L)
+    return 4 + 3 * fft_passes(L)
 
 
 def spectra_launches(n: int, nperseg: int) -> int:
     """Launches of the spectra step: two STFT calls (one launch each when the
-    frame transform fits one shared-memory launch, else k_frames, the frame
-    FFT and k_stft_out) and one Hilbert call (k_promote, FFT, k_analytic,
-    inverse FFT, k_if_amp)."""
-    stft = 1 if fft_passes(nperseg) == 1 and nperseg <= SMEM_FFT_MAX else 2 + fft_passes(nperseg)
-    return 2 * stft + 3 + 2 * fft_passes(n)
+    frames are direct lengths up to 4096, else k_frames, the frame FFT and
+    k_stft_out) and one Hilbert call (two four-step transforms with the real
+    input and the analytic weights in their loads, then k_if_amp; else
+    k_promote, FFT, k_analytic, inverse FFT, k_if_amp)."""
+    stft = 1 if nperseg <= SMEM_FFT_MAX and _fft_radices(nperseg)[1] else 2 + fft_passes(nperseg)
+    hilbert = 5 if _fft_radices(n)[1] and fft4_split(n) else 3 + 2 * fft_passes(n)
+    return 2 * stft + hilbert
 
 
 def run_spectra(args):
@@ -1341,8 +1365,8 @@ def run_spectra(args):
                 "h2d_bytes_per_step": rows * N * 8 + r.n_modes * N * 8,
                 "d2h_bytes_per_step": rows * F * T * 16 + 2 * r.n_modes * N * 8},
         "gpu_launches": spectra_launches(N, nper) * args.steps,
-        "roofline": {"bound": "hbm", "kernel": "hilbert stage (k_promote, FFT passes, k_analytic, inverse FFT "
-                                               "passes, k_if_amp)",
+        "roofline": {"bound": "hbm", "kernel": "hilbert stage (four-step FFT with the real input in its loads, "
+                                               "inverse four-step FFT with the analytic weights, k_if_amp)",
                      "achieved": round(gbs, 2), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": round(gbs / peak, 4), "traffic": None, "algorithmic_bytes": h_bytes,
                      "ms": round(h_ms, 4)},

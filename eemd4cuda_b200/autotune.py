@@ -1,8 +1,8 @@
 """Threads per trial and block size, tuned per signal-length bucket and task count.
 
 The engine spreads one (signal, trial) task over a thread-block cluster of C
-CTAs of W warps (C x W x 32 threads per trial; W = 4 or 5, four or three
-CTAs per SM).  The best (C, W) depends on the signal length (how much work
+CTAs of W warps (C x W x 32 threads per trial; W = 4 or 5; float32 storage
+runs four or three CTAs per SM, float64 three).  The best (C, W) depends on the signal length (how much work
 one CTA's segment holds) and on how many tasks share the launch (how many of
 the B200's CTA slots each task can have).  `tune()` measures the persistent
 kernel for every (length bucket, task count, W, C) on synthetic signals of

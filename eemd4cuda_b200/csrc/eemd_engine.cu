@@ -1517,7 +1517,7 @@ __device__ void step_setup(const Ctx& C, const Slot& sl, TaskSm& S) {
 // k_emd: the persistent cluster kernel
 // ---------------------------------------------------------------------------
 template <typename T, bool EXACT, int NW>
-__global__ void __launch_bounds__(32 * NW, ctas_per_sm(NW)) k_emd(const __grid_constant__ Ctx C) {
+__global__ void __launch_bounds__(32 * NW, ctas_per_sm(NW, (int)sizeof(T))) k_emd(const __grid_constant__ Ctx C) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ TaskSm S;
     __shared__ Xchg X[2];
@@ -1790,7 +1790,7 @@ int autotune_csize(int64_t n_tasks, int64_t nmin, int dtype, bool exact, int nw)
     // wave.  Signals of a million samples or more take every slot: each CTA
     // then sweeps long ranges, and measured on 64 trials of 2^22 samples 8
     // CTAs per signal (512 CTAs) run 10 % faster than 7.
-    const int64_t slots = (int64_t)ASSUMED_SMS * ctas_per_sm(nw);
+    const int64_t slots = (int64_t)ASSUMED_SMS * ctas_per_sm(nw, dtype == EEMD_F64 ? 8 : 4);
     const int64_t budget = nmin >= (1 << 20) ? slots : slots * 4 / 5;
     int c = (int)std::max<int64_t>(1, std::min<int64_t>(8, budget / std::max<int64_t>(n_tasks, 1)));
     // more tasks than slots: pairs of CTAs halve each task's time and with it
@@ -1908,7 +1908,8 @@ int make_layout(const eemd_params* p, const int64_t* lengths, int n_signals, int
     L.slot_n = (nmax + 3) / 4 * 4;
     L.slot_runs = (nmax + run - 1) / run + 1;
     L.slots = (int)std::max<int64_t>(
-        1, std::min<int64_t>(n_tasks, (int64_t)ASSUMED_SMS * ctas_per_sm(L.nw) / L.csize));
+        1, std::min<int64_t>(n_tasks, (int64_t)ASSUMED_SMS * ctas_per_sm(L.nw, p->dtype == EEMD_F64 ? 8 : 4) /
+                                     L.csize));
     L.slot_knots = (int64_t)2 * 2 * L.csize * L.nw * L.segcap;
     L.slot_M = (int64_t)2 * L.kcap * rs;
     L.scr_rows = p->exact ? (L.B + L.S) : 0;

@@ -32,11 +32,14 @@
 namespace eemd {
 
 // warps per CTA of k_emd: 4 (the default) or 5, chosen per launch (the
-// autotune table's choice per length bucket); CTAs of 128 registers per
-// thread fill an SM at 16 warps: 4 CTAs of 4 warps, 3 of 5
+// autotune table's choice per length bucket).  CTAs per SM (the launch
+// bound, and with it the registers per thread): float32 storage 4 CTAs of 4
+// warps or 3 of 5 (128 registers); float64 storage 3 CTAs of either (168
+// registers for 4 warps: at 4 CTAs the float64 build spilled 200 bytes per
+// thread)
 constexpr int NW_DEFAULT = 4;
 constexpr int MAXNW = 5;
-__host__ __device__ constexpr int ctas_per_sm(int nw) { return 16 / nw; }
+__host__ __device__ constexpr int ctas_per_sm(int nw, int bt) { return bt == 8 ? 3 : 16 / nw; }
 // largest cluster: portable clusters reach 8 CTAs; 9 to 16 are non-portable
 // and are taken only when the device reports that all of them fit at once
 constexpr int MAXC = 16;

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "../../include/eemd_spectra.h"
@@ -320,16 +321,20 @@ __device__ void smem_twiddles(double2* tab, int n) {
     }
 }
 
-// the passes over a[0..n) (b: the other buffer, tab: the twiddle table);
-// returns the buffer holding the result
-__device__ double2* smem_stockham(double2* a, double2* b, const double2* tab, const SmemPlan& P, int sign) {
+// the passes over `rows` rows of n at a stride of ld elements in a (b: the
+// other buffer, tab: the twiddle table); returns the buffer holding the result
+__device__ double2* smem_stockham(double2* a, double2* b, const double2* tab, const SmemPlan& P, int sign,
+                                  int rows = 1, int ld = 0) {
     double2* cur = a;
     double2* dst = b;
     const TwTable tw{tab, P.n};
     int Ns = 1;
     for (int s = 0; s < P.nrad; ++s) {
         const int r = P.rad[s], nb = P.n / r;
-        for (int j = threadIdx.x; j < nb; j += blockDim.x) bfly_any(cur, dst, j, nb, Ns, r, sign, tw);
+        for (int j = threadIdx.x; j < rows * nb; j += blockDim.x) {
+            const int row = j / nb, jj = j - row * nb;
+            bfly_any(cur + row * ld, dst + row * ld, jj, nb, Ns, r, sign, tw);
+        }
         __syncthreads();
         Ns *= r;
         double2* t = cur;
@@ -386,6 +391,115 @@ __global__ void __launch_bounds__(SMEM_FFT_THREADS) k_stft_smem(const double* __
         __syncthreads();
     }
 }
+
+// ---------------------------------------------------------------------------
+// Rows longer than SMEM_FFT_MAX whose length splits as N = N1 N2 with both
+// factors direct shared-memory lengths: the four-step transform (Bailey),
+//     X[k1 + N1 k2] = sum_n2 W_N2^(n2 k2) W_N^(n2 k1) sum_n1 x[n1 N2 + n2] W_N1^(n1 k1),
+// in two launches with the transposes folded into their loads and stores:
+// k_fft4_cols transforms CB columns n2 of x (viewed as N1 x N2) per CTA
+// iteration, multiplies by the twiddles W_N^(n2 k1) and writes Y[k1][n2];
+// k_fft4_rows transforms KB rows k1 of Y and writes X[k1 + N1 k2].  Shared-
+// memory rows are padded by one element (ld = n + 1) so that column-wise
+// accesses spread over the banks.  The column kernel's load can promote real
+// rows (the Hilbert transform's input) or apply the analytic-signal weights
+// to a spectrum (its inverse transform), so those need no pass of their own.
+// ---------------------------------------------------------------------------
+// small CTAs with a few rows each, so that 8 rows of 48 000 give several
+// hundred CTAs (with 96 KB per CTA they were 128 and 136: SMs stayed idle)
+constexpr int FFT4_THREADS = 128;
+constexpr size_t FFT4_SMEM = 24 * 1024;  // two padded buffers of the CTA's rows
+
+struct Fft4Plan {
+    SmemPlan p1, p2;  // column (N1) and row (N2) transforms
+    int64_t n;        // N1 N2
+    int cb, kb;       // columns / rows per CTA iteration
+};
+
+enum { LOAD_COMPLEX = 0, LOAD_REAL = 1, LOAD_ANALYTIC = 2 };
+
+// element idx of row m of the column kernel's input
+template <int LOAD>
+__device__ __forceinline__ double2 fft4_load(const void* in, int64_t m, int64_t N, int64_t idx) {
+    if constexpr (LOAD == LOAD_REAL) {
+        return make_double2(static_cast<const double*>(in)[m * N + idx], 0.0);
+    } else if constexpr (LOAD == LOAD_ANALYTIC) {
+        // k_analytic's weights and scaling
+        const int64_t k = idx;
+        double w;
+        if (k == 0) w = 1.0;
+        else if ((N & 1) == 0 && k == N / 2) w = 1.0;
+        else if (2 * k < N) w = 2.0;
+        else w = 0.0;
+        if (w == 0.0) return make_double2(0.0, 0.0);
+        const double inv = 1.0 / (double)N;
+        const double2 X = static_cast<const double2*>(in)[m * N + idx];
+        return make_double2(X.x * w * inv, X.y * w * inv);
+    } else {
+        return static_cast<const double2*>(in)[m * N + idx];
+    }
+}
+
+template <int LOAD>
+__global__ void __launch_bounds__(FFT4_THREADS) k_fft4_cols(const void* __restrict__ in, double2* Y, int M,
+                                                            const __grid_constant__ Fft4Plan F, int sign) {
+    extern __shared__ double2 s4[];
+    const int N1 = F.p1.n, N2 = F.p2.n, CB = F.cb, ld = N1 + 1;
+    const int64_t N = F.n;
+    double2* a = s4;
+    double2* b = s4 + CB * ld;
+    double2* tab = s4 + 2 * CB * ld;
+    smem_twiddles(tab, N1);
+    const int nblk = (N2 + CB - 1) / CB;
+    for (int64_t blk = blockIdx.x; blk < (int64_t)M * nblk; blk += gridDim.x) {
+        const int64_t m = blk / nblk;
+        const int c0 = (int)(blk % nblk) * CB;
+        const int cb = min(CB, N2 - c0);
+        for (int i = threadIdx.x; i < N1 * CB; i += blockDim.x) {
+            const int n1 = i / CB, c = i - n1 * CB;
+            a[c * ld + n1] = c < cb ? fft4_load<LOAD>(in, m, N, (int64_t)n1 * N2 + c0 + c) : make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+        const double2* r = smem_stockham(a, b, tab, F.p1, sign, CB, ld);
+        for (int i = threadIdx.x; i < N1 * CB; i += blockDim.x) {
+            const int k1 = i / CB, c = i - k1 * CB;
+            if (c < cb) {
+                const int64_t n2 = c0 + c;
+                Y[m * N + (int64_t)k1 * N2 + n2] = cmul(r[c * ld + k1], twiddle(n2 * k1, N, sign));
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(FFT4_THREADS) k_fft4_rows(const double2* __restrict__ Y, double2* X, int M,
+                                                            const __grid_constant__ Fft4Plan F, int sign) {
+    extern __shared__ double2 s4[];
+    const int N1 = F.p1.n, N2 = F.p2.n, KB = F.kb, ld = N2 + 1;
+    const int64_t N = F.n;
+    double2* a = s4;
+    double2* b = s4 + KB * ld;
+    double2* tab = s4 + 2 * KB * ld;
+    smem_twiddles(tab, N2);
+    const int nblk = (N1 + KB - 1) / KB;
+    for (int64_t blk = blockIdx.x; blk < (int64_t)M * nblk; blk += gridDim.x) {
+        const int64_t m = blk / nblk;
+        const int k0 = (int)(blk % nblk) * KB;
+        const int kb = min(KB, N1 - k0);
+        for (int i = threadIdx.x; i < KB * N2; i += blockDim.x) {
+            const int kk = i / N2, n2 = i - kk * N2;
+            a[kk * ld + n2] = kk < kb ? Y[m * N + (int64_t)(k0 + kk) * N2 + n2] : make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+        const double2* r = smem_stockham(a, b, tab, F.p2, sign, KB, ld);
+        for (int i = threadIdx.x; i < KB * N2; i += blockDim.x) {
+            const int k2 = i / KB, kk = i - k2 * KB;
+            if (kk < kb) X[m * N + k0 + kk + (int64_t)N1 * k2] = r[kk * ld + k2];
+        }
+        __syncthreads();
+    }
+}
+
 
 // Bluestein: chirp c_n = exp(sign pi i n^2 / N) (n^2 reduced mod 2N exactly)
 __device__ __forceinline__ double2 chirp(int64_t n, int64_t N, int sign) {
@@ -483,6 +597,54 @@ bool smem_ready(const void* fn) {
 
 unsigned smem_grid(int64_t rows) { return (unsigned)(rows < 65535 ? rows : 65535); }
 
+// the four-step split of a length: N1 the divisor nearest below sqrt(n) with
+// both N1 and n / N1 direct shared-memory lengths; false when there is none
+bool fft4_plan(int64_t n, Fft4Plan& F) {
+    if (n <= SMEM_FFT_MAX || n > (int64_t)SMEM_FFT_MAX * SMEM_FFT_MAX) return false;
+    int64_t n1 = 1;
+    while ((n1 + 1) * (n1 + 1) <= n) ++n1;
+    for (; n1 >= 2; --n1) {
+        if (n % n1) continue;
+        const int64_t n2 = n / n1;
+        if (n2 > SMEM_FFT_MAX) break;  // n2 only grows as n1 shrinks
+        std::vector<int> r1, r2;
+        if (!factor(n1, r1) || !factor(n2, r2) || !smem_plan(n1, r1, F.p1) || !smem_plan(n2, r2, F.p2)) continue;
+        F.n = n;
+        F.cb = (int)std::max<size_t>(1, FFT4_SMEM / (2 * (size_t)(n1 + 1) * sizeof(double2)));
+        F.kb = (int)std::max<size_t>(1, FFT4_SMEM / (2 * (size_t)(n2 + 1) * sizeof(double2)));
+        F.cb = (int)std::min<int64_t>(F.cb, n2);
+        F.kb = (int)std::min<int64_t>(F.kb, n1);
+        return true;
+    }
+    return false;
+}
+
+size_t fft4_cols_smem(const Fft4Plan& F) { return (2 * (size_t)F.cb * (F.p1.n + 1) + F.p1.n) * sizeof(double2); }
+size_t fft4_rows_smem(const Fft4Plan& F) { return (2 * (size_t)F.kb * (F.p2.n + 1) + F.p2.n) * sizeof(double2); }
+
+// largest shared memory a four-step launch asks for: one padded row of 4096
+// in each buffer and its table
+constexpr int FFT4_SMEM_MAX = (2 * (SMEM_FFT_MAX + 1) + SMEM_FFT_MAX) * (int)sizeof(double2);
+
+bool fft4_ready() {
+    const void* fns[] = {reinterpret_cast<const void*>(k_fft4_cols<LOAD_COMPLEX>),
+                         reinterpret_cast<const void*>(k_fft4_cols<LOAD_REAL>),
+                         reinterpret_cast<const void*>(k_fft4_cols<LOAD_ANALYTIC>),
+                         reinterpret_cast<const void*>(k_fft4_rows)};
+    for (const void* fn : fns)
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, FFT4_SMEM_MAX) != cudaSuccess)
+            return false;
+    return true;
+}
+
+// the two launches of a four-step transform of M rows: in -> y (columns), y -> out (rows)
+template <int LOAD>
+void fft4(const void* in, double2* y, double2* out, int M, const Fft4Plan& F, int sign, cudaStream_t st) {
+    const int64_t nc = (int64_t)M * ((F.p2.n + F.cb - 1) / F.cb), nr = (int64_t)M * ((F.p1.n + F.kb - 1) / F.kb);
+    k_fft4_cols<LOAD><<<smem_grid(nc), FFT4_THREADS, fft4_cols_smem(F), st>>>(in, y, M, F, sign);
+    k_fft4_rows<<<smem_grid(nr), FFT4_THREADS, fft4_rows_smem(F), st>>>(y, out, M, F, sign);
+}
+
 // Stockham passes of length len over M rows: src -> (b1, b2 alternately); returns the result buffer
 double2* stockham(const double2* src, double2* b1, double2* b2, int M, int64_t len, const std::vector<int>& rad,
                   int sign, cudaStream_t st) {
@@ -498,6 +660,13 @@ double2* stockham(const double2* src, double2* b1, double2* b2, int M, int64_t l
     if (smem_ok && smem_plan(len, rad, sp)) {
         k_fft_smem<<<smem_grid(M), SMEM_FFT_THREADS, 3 * sp.n * sizeof(double2), st>>>(src, b1, M, sp, sign);
         return b1;
+    }
+    Fft4Plan f4;
+    static const bool f4_ok = fft4_ready();
+    if (f4_ok && fft4_plan(len, f4)) {
+        // src -> b1 (columns), b1 -> b2 (rows): b2 may be src, which only the first launch reads
+        fft4<LOAD_COMPLEX>(src, b1, b2, M, f4, sign, st);
+        return b2;
     }
     for (int r : rad) {
         const unsigned g = grid_for((int64_t)M * (len / r));
@@ -626,6 +795,15 @@ int32_t eemd_sp_hilbert_if(const double* x, int32_t M, int64_t N, double sr, dou
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const Bufs b = carve(ws, L);
     const int64_t total = (int64_t)M * N;
+    Fft4Plan f4;
+    static const bool f4_ok = fft4_ready();
+    if (f4_ok && !L.P.L && fft4_plan(N, f4)) {
+        // four-step transforms with the real input and the analytic weights folded into their loads
+        fft4<LOAD_REAL>(x, b.y, b.x, M, f4, -1, st);
+        fft4<LOAD_ANALYTIC>(b.x, b.y, b.z, M, f4, +1, st);
+        k_if_amp<<<grid_for(total), 256, 0, st>>>(b.z, inst_freq, inst_amp, M, N, sr);
+        return cudaGetLastError() == cudaSuccess ? EEMD_SP_OK : EEMD_SP_E_CUDA;
+    }
     // the caller's rows stay untouched: the transform runs on complex copies
     k_promote<<<grid_for(total), 256, 0, st>>>(x, b.x, total);
     double2* spec = fft_rows(b.x, b.y, b.z, b.extra, M, L.P, -1, st);

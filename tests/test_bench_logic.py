@@ -40,14 +40,19 @@ def test_measured_traffic_per_workload():
 
 def test_spectra_launch_count():
     """The spectra line's launch count follows the FFT plan of libeemd_spectra.so:
-    48000 = 4^3 * 2 * 3 * 5^3 (8 global passes), 4096 = 4^6 (one shared-memory
-    launch), 4099 (prime) through Bluestein's 16384-point transforms
-    (4 + 3 * 7), 37 through Bluestein's 128-point ones (4 + 3 * 1); an STFT of
-    4096-sample frames is one launch, of 8192-sample frames 2 + 6."""
-    assert bench.fft_passes(48000) == 8
+    4096 = 4^6 in one shared-memory launch, 48000 = 200 x 240 and 8192 =
+    64 x 128 as four-step pairs, 2^25 as 13 global passes, 4099 (prime)
+    through Bluestein's 16384-point transforms (4 + 3 * 2), 37 through
+    Bluestein's 128-point ones (4 + 3 * 1); the Hilbert call of 48000 is 5
+    launches, an STFT of 4096-sample frames one."""
+    assert bench.fft4_split(48000) == (200, 240)
+    assert bench.fft4_split(65536) == (256, 256)
+    assert bench.fft4_split(4096) is None
+    assert bench.fft_passes(48000) == 2
     assert bench.fft_passes(4096) == 1
-    assert bench.fft_passes(8192) == 7
-    assert bench.fft_passes(4099) == 4 + 3 * 7
+    assert bench.fft_passes(8192) == 2
+    assert bench.fft_passes(1 << 25) == 13
+    assert bench.fft_passes(4099) == 4 + 3 * 2
     assert bench.fft_passes(37) == 4 + 3 * 1
-    assert bench.spectra_launches(48000, 4096) == 2 * 1 + 3 + 2 * 8
-    assert bench.spectra_launches(48000, 8192) == 2 * (2 + 7) + 3 + 2 * 8
+    assert bench.spectra_launches(48000, 4096) == 2 * 1 + 5
+    assert bench.spectra_launches(48000, 8192) == 2 * (2 + 2) + 5

@@ -82,7 +82,9 @@ def test_own_fft_against_numpy(N):
     """eemd_sp_fft (Stockham radix 4/2/3/5/odd primes <= 31, Bluestein for
     larger primes: 37, 4097 = 17 x 241) against numpy.fft on 3 rows, both signs;
     lengths up to 4096 run as one shared-memory launch per row (37's Bluestein
-    transforms of 128 too), longer ones as global passes."""
+    transforms of 128 too), longer ones as the four-step transform of two
+    shared-memory launches (6144 = 64 x 96, 7168 = 64 x 112, 48000 =
+    200 x 240, 65536 = 256 x 256, 4097's Bluestein transforms of 8192)."""
     from eemd4cuda_b200 import _sp
     rng = np.random.default_rng(N)
     x = rng.standard_normal((3, N)) + 1j * rng.standard_normal((3, N))
@@ -93,6 +95,17 @@ def test_own_fft_against_numpy(N):
     b = _sp.fft_device(z, +1).cpu().numpy()
     refb = np.fft.ifft(x, axis=1) * N
     assert np.max(np.abs(b - refb)) <= 1e-13 * max(1.0, np.max(np.abs(refb)))
+
+
+def test_fft_beyond_the_four_step_limit():
+    """A row of 2^25 (longer than 4096 x 4096) runs as global Stockham passes."""
+    from eemd4cuda_b200 import _sp
+    N = 1 << 25
+    rng = np.random.default_rng(25)
+    x = rng.standard_normal(N) + 1j * rng.standard_normal(N)
+    f = _sp.fft_device(torch.from_numpy(x[None, :]).cuda(), -1).cpu().numpy()[0]
+    ref = np.fft.fft(x)
+    assert np.max(np.abs(f - ref)) <= 1e-12 * np.max(np.abs(ref))
 
 
 @pytest.mark.parametrize("nper", [256, 1000, 4096, 8192])
