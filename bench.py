@@ -379,12 +379,12 @@ def measured_peak_hbm():
 # of the same signal and are scaled per (signal, trial) task, since every task
 # streams its own buffers.
 EMD_TRAFFIC = {
-    "harmonic48k": {"bytes_per_launch": 6861367000,
-                    "engine_sha256": "7754f01fd896a1987064dee2d8a6248e61ca6833687fc52b45c2910270572110",
+    "harmonic48k": {"bytes_per_launch": 6837855000,
+                    "engine_sha256": "3788a361741c024d3ab67bed60b11685f8a5f528f948919fb8eb3f3ad6b353ab",
                     "capture": "one k_emd launch of the 100-trial 48 kHz workload (clusters of 4 five-warp CTAs)"},
-    "amfm4m": {"bytes_per_task": 5611588672.0,
-               "engine_sha256": "7754f01fd896a1987064dee2d8a6248e61ca6833687fc52b45c2910270572110",
-               "capture": "one k_emd launch of 4 trials of the 2^22-sample signal (clusters of 16 five-warp "
+    "amfm4m": {"bytes_per_task": 5603181376.0,
+               "engine_sha256": "3788a361741c024d3ab67bed60b11685f8a5f528f948919fb8eb3f3ad6b353ab",
+               "capture": "one k_emd launch of 4 trials of the 2^22-sample signal (clusters of 16 four-warp "
                           "CTAs), per task"},
 }
 
