@@ -616,7 +616,7 @@ def run_ours(args, wl: Workload):
     from eemd4cuda_b200 import emd_par as M
 
     # the CPU baseline pool is started before any GPU work (spawn context)
-    cb = CpuBaseline(wl) if (rank == 0 and world == 1) else None
+    cb = CpuBaseline(wl) if (rank == 0 and world == 1 and not args.quick) else None
 
     eng = Engine(wl, dev, wl.seed + rank)
     L = eng.L
@@ -710,7 +710,7 @@ def run_ours(args, wl: Workload):
     # the median of at least 20 calls (each ~10 ms), with the host clock beside
     e2e_ms, e2e_wall = [], []
     n_modes_e2e = wl.max_imf
-    for _ in range(max(args.steps, 20)):
+    for _ in range(3 if args.quick else max(args.steps, 20)):
         flush.fill_(1)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -734,7 +734,7 @@ def run_ours(args, wl: Workload):
 
     # ---- the same work as one launch sequence per signal ----
     per_signal = None
-    if wl.per_signal and rank == 0:
+    if wl.per_signal and rank == 0 and not args.quick:
         ps = PerSignal(wl, dev, wl.seed + rank)
         ps.step()
         torch.cuda.synchronize()
@@ -757,7 +757,7 @@ def run_ours(args, wl: Workload):
 
     # ---- float64 storage beside the float32 headline (the reference's own precision) ----
     f64_line = None
-    if wl.dtype == "f32" and wl.name == "harmonic48k":
+    if wl.dtype == "f32" and wl.name == "harmonic48k" and not args.quick:
         wl64 = dataclasses.replace(wl, dtype="f64", _signals=wl.signals())
         eng64 = Engine(wl64, dev, wl.seed + rank)
         for _ in range(args.warmup):
@@ -794,7 +794,7 @@ def run_ours(args, wl: Workload):
 
     # ---- error against the float64 CPU oracle (rank 0, outside the timed region) ----
     accuracy, acc64 = None, None
-    if rank == 0:
+    if rank == 0 and not args.quick:
         import multiprocessing as mp
         from concurrent.futures import ProcessPoolExecutor
         pool = cb.pool if cb is not None else ProcessPoolExecutor(
@@ -849,8 +849,55 @@ def run_ours(args, wl: Workload):
         line["float64_storage"] = f64_line
     if cpu is not None:
         line["cpu_baseline"] = cpu
+    if wl.name == "harmonic48k" and world == 1 and not args.quick and not args.no_companions:
+        line["other_configs"] = run_companions()
     print(json.dumps(line), flush=True)
     return 0
+
+
+# the other configurations, measured briefly beside the headline line (each in
+# a process of its own: one timed step after 3 warm-up steps, 3 end-to-end
+# calls, no CPU baseline and no oracle comparison; `--workload W` gives the
+# full line of each)
+COMPANIONS = (("plain8k", 180), ("amfm4m", 300), ("uneven512", 400), ("surrogate", 400), ("ceemdan48k", 180),
+              ("spectra48k", 180))
+
+
+def companion_summary(line: dict) -> dict:
+    out = {"metric": line.get("metric"), "value": line.get("value"), "unit": line.get("unit"),
+           "ms_per_step": line.get("ms_per_step"), "steps": line.get("steps"), "dtype": line.get("dtype"),
+           "workload": (line.get("config") or {}).get("workload")}
+    e2e = line.get("e2e")
+    if isinstance(e2e, dict):
+        out["e2e"] = e2e.get("value")
+    rf = line.get("roofline") or {}
+    out["roofline"] = {k: rf.get(k) for k in ("kernel", "achieved", "peak", "unit", "frac")}
+    for k in ("roofline_hbm", "split_ms", "speedup_vs_plain_256"):
+        if k in line:
+            out[k] = line[k]
+    out["clocks_sm_mhz"] = (line.get("clocks") or {}).get("sm_mhz")
+    return out
+
+
+def run_companions() -> dict:
+    res = {}
+    for w, limit in COMPANIONS:
+        cmd = [sys.executable, str(Path(__file__).resolve()), "--workload", w, "--steps", "1", "--warmup", "3",
+               "--quick"]
+        env = {k: v for k, v in os.environ.items() if k not in ("RANK", "LOCAL_RANK", "WORLD_SIZE")}
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=limit, cwd=str(ROOT), env=env)
+            lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+            if r.returncode != 0 or not lines:
+                tail = (r.stderr or r.stdout).strip().splitlines()[-1:] or ["no output"]
+                res[w] = {"error": f"exit {r.returncode}: {tail[0][:200]}"}
+            else:
+                res[w] = companion_summary(json.loads(lines[-1]))
+        except subprocess.TimeoutExpired:
+            res[w] = {"error": f"no line within {limit} s"}
+        except Exception as e:  # a companion never takes the headline line down
+            res[w] = {"error": f"{type(e).__name__}: {e}"[:200]}
+    return res
 
 
 # ---------------------------------------------------------------------------
@@ -920,7 +967,7 @@ def run_surrogate(args):
     from eemd4cuda_b200 import surrogate as SU
 
     N, S, E_small, E_big = 65536, SG_SIGNALS, 8, 256
-    cb = CpuBaseline(surrogate_cpu_workload()) if world == 1 else None
+    cb = CpuBaseline(surrogate_cpu_workload()) if world == 1 and not args.quick else None
 
     if SURROGATE_WEIGHTS.exists():
         net = SU.Net(seed=0)
@@ -1128,7 +1175,7 @@ def run_ceemdan(args):
     from eemd4cuda_b200.ceemdan import ceemdan
 
     wl = CEEMDAN_WL
-    cb = CpuBaseline(wl) if world == 1 else None
+    cb = CpuBaseline(wl) if world == 1 and not args.quick else None
     x = wl.signals()[0]
     N, E = len(x), wl.E
     kw = dict(E=E, eps=wl.eps, seed=0, tau=wl.tau, max_sifts=wl.max_sifts, noise="philox")
@@ -1387,6 +1434,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["surrogate", "ceemdan48k", "spectra48k"],
                     default="harmonic48k")
+    ap.add_argument("--quick", action="store_true",
+                    help="a brief line: no CPU baseline, no oracle comparison, 3 end-to-end calls")
+    ap.add_argument("--no-companions", action="store_true",
+                    help="leave out the brief lines of the other workloads from the headline line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -27,6 +27,19 @@ def _pool() -> ThreadPoolExecutor:
         return _POOL
 
 
+def copy_into(dst: np.ndarray, src: np.ndarray) -> None:
+    """dst[...] = src (parallel slices above 16 MiB when both are C-contiguous)."""
+    if src.nbytes < PARALLEL_BYTES or not (src.flags.c_contiguous and dst.flags.c_contiguous):
+        np.copyto(dst, src)
+        return
+    s, d = src.reshape(-1), dst.reshape(-1)
+    pool = _pool()
+    step = -(-s.size // WORKERS)
+    futs = [pool.submit(np.copyto, d[i:i + step], s[i:i + step]) for i in range(0, s.size, step)]
+    for f in futs:
+        f.result()
+
+
 def fresh_copy(src: np.ndarray) -> np.ndarray:
     """A new C-contiguous array equal to src (parallel slices above 16 MiB)."""
     src = np.asarray(src)

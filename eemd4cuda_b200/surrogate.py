@@ -54,7 +54,7 @@ from . import _lib as L
 from . import _sg as SG
 from . import emd_par as M
 from . import signals
-from .hostcopy import fresh_copy
+from .hostcopy import copy_into
 
 CH = 16           # padded channels of the network's input and output
 K_IMF = 10        # IMF channels
@@ -485,13 +485,29 @@ class SurrogateEEMD:
         hb["x"][:n].numpy()[:] = np.concatenate([np.asarray(x, np.float32) for x in xs])
         self.xd[:n].copy_(hb["x"][:n], non_blocking=True)
         self.run(S)
-        for name, d in (("imfs", self.imfs), ("resid", self.resid), ("met", self.metrics), ("fb", self.fallback)):
+        for name, d in (("met", self.metrics), ("fb", self.fallback)):
             hb[name][:S].copy_(d[:S], non_blocking=True)
+        # the served modes and residuals cross to the host in groups of signals, and the
+        # host copies each group out of the pinned buffers (reused by the next call) into
+        # fresh arrays while the later groups are still on their way
+        G = max(1, -(-S // 8))
+        marks = []
+        for g0 in range(0, S, G):
+            g1 = min(S, g0 + G)
+            hb["imfs"][g0:g1].copy_(self.imfs[g0:g1], non_blocking=True)
+            hb["resid"][g0:g1].copy_(self.resid[g0:g1], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record()
+            marks.append((g0, g1, ev))
+        imfs = np.empty((S, self.K, self.N), dtype=np.float64)
+        resid = np.empty((S, self.N), dtype=np.float64)
+        hi, hr = hb["imfs"].numpy(), hb["resid"].numpy()
+        for g0, g1, ev in marks:
+            ev.synchronize()
+            copy_into(imfs[g0:g1], hi[g0:g1])
+            copy_into(resid[g0:g1], hr[g0:g1])
         torch.cuda.current_stream().synchronize()
         self.net.check()
-        # fresh arrays: the pinned buffers are reused by the next call
-        imfs = fresh_copy(hb["imfs"][:S].numpy())
-        resid = fresh_copy(hb["resid"][:S].numpy())
         met = hb["met"][:S].numpy().copy()
         fb = hb["fb"][:S].numpy().astype(bool)
         flagged = [i for i in range(S) if fb[i]]

@@ -56,3 +56,21 @@ def test_spectra_launch_count():
     assert bench.fft_passes(37) == 4 + 3 * 1
     assert bench.spectra_launches(48000, 4096) == 2 * 1 + 5
     assert bench.spectra_launches(48000, 8192) == 2 * (2 + 2) + 5
+
+
+def test_companion_summary_and_failures(monkeypatch):
+    """The headline line's brief companion lines: the summary keeps the value,
+    end-to-end figure and roofline of a workload's line, and a companion that
+    fails (here: no GPU in this process's child) becomes an error entry
+    instead of an exception."""
+    line = {"metric": "m", "value": 1.5, "unit": "u", "ms_per_step": 2.0, "steps": 1, "dtype": "f64",
+            "config": {"workload": "w"}, "e2e": {"value": 1.2}, "clocks": {"sm_mhz": 1965.0},
+            "roofline": {"kernel": "k_emd", "achieved": 10.0, "peak": 100.0, "unit": "GB/s", "frac": 0.1,
+                         "traffic": 5}}
+    s = bench.companion_summary(line)
+    assert s["value"] == 1.5 and s["e2e"] == 1.2 and s["workload"] == "w" and s["clocks_sm_mhz"] == 1965.0
+    assert s["roofline"] == {"kernel": "k_emd", "achieved": 10.0, "peak": 100.0, "unit": "GB/s", "frac": 0.1}
+    monkeypatch.setattr(bench, "COMPANIONS", (("plain8k", 120),))
+    monkeypatch.setenv("CUDA_VISIBLE_DEVICES", "")
+    res = bench.run_companions()
+    assert set(res) == {"plain8k"} and "error" in res["plain8k"]
