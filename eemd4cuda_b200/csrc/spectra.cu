@@ -597,6 +597,21 @@ bool smem_ready(const void* fn) {
 
 unsigned smem_grid(int64_t rows) { return (unsigned)(rows < 65535 ? rows : 65535); }
 
+// the Hann window's sum, added in index order (as the reference's window sum
+// is formed); the last length's sum is kept per thread, since the host loop
+// of nperseg cosines costs more than the STFT's launch
+double window_sum(int nperseg) {
+    thread_local int last_n = 0;
+    thread_local double last_sum = 0.0;
+    if (nperseg != last_n) {
+        double wsum = 0.0;
+        for (int n = 0; n < nperseg; ++n) wsum += 0.5 - 0.5 * cos(2.0 * PI * (double)n / (double)nperseg);
+        last_n = nperseg;
+        last_sum = wsum;
+    }
+    return last_sum;
+}
+
 // the four-step split of a length: N1 the divisor nearest below sqrt(n) with
 // both N1 and n / N1 direct shared-memory lengths; false when there is none
 bool fft4_plan(int64_t n, Fft4Plan& F) {
@@ -847,9 +862,7 @@ int32_t eemd_sp_stft(const double* x, int32_t M, int64_t N, int32_t nperseg, int
     if (ws_bytes < L.total) return EEMD_SP_E_NOMEM;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const Bufs b = carve(ws, L);
-    // the window's sum, added in index order (as the reference's window sum is formed)
-    double wsum = 0.0;
-    for (int n = 0; n < nperseg; ++n) wsum += 0.5 - 0.5 * cos(2.0 * PI * (double)n / (double)nperseg);
+    const double wsum = window_sum(nperseg);
     SmemPlan sp;
     static const bool smem_ok = smem_ready(reinterpret_cast<const void*>(k_stft_smem));
     if (smem_ok && !L.P.L && smem_plan(nperseg, L.P.radices, sp)) {

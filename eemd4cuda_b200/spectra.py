@@ -11,6 +11,7 @@ the reference's host reduction.
 """
 from __future__ import annotations
 
+import functools
 import warnings
 
 import numpy as np
@@ -27,6 +28,11 @@ def _torch():
     return torch
 
 
+@functools.lru_cache(maxsize=64)
+def _hilbert_ws(M, N):
+    return _sp.hilbert_workspace(M, N)
+
+
 def hilbert_if_device(x, sr):
     """x: float64 CUDA tensor [M, N] (or [N]) -> (inst_freq, inst_amp) of the same shape."""
     torch = _torch()
@@ -37,7 +43,7 @@ def hilbert_if_device(x, sr):
         raise ValueError("hilbert_if needs at least 2 samples")
     freq = torch.empty_like(x2)
     amp = torch.empty_like(x2)
-    ws = torch.empty((_sp.hilbert_workspace(M, N),), dtype=torch.uint8, device=x2.device)
+    ws = torch.empty((_hilbert_ws(M, N),), dtype=torch.uint8, device=x2.device)
     _sp.hilbert_if(x2, M, N, sr, freq, amp, ws)
     return freq.reshape(x.shape), amp.reshape(x.shape)
 
@@ -63,19 +69,34 @@ def _segments(N, nperseg, noverlap):
     return int(nperseg), int(noverlap)
 
 
+@functools.lru_cache(maxsize=64)
+def _stft_plan(M, N, nperseg, noverlap):
+    """(F, T, workspace bytes) of one STFT shape (queried once per shape)."""
+    F, T = _sp.stft_shape(N, nperseg, noverlap)
+    return F, T, _sp.stft_workspace(M, N, nperseg, noverlap)
+
+
+@functools.lru_cache(maxsize=64)
+def _stft_axes(nperseg, noverlap, T, sr):
+    f = np.fft.rfftfreq(nperseg, 1.0 / sr)
+    t = np.arange(T) * (nperseg - noverlap) / float(sr)
+    f.flags.writeable = False
+    t.flags.writeable = False
+    return f, t
+
+
 def stft_device(x, sr, nperseg=4096, noverlap=None):
     """x: float64 CUDA tensor [M, N] (or [N]) -> (f, t, Z complex128 [M, F, T] (or [F, T]))."""
     torch = _torch()
     x2 = (x.reshape(1, -1) if x.dim() == 1 else x).contiguous()
     M, N = int(x2.shape[0]), int(x2.shape[1])
     nperseg, noverlap = _segments(N, nperseg, noverlap)
-    F, T = _sp.stft_shape(N, nperseg, noverlap)
+    F, T, wsb = _stft_plan(M, N, nperseg, noverlap)
     Z = torch.empty((M, F, T), dtype=torch.complex128, device=x2.device)
-    ws = torch.empty((_sp.stft_workspace(M, N, nperseg, noverlap),), dtype=torch.uint8, device=x2.device)
+    ws = torch.empty((wsb,), dtype=torch.uint8, device=x2.device)
     _sp.stft(x2, M, N, nperseg, noverlap, Z, ws)
-    f = np.fft.rfftfreq(nperseg, 1.0 / sr)
-    t = np.arange(T) * (nperseg - noverlap) / float(sr)
-    return f, t, (Z[0] if x.dim() == 1 else Z)
+    f, t = _stft_axes(nperseg, noverlap, T, float(sr))
+    return f.copy(), t.copy(), (Z[0] if x.dim() == 1 else Z)
 
 
 def stft_block(x, sr, nperseg=4096, noverlap=None):
