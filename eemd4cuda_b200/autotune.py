@@ -29,7 +29,8 @@ from pathlib import Path
 import numpy as np
 
 TABLE_DIR = Path(__file__).resolve().parent / "tuning"
-BUCKETS = (4096, 16384, 65536, 262144, 1 << 20, 1 << 22)
+# 49152: about a second of 48 kHz audio, the audio stage's usual segment
+BUCKETS = (4096, 8192, 16384, 32768, 49152, 65536, 262144, 1 << 20, 1 << 22)
 TASKS = (1, 8, 32, 64, 100, 256, 1024, 4096)
 CANDIDATES = (1, 2, 3, 4, 5, 6, 8, 12, 16)   # CTAs per task
 WARPS = (4, 5)                                # warps per CTA
@@ -50,16 +51,18 @@ def _table(dtype: str):
             for e in d["entries"]]
 
 
-def launch_shape(n_min: int, n_tasks: int, dtype: str) -> tuple:
-    """Tuned (CTAs per task, warps per CTA) for a launch whose shortest signal
-    has n_min samples and which holds n_tasks tasks (nearest entry in log
-    length, then in log task count), or (0, 0) when the table has no entry
-    for that storage type."""
+def launch_shape(n_ref: int, n_tasks: int, dtype: str, n_min: int | None = None) -> tuple:
+    """Tuned (CTAs per task, warps per CTA) for a launch of n_tasks tasks
+    whose signals have a median length of n_ref samples and a shortest one
+    of n_min (default n_ref): the nearest entry in log length, then in log
+    task count, with no more CTAs than give the shortest signal 2048 samples
+    each; (0, 0) when the table has no entry for that storage type."""
     tab = _table(dtype)
     if not tab:
         return 0, 0
+    n_min = n_ref if n_min is None else n_min
     lengths = sorted({n for n, _, _, _ in tab})
-    bn = min(lengths, key=lambda n: abs(math.log(n) - math.log(max(n_min, 1))))
+    bn = min(lengths, key=lambda n: abs(math.log(n) - math.log(max(n_ref, 1))))
     rows = [(t, c, w) for n, t, c, w in tab if n == bn]
     t, c, w = min(rows, key=lambda r: abs(math.log(r[0]) - math.log(max(n_tasks, 1))))
     # a cluster needs at least 2048 samples per CTA (the engine's own bound)
@@ -99,10 +102,10 @@ def _measure(n: int, tasks: int, dtype: str, c: int, reps: int, nw: int = 4) -> 
     return best
 
 
-def tune(dtype: str = "f32", quick: bool = False, reps: int = 2) -> dict:
+def tune(dtype: str = "f32", quick: bool = False, reps: int = 2, buckets=None) -> dict:
     import torch
 
-    buckets = BUCKETS[:4] if quick else BUCKETS
+    buckets = tuple(buckets) if buckets else (BUCKETS[:4] if quick else BUCKETS)
     entries = []
     for n in buckets:
         for tasks in TASKS:
@@ -135,8 +138,16 @@ def main():
     ap.add_argument("--dtype", choices=["f32", "f64"], default="f32")
     ap.add_argument("--quick", action="store_true")
     ap.add_argument("--out", default=None)
+    ap.add_argument("--buckets", default="", help="comma-separated lengths to measure (default: all buckets)")
+    ap.add_argument("--merge", default="", help="a table whose entries for other lengths are kept")
     a = ap.parse_args()
-    d = tune(a.dtype, a.quick)
+    d = tune(a.dtype, a.quick, buckets=[int(v) for v in a.buckets.split(",") if v])
+    if a.merge:
+        old = json.loads(Path(a.merge).read_text())
+        mine = {e["n"] for e in d["entries"]}
+        d["entries"] = sorted([e for e in old["entries"] if e["n"] not in mine] + d["entries"],
+                              key=lambda e: (e["n"], e["tasks"]))
+        d["measured"] = f'{old.get("measured")}; lengths {sorted(mine)}: {d["measured"]}'
     out = Path(a.out) if a.out else table_path(a.dtype)
     out.parent.mkdir(parents=True, exist_ok=True)
     out.write_text(json.dumps(d, indent=1))

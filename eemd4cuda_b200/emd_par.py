@@ -168,8 +168,11 @@ def tuned(p: L.EemdParams, lengths, trial_count: int) -> L.EemdParams:
 
     if p.cluster_size or p.cta_warps:
         return p
-    c, nw = autotune.launch_shape(min(int(n) for n in lengths), len(lengths) * int(trial_count),
-                                  "f32" if p.dtype == L.EEMD_F32 else "f64")
+    ls = sorted(int(n) for n in lengths)
+    # an uneven batch is looked up by its median length (most of its work),
+    # with the shortest signal bounding the CTAs per task
+    c, nw = autotune.launch_shape(ls[len(ls) // 2], len(ls) * int(trial_count),
+                                  "f32" if p.dtype == L.EEMD_F32 else "f64", n_min=ls[0])
     if not c:
         return p
     q = L.EemdParams.from_buffer_copy(p)

@@ -21,6 +21,18 @@ def test_lookup_nearest_bucket_and_task_count(monkeypatch):
     assert A.cluster_size(48000, 100, "f64") == 0       # no table: the engine's own rule
     # never below 2048 samples per CTA
     assert A.cluster_size(20000, 1, "f32") == 9
+    # an uneven launch: looked up by its median length, capped by its shortest signal
+    assert A.launch_shape(65536, 1, "f32", n_min=8192) == (4, 4)
+    assert A.launch_shape(65536, 1, "f32", n_min=65536) == (16, 4)
+
+
+def test_uneven_batch_uses_the_median_length(monkeypatch):
+    """tuned() looks an uneven batch up by its median length (the long
+    signals' bucket), not by its shortest signal's."""
+    monkeypatch.setattr(A, "_table", lambda dtype: TABLE)
+    p = M.make_params(dtype=np.float32)
+    q = M.tuned(p, [4096] + [65536] * 4, 1)
+    assert (q.cluster_size, q.cta_warps) == (2, 4)   # 65536, 5 tasks -> 16 CTAs of 4 warps, capped to 2 by 4096
 
 
 def test_tuned_params_respect_an_explicit_choice(monkeypatch):
