@@ -27,6 +27,19 @@ def _pool() -> ThreadPoolExecutor:
         return _POOL
 
 
+def prefault(arrays) -> list:
+    """Touch every page of fresh arrays on the copy threads (zero-fills 16 MiB
+    slices) and return the futures: started before a device computation, the
+    page faults happen while the device works instead of during the copies."""
+    pool = _pool()
+    futs = []
+    for a in arrays:
+        flat = a.reshape(-1)
+        step = max(1, PARALLEL_BYTES // max(a.itemsize, 1))
+        futs += [pool.submit(np.copyto, flat[i:i + step], 0) for i in range(0, flat.size, step)]
+    return futs
+
+
 def copy_into(dst: np.ndarray, src: np.ndarray) -> None:
     """dst[...] = src (parallel slices above 16 MiB when both are C-contiguous)."""
     if src.nbytes < PARALLEL_BYTES or not (src.flags.c_contiguous and dst.flags.c_contiguous):

@@ -54,7 +54,7 @@ from . import _lib as L
 from . import _sg as SG
 from . import emd_par as M
 from . import signals
-from .hostcopy import copy_into
+from .hostcopy import copy_into, prefault
 
 CH = 16           # padded channels of the network's input and output
 K_IMF = 10        # IMF channels
@@ -484,6 +484,10 @@ class SurrogateEEMD:
         n = S * self.N
         hb["x"][:n].numpy()[:] = np.concatenate([np.asarray(x, np.float32) for x in xs])
         self.xd[:n].copy_(hb["x"][:n], non_blocking=True)
+        # the fresh result arrays are paged in on the copy threads while the device computes
+        imfs = np.empty((S, self.K, self.N), dtype=np.float64)
+        resid = np.empty((S, self.N), dtype=np.float64)
+        paged = prefault([imfs, resid])
         self.run(S)
         for name, d in (("met", self.metrics), ("fb", self.fallback)):
             hb[name][:S].copy_(d[:S], non_blocking=True)
@@ -499,8 +503,8 @@ class SurrogateEEMD:
             ev = torch.cuda.Event()
             ev.record()
             marks.append((g0, g1, ev))
-        imfs = np.empty((S, self.K, self.N), dtype=np.float64)
-        resid = np.empty((S, self.N), dtype=np.float64)
+        for f in paged:
+            f.result()
         hi, hr = hb["imfs"].numpy(), hb["resid"].numpy()
         for g0, g1, ev in marks:
             ev.synchronize()
