@@ -82,6 +82,7 @@ def ceemdan(x, E=100, eps=0.2, parallel=True, n_workers=None, seed=0, *, tau=0.2
     nm = torch.empty((1,), dtype=torch.int32, device=dev)
     r_d = torch.from_numpy(x.copy()).to(dev)
     r_next = torch.empty_like(r_d)
+    h_r = torch.empty((N,), dtype=torch.float64, pin_memory=True)  # each stage's residual, back to the host
     resid = x.copy()
     n_st = 0
     while True:
@@ -93,18 +94,27 @@ def ceemdan(x, E=100, eps=0.2, parallel=True, n_workers=None, seed=0, *, tau=0.2
         cnt = cnt_buf[stage:stage + 1]
         L.run(p1, r_d, [N], 0, E, ws, noise=Wd, imf_sum=imf_sum, mode_count=cnt, nsift=sift_buf[stage])
         L.finalize(p1, r_d, [N], imf_sum, cnt, c_buf[stage], r_next, nm)
-        resid = r_next.cpu().numpy()
+        h_r.copy_(r_next, non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+        resid = h_r.numpy().copy()
         n_st += 1
         r_d, r_next = r_next, r_d
         if all(stage >= m for m in noise_modes):
             break
-    counts = cnt_buf[:n_st].cpu().numpy()
+    # the stages' modes and counters through pinned memory, one synchronisation
+    h_c = torch.empty((n_st, N), dtype=torch.float64, pin_memory=True)
+    h_cnt = torch.empty((n_st,), dtype=torch.int32, pin_memory=True)
+    h_sift = torch.empty((n_st, E), dtype=torch.int32, pin_memory=True)
+    h_c.copy_(c_buf[:n_st], non_blocking=True)
+    h_cnt.copy_(cnt_buf[:n_st], non_blocking=True)
+    h_sift.copy_(sift_buf[:n_st], non_blocking=True)
+    torch.cuda.current_stream(dev).synchronize()
+    counts = h_cnt.numpy()
     for stage, k in enumerate(counts):
         if int(k) != E:
             raise ValueError(f"CEEMDAN stage {stage}: {E - int(k)} of {E} trials have no first IMF "
                              "(fewer than 4 extrema)")
-    c_imfs = list(c_buf[:n_st].cpu().numpy())
-    sifts = sift_buf[:n_st].cpu().numpy().tolist()
-    c = np.array(c_imfs) if c_imfs else np.zeros((0, N))
-    return c, resid, dict(E=E, n_imfs=len(c_imfs), noise_modes=noise_modes, stage_sifts=sifts, method="gpu",
+    sifts = h_sift.numpy().tolist()
+    c = h_c.numpy() if n_st else np.zeros((0, N))
+    return c, resid, dict(E=E, n_imfs=int(n_st), noise_modes=noise_modes, stage_sifts=sifts, method="gpu",
                           backend="b200", exact=bool(exact), noise=noise)
