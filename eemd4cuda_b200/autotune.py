@@ -61,6 +61,10 @@ def launch_shape(n_ref: int, n_tasks: int, dtype: str, n_min: int | None = None)
     if not tab:
         return 0, 0
     n_min = n_ref if n_min is None else n_min
+    key = (id(tab), int(n_ref), int(n_tasks), int(n_min))
+    hit = _SHAPES.get(key)
+    if hit is not None:
+        return hit
     lengths = sorted({n for n, _, _, _ in tab})
     bn = min(lengths, key=lambda n: abs(math.log(n) - math.log(max(n_ref, 1))))
     rows = [(t, c, w) for n, t, c, w in tab if n == bn]
@@ -68,7 +72,13 @@ def launch_shape(n_ref: int, n_tasks: int, dtype: str, n_min: int | None = None)
     # a cluster needs at least 2048 samples per CTA (the engine's own bound)
     while c > 1 and n_min // c < 2048:
         c -= 1
+    if len(_SHAPES) > 4096:
+        _SHAPES.clear()
+    _SHAPES[key] = (c, w)
     return c, w
+
+
+_SHAPES: dict = {}  # looked-up shapes per (table, lengths, task count)
 
 
 def cluster_size(n_min: int, n_tasks: int, dtype: str) -> int:

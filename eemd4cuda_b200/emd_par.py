@@ -417,24 +417,20 @@ def _run_single(x, *, tau, max_sifts, max_imf, min_extrema, end, rules, exact, d
     p = tuned(p, [N], 1)
     xd = torch.from_numpy(np.ascontiguousarray(x, dtype=dt)).to(dev)
     ws = torch.empty((L.workspace_size(p, [N], 1, True),), dtype=torch.uint8, device=dev)
-    imfs = torch.zeros((1, slots, N), dtype=tdt, device=dev)
+    # (the engine writes every IMF row it returns; the rows past the mode count are not read)
+    imfs = torch.empty((1, slots, N), dtype=tdt, device=dev)
     resid = torch.empty((1, N), dtype=tdt, device=dev)
-    nsift = torch.empty((1,), dtype=torch.int32, device=dev)
-    nmode = torch.empty((1,), dtype=torch.int32, device=dev)
-    msifts = torch.empty((1, slots), dtype=torch.int32, device=dev)
-    flags = torch.empty((1,), dtype=torch.int32, device=dev)
+    # the counters in one array (sifts, modes, flags, sifts per mode): one copy back
+    cnt = torch.empty((3 + slots,), dtype=torch.int32, device=dev)
     t0 = time.time()
-    L.run(p, xd, [N], 0, 1, ws, imfs=imfs, resid_out=resid, nsift=nsift, nmode=nmode,
-          mode_sifts=msifts, flags=flags)
+    L.run(p, xd, [N], 0, 1, ws, imfs=imfs, resid_out=resid, nsift=cnt[0:1], nmode=cnt[1:2],
+          mode_sifts=cnt[3:], flags=cnt[2:3])
     # every output into pinned memory, one synchronisation
     h_imfs, h_res = _pinned(torch, (slots, N), torch.float64), _pinned(torch, (N,), torch.float64)
     h_cnt = _pinned(torch, (3 + slots,), torch.int32)
     h_imfs.copy_(imfs[0].to(torch.float64), non_blocking=True)
     h_res.copy_(resid[0].to(torch.float64), non_blocking=True)
-    h_cnt[0:1].copy_(nsift, non_blocking=True)
-    h_cnt[1:2].copy_(nmode, non_blocking=True)
-    h_cnt[2:3].copy_(flags, non_blocking=True)
-    h_cnt[3:].copy_(msifts[0], non_blocking=True)
+    h_cnt.copy_(cnt, non_blocking=True)
     torch.cuda.current_stream(dev).synchronize()
     c = h_cnt.tolist()
     nm = int(c[1])
