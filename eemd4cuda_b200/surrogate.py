@@ -99,7 +99,11 @@ class Ensembles:
         torch = _torch()
         self.torch = torch
         self.S, self.N = S, N
-        self.p = p if p is not None else engine_params()
+        # p_base: the caller's settings; p: the same with the launch shape of
+        # the group's largest launch from the autotune table (the workspace is
+        # sized for it, and every launch of the group uses it)
+        self.p_base = p if p is not None else engine_params()
+        self.p = M.tuned(self.p_base, [N] * S, max_trials)
         self.K = int(self.p.max_imf)
         self.ws = torch.empty((L.workspace_size(self.p, [N] * S, max_trials, False),), dtype=torch.uint8,
                               device="cuda")
@@ -517,7 +521,7 @@ class SurrogateEEMD:
         flagged = [i for i in range(S) if fb[i]]
         plain = {}
         if flagged:
-            plain = dict(zip(flagged, plain_eemd([xs[i] for i in flagged], self.N, self.E_big, self.ens.p)))
+            plain = dict(zip(flagged, plain_eemd([xs[i] for i in flagged], self.N, self.E_big, self.ens.p_base)))
         out = []
         for i in range(S):
             st = dict(method="surrogate", recon=float(met[i, 0]), io=float(met[i, 1]), io_all=float(met[i, 2]),
