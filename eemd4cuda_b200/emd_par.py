@@ -43,7 +43,7 @@ from dataclasses import asdict, dataclass, field
 import numpy as np
 
 from . import _lib as L
-from .hostcopy import fresh_copy
+from .hostcopy import copy_into, fresh_copy, prefault
 
 __all__ = ["decompose", "decompose_many", "EMDResult", "make_reference_sweep", "gpu_eemd_full", "EngineConfig"]
 
@@ -525,6 +525,11 @@ def decompose_many(xs, E=64, eps=0.2, tau=0.25, max_sifts=50, max_imf=-1, min_ex
     imf_sum = torch.zeros((slots * NS,), dtype=torch.float64, device=dev)
     mode_count = torch.zeros((S * slots,), dtype=torch.int32, device=dev)
     ws = torch.empty((L.workspace_size(p, lengths, batch, False),), dtype=torch.uint8, device=dev)
+    paged = None
+    if slots * NS * 8 > PINNED_RESULT_BYTES:
+        # large results: their host arrays are paged in on the copy threads while the device works
+        mh_host, rh_host = np.empty((slots * NS,), dtype=np.float64), np.empty((NS,), dtype=np.float64)
+        paged = (mh_host, rh_host, prefault([mh_host, rh_host]))
     sifts = np.zeros((S, E), dtype=np.int64)
     modes = np.zeros((S, E), dtype=np.int64)
     flags = np.zeros((S, E), dtype=np.int64)
@@ -540,20 +545,64 @@ def decompose_many(xs, E=64, eps=0.2, tau=0.25, max_sifts=50, max_imf=-1, min_ex
     resid = torch.empty((NS,), dtype=torch.float64, device=dev)
     n_modes = torch.empty((S,), dtype=torch.int32, device=dev)
     L.finalize(p, xd, lengths, imf_sum, mode_count, imf_mean, resid, n_modes)
-    mh, rh, nh = imf_mean.cpu().numpy(), resid.cpu().numpy(), n_modes.cpu().numpy()
+    mh, rh, nh = _download(torch, dev, imf_mean, resid, n_modes, paged)
     wall = time.time() - t0
+    # every signal's result is a view of the launch's host arrays (no per-signal copy)
     out, off = [], 0
     for s, x in enumerate(xs):
         n = lengths[s]
         m = int(nh[s])
-        imfs = mh[slots * off:slots * (off + n)].reshape(slots, n)[:m].copy()
+        imfs = mh[slots * off:slots * (off + n)].reshape(slots, n)[:m]
         stats = dict(method="gpu", backend="b200", E=E, n_modes=m, batch=batch, signal=s, signals=S,
                      per_trial_total_sifts=sifts[s].copy(), per_trial_n_modes=modes[s].copy(),
                      max_imf_reached=bool((flags[s] & 1).any() and max_imf == -1), gpu_time_s=wall,
                      noise="philox" if E > 1 else "none", x=x)
-        out.append(EMDResult(imfs=imfs, residual=rh[off:off + n].copy(), n_modes=m, stats=stats))
+        out.append(EMDResult(imfs=imfs, residual=rh[off:off + n], n_modes=m, stats=stats))
         off += n
     return out
+
+
+def _download(torch, dev, imf_mean, resid, n_modes, paged):
+    """The finalised means, residuals and mode counts of a batch into host
+    arrays: small results through pinned tensors of the call, large ones
+    through the shared pinned staging in slices, each slice copied out on the
+    copy threads into fresh arrays paged in beforehand (`paged`: their
+    prefault futures) while the next slice crosses."""
+    nb = imf_mean.numel() * 8
+    if nb <= PINNED_RESULT_BYTES:
+        h_m, h_r = _pinned(torch, (imf_mean.numel(),), torch.float64), _pinned(torch, (resid.numel(),), torch.float64)
+        h_n = _pinned(torch, (n_modes.numel(),), torch.int32)
+        h_m.copy_(imf_mean, non_blocking=True)
+        h_r.copy_(resid, non_blocking=True)
+        h_n.copy_(n_modes, non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+        return h_m.numpy(), h_r.numpy(), h_n.numpy()
+    mh, rh, futs = paged
+    nh = n_modes.cpu().numpy()
+    with _STAGE_LOCK:
+        stage = _staging(torch, 2, PINNED_RESULT_BYTES // 16)[0].reshape(-1)  # 64 MB, two halves
+        half = stage.numel() // 2
+        for f in futs:
+            f.result()
+        for dst, src in ((mh, imf_mean), (rh, resid)):
+            n, marks, i0 = src.numel(), [], 0
+            hs = stage.numpy()
+            while i0 < n:
+                i1 = min(n, i0 + half)
+                buf = (len(marks) & 1) * half
+                if len(marks) >= 2:  # the half this slice reuses has been copied out
+                    marks[-2][2].synchronize()
+                    a0, a1, _, b0 = marks[-2]
+                    copy_into(dst[a0:a1], hs[b0:b0 + (a1 - a0)])
+                stage[buf:buf + (i1 - i0)].copy_(src[i0:i1], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record()
+                marks.append((i0, i1, ev, buf))
+                i0 = i1
+            for a0, a1, ev, b0 in marks[-2:]:
+                ev.synchronize()
+                copy_into(dst[a0:a1], hs[b0:b0 + (a1 - a0)])
+    return mh, rh, nh
 
 
 def gpu_eemd_full(x, E=64, tau=0.25, max_sifts=50, max_imf=12, seed=0, K=None, nthreads=128,
