@@ -48,13 +48,30 @@ def hilbert_if_device(x, sr):
     return freq.reshape(x.shape), amp.reshape(x.shape)
 
 
+def _to_device(torch, a):
+    """A host array on the device through a pinned copy (asynchronous upload)."""
+    h = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+    h.numpy()[...] = a
+    return h.to("cuda", non_blocking=True)
+
+
+def _to_host(torch, *ts):
+    """Device tensors as host arrays: views of pinned tensors of this call
+    (torch's caching host allocator), one synchronisation."""
+    hs = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in ts]
+    for h, t in zip(hs, ts):
+        h.copy_(t, non_blocking=True)
+    torch.cuda.current_stream().synchronize()
+    return tuple(h.numpy() for h in hs)
+
+
 def hilbert_if(imf, sr):
     """Instantaneous frequency [Hz] and amplitude of one IMF (or of each row):
     z = imf + i H(imf), d/dt arg(z) / 2 pi, |z| (spectra.py:32-45)."""
     torch = _torch()
     a = np.ascontiguousarray(imf, dtype=np.float64)
-    f, A = hilbert_if_device(torch.from_numpy(a).cuda(), sr)
-    return f.cpu().numpy(), A.cpu().numpy()
+    f, A = hilbert_if_device(_to_device(torch, a), sr)
+    return _to_host(torch, f, A)
 
 
 def _segments(N, nperseg, noverlap):
@@ -104,8 +121,8 @@ def stft_block(x, sr, nperseg=4096, noverlap=None):
     default, zero-extended ends, one-sided (spectra.py:18-29).  Returns (f, t, Zxx)."""
     torch = _torch()
     a = np.ascontiguousarray(x, dtype=np.float64)
-    f, t, Z = stft_device(torch.from_numpy(a).cuda(), sr, nperseg, noverlap)
-    return f, t, Z.cpu().numpy()
+    f, t, Z = stft_device(_to_device(torch, a), sr, nperseg, noverlap)
+    return f, t, _to_host(torch, Z)[0]
 
 
 def if_stats(w: np.ndarray) -> dict:
