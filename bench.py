@@ -1384,13 +1384,20 @@ def run_spectra(args):
     peak, peak_kind = measured_peak_hbm()
     # end to end through the host API (host rows in, host spectra out)
     hx, himfs = np.ascontiguousarray(x, dtype=np.float64), np.ascontiguousarray(r.imfs)
+
+    def e2e_call():
+        spectra.stft_block(hx, sr, nper)
+        spectra.stft_block(himfs, sr, nper)
+        spectra.hilbert_if(himfs, sr)
+
+    # one untimed call first: it brings the pinned host blocks of the results'
+    # sizes into torch's host allocator cache, as the EEMD lines' warm-up does
+    e2e_call()
     e2e_ms = []
     for _ in range(max(1, args.steps)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        spectra.stft_block(hx, sr, nper)
-        spectra.stft_block(himfs, sr, nper)
-        spectra.hilbert_if(himfs, sr)
+        e2e_call()
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2e = statistics.median(e2e_ms)
     F, T = nper // 2 + 1, (N + nper - nper // 2) // (nper // 2)
