@@ -75,12 +75,15 @@ def hilbert_if(imf, sr):
 
 
 def _segments(N, nperseg, noverlap):
-    # scipy's rule: a segment longer than the input is cut to it (with a warning)
-    if nperseg > N:
-        warnings.warn(f"nperseg = {nperseg} is greater than input length = {N}, using nperseg = {N}")
-        nperseg = N
+    # the default overlap is half the requested frame (spectra.py:25-26),
+    # filled in before scipy's rule cuts a frame longer than the input to the
+    # input (with a warning); a short input with the default overlap is
+    # therefore an error, as in the reference
     if noverlap is None:
         noverlap = nperseg // 2
+    if nperseg > N:
+        warnings.warn(f"nperseg = {nperseg} is greater than input length  = {N}, using nperseg = {N}")
+        nperseg = N
     if noverlap >= nperseg:
         raise ValueError("noverlap must be less than nperseg.")
     return int(nperseg), int(noverlap)

@@ -121,3 +121,68 @@ def test_stft_frame_lengths_against_oracle(nper):
         of, ot, oZ = SP.stft(X[r], sr, nper)
         assert np.allclose(f, of) and np.allclose(t, ot)
         assert np.max(np.abs(Z[r] - oZ)) <= 1e-11 * np.max(np.abs(oZ))
+
+
+def tones(rng, rows, N):
+    """rows of three tones of random frequency and phase, slight noise"""
+    t = np.arange(N, dtype=float)
+    out = np.zeros((rows, N))
+    for r in range(rows):
+        for _ in range(3):
+            out[r] += rng.uniform(0.2, 1.0) * np.cos(2 * np.pi * rng.uniform(0.002, 0.2) * t + rng.uniform(0, 6.3))
+        out[r] += 0.01 * rng.standard_normal(N)
+    return out
+
+
+@pytest.mark.parametrize("N", [2, 3, 5, 8, 31, 33, 1001, 4097])
+def test_hilbert_short_and_odd_lengths_against_oracle(N):
+    """The analytic signal's one-sided weights for even and odd N (a single
+    Nyquist bin only when N is even) down to two samples: amplitude and
+    instantaneous frequency against the oracle's restatement of
+    scipy.signal.hilbert + unwrap + gradient (audio_eemd/spectra.py:18-30)."""
+    rng = np.random.default_rng(N)
+    sr = 48000
+    X = tones(rng, 3, N)
+    w, A = spectra.hilbert_if(X, sr)
+    assert w.shape == A.shape == (3, N)
+    for r in range(3):
+        ow, oA = SP.hilbert_if(X[r], sr)
+        assert np.max(np.abs(A[r] - oA)) <= 1e-12 * max(1.0, np.max(oA)), r
+        m = steady(oA)
+        if m.any():
+            assert np.max(np.abs(w[r] - ow)[m]) <= 1e-6 * sr, r
+
+
+@pytest.mark.parametrize("N,nper,nov", [(5000, 1000, 333), (4096, 512, 384), (777, 64, 1), (20000, 4096, 0)])
+def test_stft_other_overlaps_against_oracle(N, nper, nov):
+    """Hops other than half a frame (a third, an eighth, one sample short of
+    a whole frame, no overlap): frame count, axes and bins against the
+    oracle."""
+    rng = np.random.default_rng(N + nov)
+    sr = 48000
+    X = tones(rng, 2, N)
+    f, t, Z = spectra.stft_block(X, sr, nperseg=nper, noverlap=nov)
+    for r in range(2):
+        of, ot, oZ = SP.stft(X[r], sr, nper, nov)
+        assert Z[r].shape == oZ.shape
+        assert np.allclose(f, of) and np.allclose(t, ot)
+        assert np.max(np.abs(Z[r] - oZ)) <= 1e-11 * np.max(np.abs(oZ))
+
+
+def test_stft_of_a_signal_shorter_than_the_frame():
+    """nperseg above the signal length (audio_eemd/spectra.py:25-29 over
+    scipy.signal.stft): the default overlap, half the requested frame, is
+    then not below the cut frame, a ValueError; with an explicit overlap a
+    warning and frames of the signal's length."""
+    rng = np.random.default_rng(3)
+    sr, N = 48000, 1000
+    X = tones(rng, 2, N)
+    with pytest.warns(UserWarning, match="nperseg"), pytest.raises(ValueError, match="noverlap"):
+        spectra.stft_block(X, sr, nperseg=4096)
+    with pytest.warns(UserWarning, match="nperseg"):
+        f, t, Z = spectra.stft_block(X, sr, nperseg=4096, noverlap=300)
+    for r in range(2):
+        of, ot, oZ = SP.stft(X[r], sr, N, 300)
+        assert Z[r].shape == oZ.shape
+        assert np.allclose(f, of) and np.allclose(t, ot)
+        assert np.max(np.abs(Z[r] - oZ)) <= 1e-11 * np.max(np.abs(oZ))
