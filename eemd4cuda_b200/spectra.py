@@ -48,8 +48,17 @@ def hilbert_if_device(x, sr):
     return freq.reshape(x.shape), amp.reshape(x.shape)
 
 
+# arrays up to this size move through pinned tensors of the call (torch's
+# caching host allocator keeps their blocks for reuse); larger ones through
+# pageable memory, so that large calls leave no large pinned blocks behind
+PINNED_BYTES = 64 << 20
+
+
 def _to_device(torch, a):
-    """A host array on the device through a pinned copy (asynchronous upload)."""
+    """A host array on the device: through a pinned copy (asynchronous
+    upload) up to PINNED_BYTES, else a pageable copy."""
+    if a.nbytes > PINNED_BYTES:
+        return torch.from_numpy(a).to("cuda")
     h = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
     h.numpy()[...] = a
     return h.to("cuda", non_blocking=True)
@@ -57,12 +66,16 @@ def _to_device(torch, a):
 
 def _to_host(torch, *ts):
     """Device tensors as host arrays: views of pinned tensors of this call
-    (torch's caching host allocator), one synchronisation."""
-    hs = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in ts]
+    (torch's caching host allocator) with one synchronisation, or pageable
+    copies for tensors above PINNED_BYTES."""
+    hs = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+          if t.numel() * t.element_size() <= PINNED_BYTES else None for t in ts]
     for h, t in zip(hs, ts):
-        h.copy_(t, non_blocking=True)
+        if h is not None:
+            h.copy_(t, non_blocking=True)
+    out = [t.cpu() if h is None else None for h, t in zip(hs, ts)]  # (each synchronises)
     torch.cuda.current_stream().synchronize()
-    return tuple(h.numpy() for h in hs)
+    return tuple((h if h is not None else o).numpy() for h, o in zip(hs, out))
 
 
 def hilbert_if(imf, sr):

@@ -186,3 +186,19 @@ def test_stft_of_a_signal_shorter_than_the_frame():
         assert Z[r].shape == oZ.shape
         assert np.allclose(f, of) and np.allclose(t, ot)
         assert np.max(np.abs(Z[r] - oZ)) <= 1e-11 * np.max(np.abs(oZ))
+
+
+def test_large_rows_through_pageable_copies():
+    """Rows whose results exceed the pinned-transfer size (two rows of 2^23
+    samples: 128 MB per result array) move through pageable copies, with the
+    same results as the oracle."""
+    assert 2 * (1 << 23) * 8 > spectra.PINNED_BYTES
+    rng = np.random.default_rng(23)
+    sr, N = 48000, 1 << 23
+    X = tones(rng, 2, N)
+    w, A = spectra.hilbert_if(X, sr)
+    for r in range(2):
+        ow, oA = SP.hilbert_if(X[r], sr)
+        assert np.max(np.abs(A[r] - oA)) <= 1e-10 * np.max(oA)
+        m = steady(oA)
+        assert np.max(np.abs(w[r] - ow)[m]) <= 1e-6 * sr
