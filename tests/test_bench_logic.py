@@ -74,3 +74,25 @@ def test_companion_summary_and_failures(monkeypatch):
     monkeypatch.setenv("CUDA_VISIBLE_DEVICES", "")
     res = bench.run_companions()
     assert set(res) == {"plain8k"} and "error" in res["plain8k"]
+
+
+def test_reference_arm_line():
+    """`bench.py --impl reference` (the reference's CPU path on the host
+    cores, no GPU) prints one JSON line with the GPU arm's metric and unit,
+    a cpu_baseline describing the run and an e2e entry with no host-device
+    bytes."""
+    import json
+    import subprocess
+
+    r = subprocess.run([sys.executable, str(Path(bench.__file__)), "--impl", "reference", "--steps", "1",
+                        "--warmup", "3"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout[-2000:]
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["metric"] == bench.METRIC and d["unit"] == bench.UNIT
+    assert d["higher_is_better"] is True and d["steps"] == 1 and d["warmup"] == 3 and d["value"] > 0
+    cb = d["cpu_baseline"]
+    assert cb["value"] == d["value"] and cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    assert d["config"]["workload"] == "harmonic_clicks_48k_eemd"
