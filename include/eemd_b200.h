@@ -224,7 +224,8 @@ int32_t eemd_run_static(const eemd_params* p, const void* x, const int64_t* leng
  *   imf_mean[s][m][n] = imf_sum[s][m][n] / max(mode_count[s][m], 1)
  *   residual[s][n]    = x[s][n] - (sum over m < n_modes[s] of imf_mean)
  * n_modes[s] (device int32, out) = number of modes with mode_count > 0.
- * x is the original signal (dtype); imf_mean and residual are float64. */
+ * x is the original signal (dtype); imf_mean and residual are float64.
+ * Synchronises `stream` before returning (the outputs are complete). */
 int32_t eemd_finalize(const eemd_params* p, const void* x,
                       const int64_t* lengths, int32_t n_signals,
                       const double* imf_sum, const int32_t* mode_count,
